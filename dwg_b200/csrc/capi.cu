@@ -1,0 +1,656 @@
+// capi.cu -- extern "C" entry points of libdwg_b200.so (see include/dwg_b200.h).
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "pipeline.cuh"
+
+namespace dwg {
+
+static thread_local char g_err[1024] = {0};
+
+void set_error(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+}  // namespace dwg
+
+using namespace dwg;
+
+struct dwg_octree {
+    Octree t;
+};
+struct dwg_knn_index {
+    KnnIndex ix;
+};
+struct dwg_pipeline {
+    Pipeline p;
+};
+
+#define S(stream) ((cudaStream_t)(stream))
+
+#define API_GUARD(...)                                           \
+    try {                                                        \
+        __VA_ARGS__                                              \
+    } catch (const std::bad_alloc&) {                            \
+        set_error("host allocation failed");                     \
+        return DWG_ERR_NOMEM;                                    \
+    } catch (...) {                                              \
+        set_error("unexpected exception");                       \
+        return DWG_ERR_INVALID;                                  \
+    }
+
+extern "C" {
+
+const char* dwg_last_error(void) { return g_err; }
+const char* dwg_version(void) { return "dwg_b200 0.1 (sm_100a)"; }
+
+int dwg_gauss_map_init(const float* points_dev, int n, float* normals_dev, void* stream) {
+    API_GUARD(return gauss_map(points_dev, n, normals_dev, S(stream));)
+}
+
+int dwg_octree_build(const float* points_dev, int n, int max_depth, const float* areas_dev, void* stream,
+                     dwg_octree** out) {
+    API_GUARD({
+        DWG_REQUIRE(out != nullptr, "octree_build: out is null");
+        DWG_REQUIRE(points_dev != nullptr, "octree_build: points are null");
+        *out = nullptr;
+        dwg_octree* o = new dwg_octree();
+        int st = octree_build(o->t, points_dev, n, max_depth, areas_dev, S(stream));
+        if (st != DWG_OK) {
+            delete o;
+            return st;
+        }
+        *out = o;
+        return DWG_OK;
+    })
+}
+
+int dwg_octree_destroy(dwg_octree* tree) {
+    delete tree;
+    return DWG_OK;
+}
+
+int dwg_octree_num_nodes(const dwg_octree* tree, int* num_nodes) {
+    DWG_REQUIRE(tree && num_nodes, "octree_num_nodes: null argument");
+    *num_nodes = tree->t.M;
+    return DWG_OK;
+}
+
+int dwg_octree_update_normals(dwg_octree* tree, const float* normals_dev, const float* areas_dev, void* stream) {
+    API_GUARD({
+        DWG_REQUIRE(tree && normals_dev, "octree_update_normals: null argument");
+        DWG_TRY(octree_set_point_data(tree->t, normals_dev, areas_dev, nullptr, S(stream)));
+        return octree_update_normals(tree->t, S(stream));
+    })
+}
+
+int dwg_octree_update_info(dwg_octree* tree, const float* normals_dev, const float* areas_dev, void* stream) {
+    API_GUARD({
+        DWG_REQUIRE(tree, "octree_update_info: null tree");
+        DWG_TRY(octree_set_point_data(tree->t, normals_dev, areas_dev, nullptr, S(stream)));
+        DWG_TRY(octree_update_centres(tree->t, S(stream)));
+        return octree_update_normals(tree->t, S(stream));
+    })
+}
+
+int dwg_octree_status(const dwg_octree* tree, unsigned int* flags) {
+    API_GUARD({
+        DWG_REQUIRE(tree && flags, "octree_status: null argument");
+        DWG_CHECK_CUDA(cudaDeviceSynchronize());
+        unsigned int w[2] = {0, 0};
+        DWG_CHECK_CUDA(cudaMemcpy(w, tree->t.work.ptr, sizeof(w), cudaMemcpyDeviceToHost));
+        *flags = w[1];
+        if (w[1]) {
+            set_error("octree traversal reported error flags 0x%x", w[1]);
+            return DWG_ERR_DEVICE;
+        }
+        return DWG_OK;
+    })
+}
+
+int dwg_octree_export(const dwg_octree* tree, int* depth, int* pt_start, int* pt_count, int* skip, double* cm,
+                      double* radius, double* ec, int* perm) {
+    API_GUARD({
+        DWG_REQUIRE(tree, "octree_export: null tree");
+        const Octree& t = tree->t;
+        DWG_CHECK_CUDA(cudaDeviceSynchronize());
+        std::vector<int4> info(t.M);
+        DWG_CHECK_CUDA(cudaMemcpy(info.data(), t.info.ptr, sizeof(int4) * t.M, cudaMemcpyDeviceToHost));
+        for (int v = 0; v < t.M; ++v) {
+            if (depth) depth[v] = info[v].w & 0xff;
+            if (pt_start) pt_start[v] = info[v].x;
+            if (pt_count) pt_count[v] = info[v].y;
+            if (skip) skip[v] = info[v].z;
+        }
+        if (cm) DWG_CHECK_CUDA(cudaMemcpy(cm, t.cm_d.ptr, sizeof(double) * 3 * t.M, cudaMemcpyDeviceToHost));
+        if (radius) DWG_CHECK_CUDA(cudaMemcpy(radius, t.r_d.ptr, sizeof(double) * t.M, cudaMemcpyDeviceToHost));
+        if (ec) DWG_CHECK_CUDA(cudaMemcpy(ec, t.ec_d.ptr, sizeof(double) * 3 * t.M, cudaMemcpyDeviceToHost));
+        if (perm) DWG_CHECK_CUDA(cudaMemcpy(perm, t.perm.ptr, sizeof(int) * t.n, cudaMemcpyDeviceToHost));
+        return DWG_OK;
+    })
+}
+
+static int gwn_common(dwg_octree* tree, const float* normals_dev, const float* areas_dev, const float* radii_dev,
+                      const GwnQuery& q, const dwg_gwn_params* params, float* out_dev,
+                      unsigned long long* terms_dev, int* per_query, void* stream) {
+    DWG_REQUIRE(tree && params && out_dev, "gwn: null argument");
+    DWG_REQUIRE(params->beta >= 0.f, "gwn: beta must be >= 0");
+    DWG_TRY(octree_set_point_data(tree->t, normals_dev, areas_dev, radii_dev, S(stream)));
+    if (normals_dev || areas_dev) DWG_TRY(octree_update_normals(tree->t, S(stream)));
+    return gwn_eval(tree->t, q, *params, out_dev, terms_dev, per_query, S(stream));
+}
+
+int dwg_gwn_points(dwg_octree* tree, const float* normals_dev, const float* areas_dev, const float* radii_dev,
+                   const float* queries_dev, long long num_queries, const dwg_gwn_params* params, float* out_dev,
+                   unsigned long long* terms_dev, void* stream) {
+    API_GUARD({
+        DWG_REQUIRE(queries_dev && num_queries >= 0, "gwn_points: bad queries");
+        GwnQuery q;
+        q.q = queries_dev;
+        q.nq = num_queries;
+        return gwn_common(tree, normals_dev, areas_dev, radii_dev, q, params, out_dev, terms_dev, nullptr, stream);
+    })
+}
+
+// per-query term counts (checking the opening decisions)
+int dwg_gwn_points_counted(dwg_octree* tree, const float* normals_dev, const float* areas_dev,
+                           const float* radii_dev, const float* queries_dev, long long num_queries,
+                           const dwg_gwn_params* params, float* out_dev, int* per_query_terms_dev, void* stream) {
+    API_GUARD({
+        DWG_REQUIRE(queries_dev && num_queries >= 0, "gwn_points: bad queries");
+        GwnQuery q;
+        q.q = queries_dev;
+        q.nq = num_queries;
+        return gwn_common(tree, normals_dev, areas_dev, radii_dev, q, params, out_dev, nullptr, per_query_terms_dev,
+                          stream);
+    })
+}
+
+int dwg_gwn_grid(dwg_octree* tree, const float* normals_dev, const float* areas_dev, const float* radii_dev,
+                 const int res[3], const float origin[3], float spacing, const dwg_gwn_params* params,
+                 float* out_dev, unsigned long long* terms_dev, void* stream) {
+    API_GUARD({
+        DWG_REQUIRE(res && origin, "gwn_grid: null grid");
+        GwnQuery q;
+        for (int d = 0; d < 3; ++d) {
+            q.res[d] = res[d];
+            q.origin[d] = origin[d];
+        }
+        q.spacing = spacing;
+        return gwn_common(tree, normals_dev, areas_dev, radii_dev, q, params, out_dev, terms_dev, nullptr, stream);
+    })
+}
+
+int dwg_voxel_grid(const float* points_dev, int n, float offset, int s, void* stream, int res[3], float origin[3],
+                   float* spacing) {
+    API_GUARD({
+        DWG_REQUIRE(res && origin && spacing, "voxel_grid: null output");
+        return voxel_grid_host(points_dev, n, offset, s, S(stream), res, origin, spacing);
+    })
+}
+
+int dwg_marching_cubes(const float* field_dev, const int res[3], const float* positions_dev, const float origin[3],
+                       float spacing, float iso, float* tris_dev, float* centroids_dev, float* normals_dev,
+                       long long capacity, unsigned long long* num_tris_dev, long long* num_tris_host, void* stream) {
+    API_GUARD({
+        DWG_REQUIRE(res && (origin || positions_dev), "marching_cubes: grid undefined");
+        DWG_REQUIRE(capacity >= 0, "marching_cubes: negative capacity");
+        McGrid g;
+        for (int d = 0; d < 3; ++d) {
+            g.res[d] = res[d];
+            g.origin[d] = origin ? origin[d] : 0.f;
+        }
+        g.spacing = spacing;
+        g.positions = positions_dev;
+        static thread_local McWorkspace ws;
+        DevBuf<unsigned long long> own;
+        unsigned long long* cnt = num_tris_dev;
+        if (!cnt) {
+            DWG_TRY(own.reserve(1));
+            cnt = own.ptr;
+        }
+        DWG_TRY(mc_run(field_dev, g, iso, nullptr, tris_dev, centroids_dev, normals_dev, capacity, cnt, ws,
+                       S(stream)));
+        if (num_tris_host || !num_tris_dev) {
+            unsigned long long T = 0;
+            DWG_CHECK_CUDA(cudaMemcpyAsync(&T, cnt, sizeof(T), cudaMemcpyDeviceToHost, S(stream)));
+            DWG_CHECK_CUDA(cudaStreamSynchronize(S(stream)));
+            if (num_tris_host) *num_tris_host = (long long)T;
+            if ((long long)T > capacity) {
+                set_error("marching_cubes: %llu triangles exceed capacity %lld", T, capacity);
+                return DWG_ERR_OVERFLOW;
+            }
+        }
+        return DWG_OK;
+    })
+}
+
+int dwg_mc_tables(int* edge_table_host, signed char* tri_table_host) {
+    DWG_REQUIRE(edge_table_host && tri_table_host, "mc_tables: null output");
+    mc_tables_host(edge_table_host, tri_table_host);
+    return DWG_OK;
+}
+
+int dwg_knn_build(const float* points_dev, int n, void* stream, dwg_knn_index** out) {
+    API_GUARD({
+        DWG_REQUIRE(out, "knn_build: out is null");
+        *out = nullptr;
+        dwg_knn_index* o = new dwg_knn_index();
+        int st = knn_build(o->ix, points_dev, n, S(stream));
+        if (st != DWG_OK) {
+            delete o;
+            return st;
+        }
+        *out = o;
+        return DWG_OK;
+    })
+}
+
+int dwg_knn_destroy(dwg_knn_index* index) {
+    delete index;
+    return DWG_OK;
+}
+
+int dwg_knn_query(dwg_knn_index* index, const float* queries_dev, long long num_queries, int k, int* out_dev,
+                  void* stream) {
+    API_GUARD({
+        DWG_REQUIRE(index && queries_dev && out_dev, "knn_query: null argument");
+        DWG_REQUIRE(k <= index->ix.n, "knn_query: k=%d exceeds the number of points %d", k, index->ix.n);
+        KnnQuery q;
+        q.q = queries_dev;
+        q.nq = num_queries;
+        return knn_query(index->ix, q, k, out_dev, S(stream));
+    })
+}
+
+int dwg_knn(const float* points_dev, int n, const float* queries_dev, long long num_queries, int k, int* out_dev,
+            void* stream) {
+    API_GUARD({
+        DWG_REQUIRE(k >= 1 && k <= n, "knn: k=%d must be in [1, n=%d]", k, n);
+        KnnIndex ix;
+        DWG_TRY(knn_build(ix, points_dev, n, S(stream)));
+        KnnQuery q;
+        q.q = queries_dev;
+        q.nq = num_queries;
+        DWG_TRY(knn_query(ix, q, k, out_dev, S(stream)));
+        DWG_CHECK_CUDA(cudaStreamSynchronize(S(stream)));
+        return DWG_OK;
+    })
+}
+
+int dwg_diffuse_normals(const int* knn_dev, const float* tri_normals_dev, long long num_tris, int k, int num_points,
+                        float* normals_dev, unsigned char* is_zero_dev, int* zero_count_dev, void* stream) {
+    API_GUARD({
+        DevBuf<long long> acc;
+        DWG_TRY(acc.reserve((size_t)num_points * 3));
+        DWG_CHECK_CUDA(cudaMemsetAsync(acc.ptr, 0, sizeof(long long) * 3 * num_points, S(stream)));
+        DWG_TRY(diffuse_normals(knn_dev, tri_normals_dev, num_tris, nullptr, k, num_points, normals_dev, acc.ptr,
+                                is_zero_dev, zero_count_dev, S(stream)));
+        DWG_CHECK_CUDA(cudaStreamSynchronize(S(stream)));
+        return DWG_OK;
+    })
+}
+
+int dwg_zero_repair(dwg_knn_index* index, float* normals_dev, const unsigned char* is_zero_dev,
+                    const int* zero_count_dev, int k, int min_zero, void* stream) {
+    API_GUARD({
+        DWG_REQUIRE(index, "zero_repair: null index");
+        (void)zero_count_dev;
+        ZeroRepairWs ws;
+        // positions in input order are needed for the query side
+        DevBuf<float> pos;
+        DWG_TRY(pos.reserve((size_t)index->ix.n * 3));
+        std::vector<float4> h(index->ix.n);
+        std::vector<float> hp((size_t)index->ix.n * 3);
+        DWG_CHECK_CUDA(cudaMemcpyAsync(h.data(), index->ix.pts.ptr, sizeof(float4) * index->ix.n,
+                                       cudaMemcpyDeviceToHost, S(stream)));
+        DWG_CHECK_CUDA(cudaStreamSynchronize(S(stream)));
+        for (int j = 0; j < index->ix.n; ++j) {
+            int id;
+            memcpy(&id, &h[j].w, 4);
+            hp[(size_t)id * 3] = h[j].x;
+            hp[(size_t)id * 3 + 1] = h[j].y;
+            hp[(size_t)id * 3 + 2] = h[j].z;
+        }
+        DWG_CHECK_CUDA(cudaMemcpyAsync(pos.ptr, hp.data(), sizeof(float) * hp.size(), cudaMemcpyHostToDevice,
+                                       S(stream)));
+        DWG_TRY(zero_repair(index->ix, pos.ptr, index->ix.n, normals_dev, is_zero_dev, k, min_zero, ws, S(stream)));
+        DWG_CHECK_CUDA(cudaStreamSynchronize(S(stream)));
+        return DWG_OK;
+    })
+}
+
+int dwg_load_normals(const int* knn_dev, int k, long long num_queries, const float* leaf_normals_dev, float* out_dev,
+                     void* stream) {
+    API_GUARD(return load_normals(knn_dev, k, num_queries, leaf_normals_dev, out_dev, S(stream));)
+}
+
+int dwg_radii(const float* points_dev, int n, const int* knn_dev, int k, float* radii_dev, void* stream) {
+    API_GUARD(return radii(points_dev, n, knn_dev, k, radii_dev, S(stream));)
+}
+
+void dwg_params_default(dwg_params* p) {
+    if (!p) return;
+    p->in_normal = 3;
+    p->grid_reso = 400;
+    p->final_reso = 500;
+    p->kw = 10;
+    p->final_kw = 10;
+    p->normal_kw = 10;
+    p->max_depth = 10;
+    p->lambda = 10.f;
+    p->min_num = 0;
+    p->use_radii = 0;
+    p->offset_1 = 0.05f;
+    p->offset_2 = 0.01f;
+    p->use_leaves_generate = 0;
+    p->total_iter = 40;
+    p->beta = 2.3f;
+    p->area = 2e-6f;
+    p->screen = 0.0015f;
+    p->knn_tri = 15;
+    p->knn_zero = 10;
+    p->precision = 1;
+    p->use_graph = 1;
+}
+
+int dwg_pipeline_create(const float* points_dev, const float* normals_dev, int n, const dwg_params* params,
+                        void* stream, dwg_pipeline** out) {
+    API_GUARD({
+        DWG_REQUIRE(out && params, "pipeline_create: null argument");
+        *out = nullptr;
+        dwg_pipeline* o = new dwg_pipeline();
+        int st = o->p.setup(points_dev, normals_dev, n, *params, S(stream));
+        if (st != DWG_OK) {
+            delete o;
+            return st;
+        }
+        *out = o;
+        return DWG_OK;
+    })
+}
+
+int dwg_pipeline_destroy(dwg_pipeline* p) {
+    if (p) cudaStreamSynchronize(p->p.s);
+    delete p;
+    return DWG_OK;
+}
+
+int dwg_pipeline_iterate(dwg_pipeline* p, int n_iters) {
+    API_GUARD({
+        DWG_REQUIRE(p, "pipeline_iterate: null pipeline");
+        return p->p.iterate(n_iters);
+    })
+}
+
+int dwg_pipeline_finalize(dwg_pipeline* p) {
+    API_GUARD({
+        DWG_REQUIRE(p, "pipeline_finalize: null pipeline");
+        return p->p.finalize();
+    })
+}
+
+int dwg_pipeline_size(dwg_pipeline* p, const char* what, long long* value) {
+    API_GUARD({
+        DWG_REQUIRE(p && what && value, "pipeline_size: null argument");
+        Pipeline& q = p->p;
+        if (!strcmp(what, "leaves"))
+            *value = q.L;
+        else if (!strcmp(what, "points"))
+            *value = q.n;
+        else if (!strcmp(what, "iterations"))
+            *value = q.iter;
+        else if (!strcmp(what, "grid"))
+            *value = (long long)q.gres[0] * q.gres[1] * q.gres[2];
+        else if (!strcmp(what, "final_grid"))
+            *value = (long long)q.fres[0] * q.fres[1] * q.fres[2];
+        else if (!strcmp(what, "triangles")) {
+            DWG_REQUIRE(q.finalized, "pipeline_size: not finalized");
+            unsigned long long T = 0;
+            DWG_CHECK_CUDA(cudaMemcpyAsync(&T, q.final_ntri.ptr, sizeof(T), cudaMemcpyDeviceToHost, q.s));
+            DWG_CHECK_CUDA(cudaStreamSynchronize(q.s));
+            *value = (long long)T < q.final_cap ? (long long)T : q.final_cap;
+        } else {
+            set_error("pipeline_size: unknown item '%s'", what);
+            return DWG_ERR_INVALID;
+        }
+        return DWG_OK;
+    })
+}
+
+int dwg_pipeline_get(dwg_pipeline* p, const char* what, void* dst) {
+    API_GUARD({
+        DWG_REQUIRE(p && what && dst, "pipeline_get: null argument");
+        Pipeline& q = p->p;
+        DWG_CHECK_CUDA(cudaStreamSynchronize(q.s));
+        auto cp = [&](const void* src, size_t bytes) -> int {
+            DWG_CHECK_CUDA(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost));
+            return DWG_OK;
+        };
+        const int it = q.iter;
+        if (!strcmp(what, "leaf_pos")) return cp(q.leaf_pos.ptr, sizeof(float) * 3 * q.L);
+        if (!strcmp(what, "leaf_nrm")) return cp(q.leaf_nrm.ptr, sizeof(float) * 3 * q.L);
+        if (!strcmp(what, "iso")) return it ? cp(q.iso_hist.ptr, sizeof(float) * it) : DWG_OK;
+        if (!strcmp(what, "tri_count")) return it ? cp(q.tri_hist.ptr, sizeof(long long) * it) : DWG_OK;
+        if (!strcmp(what, "zero_count")) return it ? cp(q.zero_hist.ptr, sizeof(int) * it) : DWG_OK;
+        if (!strcmp(what, "terms")) return it ? cp(q.terms_hist.ptr, sizeof(unsigned long long) * it) : DWG_OK;
+        if (!strcmp(what, "field")) return cp(q.field.ptr, sizeof(float) * q.gres[0] * q.gres[1] * (size_t)q.gres[2]);
+        if (!strcmp(what, "grid_res")) {
+            memcpy(dst, q.gres, sizeof(q.gres));
+            return DWG_OK;
+        }
+        if (!strcmp(what, "grid_origin")) {
+            float v[4] = {q.gorg[0], q.gorg[1], q.gorg[2], q.gh};
+            memcpy(dst, v, sizeof(v));
+            return DWG_OK;
+        }
+        DWG_REQUIRE(q.finalized, "pipeline_get: '%s' needs finalize()", what);
+        if (!strcmp(what, "point_nrm")) return cp(q.point_nrm.ptr, sizeof(float) * 3 * q.n);
+        if (!strcmp(what, "final_field"))
+            return cp(q.final_field.ptr, sizeof(float) * q.fres[0] * q.fres[1] * (size_t)q.fres[2]);
+        if (!strcmp(what, "final_iso")) return cp(q.final_iso.ptr, sizeof(float));
+        if (!strcmp(what, "final_res")) {
+            memcpy(dst, q.fres, sizeof(q.fres));
+            return DWG_OK;
+        }
+        if (!strcmp(what, "final_origin")) {
+            float v[4] = {q.forg[0], q.forg[1], q.forg[2], q.fh};
+            memcpy(dst, v, sizeof(v));
+            return DWG_OK;
+        }
+        if (!strcmp(what, "tris")) {
+            unsigned long long T = 0;
+            DWG_CHECK_CUDA(cudaMemcpy(&T, q.final_ntri.ptr, sizeof(T), cudaMemcpyDeviceToHost));
+            long long t = (long long)T < q.final_cap ? (long long)T : q.final_cap;
+            return t ? cp(q.tris.ptr, sizeof(float) * 9 * (size_t)t) : DWG_OK;
+        }
+        set_error("pipeline_get: unknown item '%s'", what);
+        return DWG_ERR_INVALID;
+    })
+}
+
+int dwg_pipeline_device_ptr(dwg_pipeline* p, const char* what, void** ptr) {
+    DWG_REQUIRE(p && what && ptr, "pipeline_device_ptr: null argument");
+    Pipeline& q = p->p;
+    if (!strcmp(what, "leaf_pos")) *ptr = q.leaf_pos.ptr;
+    else if (!strcmp(what, "leaf_nrm")) *ptr = q.leaf_nrm.ptr;
+    else if (!strcmp(what, "point_nrm")) *ptr = q.point_nrm.ptr;
+    else if (!strcmp(what, "tris")) *ptr = q.tris.ptr;
+    else if (!strcmp(what, "field")) *ptr = q.field.ptr;
+    else if (!strcmp(what, "final_field")) *ptr = q.final_field.ptr;
+    else {
+        set_error("pipeline_device_ptr: unknown item '%s'", what);
+        return DWG_ERR_INVALID;
+    }
+    return DWG_OK;
+}
+
+int dwg_reconstruct_host(const float* points_host, const float* normals_host, int n, const dwg_params* params,
+                         float* point_normals_host, float* tris_host, long long tri_capacity, long long* num_tris,
+                         void* stream) {
+    API_GUARD({
+        DWG_REQUIRE(points_host && params && n >= 2, "reconstruct_host: bad arguments");
+        cudaStream_t st = S(stream);
+        DevBuf<float> P, N;
+        DWG_TRY(P.reserve((size_t)n * 3));
+        DWG_CHECK_CUDA(cudaMemcpyAsync(P.ptr, points_host, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, st));
+        if (normals_host) {
+            DWG_TRY(N.reserve((size_t)n * 3));
+            DWG_CHECK_CUDA(cudaMemcpyAsync(N.ptr, normals_host, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, st));
+        }
+        dwg_pipeline* p = nullptr;
+        DWG_TRY(dwg_pipeline_create(P.ptr, normals_host ? N.ptr : nullptr, n, params, stream, &p));
+        int rc = dwg_pipeline_iterate(p, params->total_iter);
+        if (rc == DWG_OK) rc = dwg_pipeline_finalize(p);
+        long long T = 0;
+        if (rc == DWG_OK) rc = dwg_pipeline_size(p, "triangles", &T);
+        if (rc == DWG_OK && point_normals_host && !params->use_leaves_generate)
+            rc = dwg_pipeline_get(p, "point_nrm", point_normals_host);
+        if (rc == DWG_OK && num_tris) *num_tris = T;
+        if (rc == DWG_OK && tris_host && T > 0) {
+            long long c = T < tri_capacity ? T : tri_capacity;
+            if (c > 0) {
+                cudaError_t e = cudaMemcpy(tris_host, p->p.tris.ptr, sizeof(float) * 9 * (size_t)c,
+                                           cudaMemcpyDeviceToHost);
+                if (e != cudaSuccess) {
+                    set_error("reconstruct_host: copy failed: %s", cudaGetErrorString(e));
+                    rc = DWG_ERR_CUDA;
+                }
+            }
+            if (rc == DWG_OK && T > tri_capacity) {
+                set_error("reconstruct_host: %lld triangles exceed capacity %lld", T, tri_capacity);
+                rc = DWG_ERR_OVERFLOW;
+            }
+        }
+        dwg_pipeline_destroy(p);
+        return rc;
+    })
+}
+
+// ------------------------------------------------------------------ IO --
+// ReadPointandNormals (include/DWGProcess.h:53-97)
+int dwg_read_xyz(const char* path, int normalize, float** points, float** normals, int* n) {
+    API_GUARD({
+        DWG_REQUIRE(path && points && n, "read_xyz: null argument");
+        FILE* f = fopen(path, "r");
+        DWG_REQUIRE(f != nullptr, "read_xyz: cannot open '%s'", path);
+        std::vector<double> P, N;
+        char line[4096];
+        long long lineno = 0;
+        while (fgets(line, sizeof(line), f)) {
+            ++lineno;
+            double v[6];
+            int k = sscanf(line, "%lf %lf %lf %lf %lf %lf", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5]);
+            if (k <= 0) continue;  // blank line
+            if (k < 3) {
+                fclose(f);
+                set_error("read_xyz: line %lld of '%s' has %d values (need 3 or 6)", lineno, path, k);
+                return DWG_ERR_INVALID;
+            }
+            for (int d = 0; d < 3; ++d) {
+                if (!std::isfinite(v[d])) {
+                    fclose(f);
+                    set_error("read_xyz: non-finite coordinate on line %lld of '%s'", lineno, path);
+                    return DWG_ERR_INVALID;
+                }
+                P.push_back(v[d]);
+            }
+            for (int d = 3; d < 6; ++d) N.push_back(k == 6 ? v[d] : 0.0);
+        }
+        fclose(f);
+        int cnt = (int)(P.size() / 3);
+        DWG_REQUIRE(cnt > 0, "read_xyz: no points in '%s'", path);
+        if (normalize) {
+            double c[3] = {0, 0, 0};
+            for (int i = 0; i < cnt; ++i)
+                for (int d = 0; d < 3; ++d) c[d] += P[(size_t)i * 3 + d];
+            for (int d = 0; d < 3; ++d) c[d] /= (1.0 * cnt);
+            double scale = 0;
+            for (int i = 0; i < cnt; ++i)
+                for (int d = 0; d < 3; ++d) {
+                    P[(size_t)i * 3 + d] -= c[d];
+                    scale = std::max(2.0 * std::fabs(P[(size_t)i * 3 + d]), scale);
+                }
+            if (scale == 0) scale = 1;
+            for (auto& x : P) x /= scale;
+        }
+        float* po = (float*)malloc(sizeof(float) * 3 * cnt);
+        float* no = normals ? (float*)malloc(sizeof(float) * 3 * cnt) : nullptr;
+        if (!po || (normals && !no)) {
+            free(po);
+            free(no);
+            set_error("read_xyz: host allocation failed");
+            return DWG_ERR_NOMEM;
+        }
+        for (size_t i = 0; i < P.size(); ++i) po[i] = (float)P[i];
+        if (no)
+            for (size_t i = 0; i < N.size(); ++i) no[i] = (float)N[i];
+        *points = po;
+        if (normals) *normals = no;
+        *n = cnt;
+        return DWG_OK;
+    })
+}
+
+void dwg_free_host(void* p) { free(p); }
+
+// save_binary_STL (src/TurboMC.cu:344-371): 80-byte header, uint32 count,
+// per triangle normal (cross / |cross|, 0 if degenerate), 3 vertices, uint16 0
+int dwg_write_stl(const char* path, const float* tris, long long T) {
+    API_GUARD({
+        DWG_REQUIRE(path && (tris || T == 0) && T >= 0 && T <= 0xffffffffll, "write_stl: bad arguments");
+        FILE* f = fopen(path, "wb");
+        DWG_REQUIRE(f != nullptr, "write_stl: cannot create '%s'", path);
+        char header[80] = {0};
+        uint32_t cnt = (uint32_t)T;
+        bool ok = fwrite(header, 1, 80, f) == 80 && fwrite(&cnt, 4, 1, f) == 1;
+        std::vector<unsigned char> rec(50);
+        for (long long t = 0; ok && t < T; ++t) {
+            const float* v = tris + t * 9;
+            float e1[3] = {v[3] - v[0], v[4] - v[1], v[5] - v[2]};
+            float e2[3] = {v[6] - v[0], v[7] - v[1], v[8] - v[2]};
+            float c[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
+            float len = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+            float nrm[3] = {0, 0, 0};
+            if (len > 0)
+                for (int d = 0; d < 3; ++d) nrm[d] = c[d] / len;
+            memcpy(rec.data(), nrm, 12);
+            memcpy(rec.data() + 12, v, 36);
+            rec[48] = rec[49] = 0;
+            ok = fwrite(rec.data(), 1, 50, f) == 50;
+        }
+        fclose(f);
+        DWG_REQUIRE(ok, "write_stl: cannot write '%s'", path);
+        return DWG_OK;
+    })
+}
+
+// oriented point cloud output (src/TurboDWG.cu:903-923)
+int dwg_write_xyz(const char* path, const float* P, const float* N, int n) {
+    API_GUARD({
+        DWG_REQUIRE(path && P && n >= 0, "write_xyz: bad arguments");
+        FILE* f = fopen(path, "w");
+        DWG_REQUIRE(f != nullptr, "write_xyz: cannot create '%s'", path);
+        for (int i = 0; i < n; ++i) {
+            if (N)
+                fprintf(f, "%g %g %g %g %g %g\n", P[i * 3], P[i * 3 + 1], P[i * 3 + 2], N[i * 3], N[i * 3 + 1],
+                        N[i * 3 + 2]);
+            else
+                fprintf(f, "%g %g %g\n", P[i * 3], P[i * 3 + 1], P[i * 3 + 2]);
+        }
+        fclose(f);
+        return DWG_OK;
+    })
+}
+
+}  // extern "C"

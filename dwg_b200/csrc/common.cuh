@@ -1,0 +1,107 @@
+// common.cuh -- shared helpers of the dwg_b200 CUDA library (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "../../include/dwg_b200.h"
+
+namespace dwg {
+
+// ---------------------------------------------------------------- errors --
+void set_error(const char* fmt, ...);
+
+struct Status {
+    int code = DWG_OK;
+};
+
+#define DWG_CHECK_CUDA(expr)                                                     \
+    do {                                                                         \
+        cudaError_t _e = (expr);                                                 \
+        if (_e != cudaSuccess) {                                                 \
+            ::dwg::set_error("%s failed: %s (%s:%d)", #expr, cudaGetErrorString(_e), \
+                             __FILE__, __LINE__);                                \
+            return _e == cudaErrorMemoryAllocation ? DWG_ERR_NOMEM : DWG_ERR_CUDA; \
+        }                                                                        \
+    } while (0)
+
+#define DWG_CHECK_LAUNCH() DWG_CHECK_CUDA(cudaGetLastError())
+
+#define DWG_REQUIRE(cond, ...)              \
+    do {                                    \
+        if (!(cond)) {                      \
+            ::dwg::set_error(__VA_ARGS__);  \
+            return DWG_ERR_INVALID;         \
+        }                                   \
+    } while (0)
+
+#define DWG_TRY(expr)              \
+    do {                           \
+        int _s = (expr);           \
+        if (_s != DWG_OK) return _s; \
+    } while (0)
+
+// ------------------------------------------------------ device buffers --
+// Grow-only device buffer; owner frees.
+template <typename T>
+struct DevBuf {
+    T* ptr = nullptr;
+    size_t n = 0;
+    int reserve(size_t count) {
+        if (count <= n && ptr) return DWG_OK;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        n = 0;
+        size_t bytes = (count ? count : 1) * sizeof(T);
+        cudaError_t e = cudaMalloc(&ptr, bytes);
+        if (e != cudaSuccess) {
+            set_error("cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
+            ptr = nullptr;
+            return DWG_ERR_NOMEM;
+        }
+        n = count ? count : 1;
+        return DWG_OK;
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        n = 0;
+    }
+    ~DevBuf() { release(); }
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+};
+
+inline int num_sms() {
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    return sms;
+}
+
+inline unsigned div_up(long long a, long long b) { return (unsigned)((a + b - 1) / b); }
+
+// ------------------------------------------- exact single-precision ops --
+// The discrete decisions (opening test, kNN keys, marching-cubes geometry)
+// use round-to-nearest intrinsics so that they cannot be contracted into
+// FMAs and match the CPU oracle operation for operation.
+__device__ __forceinline__ float sq3_rn(float dx, float dy, float dz) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+}
+
+__device__ __forceinline__ float inv_len_eps(float len) {
+    // 1 / (len + 1e-8), the sum taken in double and rounded to float, like the
+    // reference's __frcp_rn(length + 1e-8)
+    return __frcp_rn(__double2float_rn(__dadd_rn((double)len, 1e-8)));
+}
+
+}  // namespace dwg

@@ -1,0 +1,299 @@
+// gwn.cu -- Barnes-Hut generalised-winding-number sums, one warp per 32 queries.
+//
+// The reference (src/TurboLibiGWN.cu:328-836) runs one thread per query over
+// pointer-chasing AoS nodes with a stackless DFS.  Here a warp walks the
+// octree for 32 spatially coherent queries at once (a 4x4x2 brick of grid
+// samples, or 32 consecutive Morton-ordered points).  Every stack entry
+// carries the mask of lanes that opened the node, so each lane still takes
+// exactly the reference's per-query decisions -- a child is a dipole term
+// when |CM - q| > beta R, otherwise it is opened, and leaves are summed point
+// by point -- while node and point loads are warp-broadcast.  Sums are FP32
+// with an optional compensated (two-sum) accumulator per lane.
+#include "gwn.cuh"
+
+namespace dwg {
+
+constexpr int kGwnWarps = 8;
+constexpr int kGwnStack = 8 * (kMaxDepth + 1) + 8;
+constexpr float kFourPi = 12.566370614359172f;
+
+template <bool SCREENED, int PREC>
+__device__ __forceinline__ bool gwn_term(float dx, float dy, float dz, float d, float s, float sigma,
+                                         float& v) {
+    float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    if (SCREENED) {
+        float r = (PREC >= 2) ? sqrtf(r2) : r2 * rsqrtf(r2);
+        if (!(r > 1e-10f)) return false;
+        float rho = fmaxf(r, s);
+        float sr = sigma * rho;
+        float e = (PREC >= 2) ? expf(sr) : __expf(sr);
+        float r3 = rho * rho * rho;
+        float den = fmaf(e, kFourPi * r3, 1e-7f);
+        float num = fmaf(sigma, rho, 1.0f) * d;
+        float res = (PREC >= 2) ? __fdiv_rn(num, den) : __fdividef(num, den);
+        // sign of d = A (p - q).n, src/TurboLibiGWN.cu:550-584
+        v = copysignf(fabsf(res), d);
+        return true;
+    } else {
+        if (r2 == 0.0f) {
+            v = 0.0f;
+            return true;
+        }
+        float r = (PREC >= 2) ? sqrtf(r2) : r2 * rsqrtf(r2);
+        float den = fmaf(kFourPi * r, r2, 1e-8f);
+        v = (PREC >= 2) ? __fdiv_rn(d, den) : __fdividef(d, den);
+        return true;
+    }
+}
+
+template <int PREC>
+__device__ __forceinline__ void acc_add(float& s, float& c, float v) {
+    if (PREC == 0) {
+        s += v;
+    } else {
+        // Knuth two-sum: s + v = t + err exactly
+        float t = __fadd_rn(s, v);
+        float bp = __fsub_rn(t, s);
+        float err = __fadd_rn(__fsub_rn(s, __fsub_rn(t, bp)), __fsub_rn(v, bp));
+        s = t;
+        c = __fadd_rn(c, err);
+    }
+}
+
+struct GwnArgs {
+    const int4* __restrict__ info;
+    const float4* __restrict__ cmr;
+    const float4* __restrict__ ec;
+    const float4* __restrict__ pa;
+    const float4* __restrict__ nr;
+    float beta, sigma, screen;
+    const float* sigma_dev;
+    int use_radii;
+    const float* __restrict__ q;
+    long long nq;
+    int rx, ry, rz;
+    float ox, oy, oz, h;
+    int bx, by;  // bricks per row / column
+    long long ngroups;
+    float* __restrict__ out;
+    unsigned long long* terms_total;
+    int* per_query_terms;
+    unsigned int* work;  // [0] counter, [1] error flags (sticky)
+    int num_nodes, num_points;
+};
+
+template <bool GRID, bool SCREENED, int PREC>
+__global__ void __launch_bounds__(kGwnWarps * 32) k_gwn(GwnArgs a) {
+    __shared__ int2 stack[kGwnWarps][kGwnStack];
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    const float sigma = a.sigma_dev ? *a.sigma_dev : a.sigma;
+    unsigned long long my_terms = 0;
+    for (;;) {
+        unsigned g = 0;
+        if (lane == 0) g = atomicAdd(&a.work[0], 1u);
+        g = __shfl_sync(FULL, g, 0);
+        if ((long long)g >= a.ngroups) break;
+        bool valid;
+        float qx = 0.f, qy = 0.f, qz = 0.f;
+        long long qi;
+        if (GRID) {
+            int bxi = (int)(g % (unsigned)a.bx);
+            unsigned t = g / (unsigned)a.bx;
+            int byi = (int)(t % (unsigned)a.by);
+            int bzi = (int)(t / (unsigned)a.by);
+            int x = bxi * 4 + (lane & 3), y = byi * 4 + ((lane >> 2) & 3), z = bzi * 2 + (lane >> 4);
+            valid = x < a.rx && y < a.ry && z < a.rz;
+            qi = (long long)x + (long long)a.rx * ((long long)y + (long long)a.ry * z);
+            qx = __fadd_rn(a.ox, __fmul_rn((float)x, a.h));
+            qy = __fadd_rn(a.oy, __fmul_rn((float)y, a.h));
+            qz = __fadd_rn(a.oz, __fmul_rn((float)z, a.h));
+        } else {
+            qi = (long long)g * 32 + lane;
+            valid = qi < a.nq;
+            if (valid) {
+                qx = a.q[qi * 3];
+                qy = a.q[qi * 3 + 1];
+                qz = a.q[qi * 3 + 2];
+            }
+        }
+        const unsigned vm = __ballot_sync(FULL, valid);
+        float s = 0.f, c = 0.f;
+        int nterm = 0;
+
+        auto leaf_points = [&](int start, int cnt) {
+            for (int j = start; j < start + cnt; ++j) {
+                float4 p = a.pa[j];
+                float4 nn = a.nr[j];
+                float dx = p.x - qx, dy = p.y - qy, dz = p.z - qz;
+                float d = p.w * fmaf(dx, nn.x, fmaf(dy, nn.y, dz * nn.z));
+                float sc = a.use_radii ? nn.w : a.screen;
+                float v;
+                if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, sc, sigma, v)) {
+                    acc_add<PREC>(s, c, v);
+                    ++nterm;
+                }
+            }
+        };
+
+        const int4 root = a.info[0];
+        int sp = 0;
+        if (root.w & kLeafFlag) {
+            if (valid && root.x >= 0 && root.y >= 0 && root.x + root.y <= a.num_points) leaf_points(root.x, root.y);
+        } else {
+            if (lane == 0) stack[w][0] = make_int2(0, (int)vm);
+            sp = 1;
+        }
+        while (sp > 0) {
+            __syncwarp();
+            const int2 e = stack[w][--sp];
+            __syncwarp();
+            if (e.x < 0 || e.x >= a.num_nodes) {
+                if (lane == 0) atomicOr(&a.work[1], 2u);
+                continue;
+            }
+            const bool act = (((unsigned)e.y) >> lane) & 1u;
+            const int end = a.info[e.x].z;
+            int ch = e.x + 1;
+            while (ch < end) {
+                const int4 ic = a.info[ch];
+                // structural guard: a child's subtree ends after it and within
+                // its parent's; a leaf's points lie inside the point array
+                if (ic.z <= ch || ic.z > end || end > a.num_nodes) {
+                    if (lane == 0) atomicOr(&a.work[1], 2u);
+                    break;
+                }
+                if (ic.w & kLeafFlag) {
+                    if (ic.x < 0 || ic.y < 0 || ic.x + ic.y > a.num_points) {
+                        if (lane == 0) atomicOr(&a.work[1], 4u);
+                    } else if (act) {
+                        leaf_points(ic.x, ic.y);
+                    }
+                } else {
+                    bool near = false;
+                    if (act) {
+                        const float4 cm = a.cmr[ch];
+                        // opening test in round-to-nearest single precision
+                        // (src/TurboLibiGWN.cu:636-644)
+                        float dx = __fsub_rn(cm.x, qx), dy = __fsub_rn(cm.y, qy), dz = __fsub_rn(cm.z, qz);
+                        float dist = __fsqrt_rn(sq3_rn(dx, dy, dz));
+                        if (dist > __fmul_rn(a.beta, cm.w)) {
+                            const float4 m = a.ec[ch];
+                            float d = fmaf(dx, m.x, fmaf(dy, m.y, dz * m.z));
+                            float v;
+                            if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, a.screen, sigma, v)) {
+                                acc_add<PREC>(s, c, v);
+                                ++nterm;
+                            }
+                        } else {
+                            near = true;
+                        }
+                    }
+                    const unsigned nm = __ballot_sync(FULL, near);
+                    if (nm) {
+                        if (sp < kGwnStack) {
+                            if (lane == 0) stack[w][sp] = make_int2(ch, (int)nm);
+                            ++sp;
+                        } else if (lane == 0) {
+                            atomicOr(&a.work[1], 1u);
+                        }
+                    }
+                }
+                ch = ic.z;
+            }
+        }
+        if (valid) {
+            a.out[qi] = (PREC == 0) ? s : __fadd_rn(s, c);
+            if (a.per_query_terms) a.per_query_terms[qi] = nterm;
+        }
+        my_terms += (unsigned long long)nterm;
+    }
+    if (a.terms_total) {
+        for (int o = 16; o > 0; o >>= 1) my_terms += __shfl_down_sync(FULL, my_terms, o);
+        if (lane == 0 && my_terms) atomicAdd(a.terms_total, my_terms);
+    }
+}
+
+template <bool GRID, bool SCREENED, int PREC>
+static int launch(const GwnArgs& a, cudaStream_t s) {
+    static int blocks_per_sm = 0;
+    if (!blocks_per_sm) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_gwn<GRID, SCREENED, PREC>,
+                                                      kGwnWarps * 32, 0);
+        if (blocks_per_sm <= 0) blocks_per_sm = 1;
+    }
+    long long want = (a.ngroups + kGwnWarps - 1) / kGwnWarps;
+    long long grid = (long long)num_sms() * blocks_per_sm;
+    if (want < grid) grid = want > 0 ? want : 1;
+    k_gwn<GRID, SCREENED, PREC><<<(unsigned)grid, kGwnWarps * 32, 0, s>>>(a);
+    DWG_CHECK_LAUNCH();
+    return DWG_OK;
+}
+
+template <bool GRID>
+static int dispatch(const GwnArgs& a, const dwg_gwn_params& p, cudaStream_t s) {
+    const int prec = p.precision < 0 ? 0 : (p.precision > 2 ? 2 : p.precision);
+    if (p.screened) {
+        if (prec == 0) return launch<GRID, true, 0>(a, s);
+        if (prec == 1) return launch<GRID, true, 1>(a, s);
+        return launch<GRID, true, 2>(a, s);
+    }
+    if (prec == 0) return launch<GRID, false, 0>(a, s);
+    if (prec == 1) return launch<GRID, false, 1>(a, s);
+    return launch<GRID, false, 2>(a, s);
+}
+
+int gwn_eval(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, float* out,
+             unsigned long long* terms_total, int* per_query_terms, cudaStream_t s,
+             const float* sigma_dev) {
+    DWG_REQUIRE(t.M > 0, "gwn: octree is empty");
+    DWG_REQUIRE(out != nullptr, "gwn: output is null");
+    GwnArgs a;
+    a.info = t.info.ptr;
+    a.cmr = t.cmr.ptr;
+    a.ec = t.ec.ptr;
+    a.pa = t.pa.ptr;
+    a.nr = t.nr.ptr;
+    a.beta = p.beta;
+    a.sigma = p.sigma;
+    a.sigma_dev = sigma_dev;
+    a.screen = p.screen;
+    a.use_radii = p.use_radii;
+    a.out = out;
+    a.terms_total = terms_total;
+    a.per_query_terms = per_query_terms;
+    DWG_TRY(t.work.reserve(2));
+    a.work = t.work.ptr;
+    a.num_nodes = t.M;
+    a.num_points = t.n;
+    // the counter restarts with every launch; the error word is sticky
+    DWG_CHECK_CUDA(cudaMemsetAsync(t.work.ptr, 0, sizeof(unsigned int), s));
+    if (q.q) {
+        a.q = q.q;
+        a.nq = q.nq;
+        a.rx = a.ry = a.rz = 0;
+        a.ox = a.oy = a.oz = a.h = 0.f;
+        a.bx = a.by = 1;
+        a.ngroups = (q.nq + 31) / 32;
+        if (a.ngroups == 0) return DWG_OK;
+        return dispatch<false>(a, p, s);
+    }
+    DWG_REQUIRE(q.res[0] > 0 && q.res[1] > 0 && q.res[2] > 0, "gwn: bad grid resolution");
+    a.q = nullptr;
+    a.nq = (long long)q.res[0] * q.res[1] * q.res[2];
+    a.rx = q.res[0];
+    a.ry = q.res[1];
+    a.rz = q.res[2];
+    a.ox = q.origin[0];
+    a.oy = q.origin[1];
+    a.oz = q.origin[2];
+    a.h = q.spacing;
+    a.bx = (q.res[0] + 3) / 4;
+    a.by = (q.res[1] + 3) / 4;
+    a.ngroups = (long long)a.bx * a.by * ((q.res[2] + 1) / 2);
+    DWG_REQUIRE(a.ngroups < (1ll << 32), "gwn: grid too large");
+    return dispatch<true>(a, p, s);
+}
+
+}  // namespace dwg

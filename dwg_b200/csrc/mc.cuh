@@ -1,0 +1,30 @@
+// mc.cuh -- marching cubes on a regular grid (two passes, cell-ordered output).
+#pragma once
+
+#include "common.cuh"
+
+namespace dwg {
+
+struct McGrid {
+    int res[3];
+    float origin[3];
+    float spacing;
+    const float* positions = nullptr;  // optional materialised sample positions
+};
+
+struct McWorkspace {
+    DevBuf<unsigned int> block_counts;
+    DevBuf<unsigned int> block_offsets;
+    DevBuf<unsigned char> scratch;
+};
+
+// generated tables (host copies)
+void mc_tables_host(int* edge_table, signed char* tri_table);
+int mc_upload_tables();
+
+// count -> scan -> emit.  *num_tris_dev receives the full count (may exceed cap).
+int mc_run(const float* field, const McGrid& g, float iso, const float* iso_dev, float* tris,
+           float* centroids, float* normals, long long cap, unsigned long long* num_tris_dev,
+           McWorkspace& ws, cudaStream_t s);
+
+}  // namespace dwg

@@ -1,0 +1,37 @@
+// normals.cuh -- normal initialisation, diffusion and repair kernels.
+#pragma once
+
+#include "common.cuh"
+#include "knn.cuh"
+
+namespace dwg {
+
+int gauss_map(const float* P, int n, float* normals, cudaStream_t s);
+
+// tri -> k nearest points scatter into 2^-40 fixed-point accumulators (acc,
+// 3*L int64, must be zero on entry), then normalise; acc is cleared again on
+// exit.  The triangle count is min(num_tris, *num_tris_dev) when num_tris_dev
+// is given.
+int diffuse_normals(const int* knn, const float* tri_normals, long long num_tris,
+                    const unsigned long long* num_tris_dev, int k, int L, float* normals,
+                    long long* acc, unsigned char* is_zero, int* zero_count, cudaStream_t s);
+
+struct ZeroRepairWs {
+    DevBuf<int> list;
+    DevBuf<int> count;
+    DevBuf<int> nb;
+    DevBuf<unsigned char> scratch;
+};
+int zero_repair(const KnnIndex& ix, const float* positions, int L, float* normals, const unsigned char* is_zero,
+                int k, int min_zero, ZeroRepairWs& ws, cudaStream_t s);
+
+int load_normals(const int* knn, int k, long long nq, const float* leaf_normals, float* out, cudaStream_t s);
+int radii(const float* P, int n, const int* knn, int k, float* out, cudaStream_t s);
+
+// Deterministic FP64 mean of x[0..n) -> *mean_dev (float).  When half_dev is
+// non-null and *half_dev != 0 the value is halved (src/TurboDWG.cu:547-550).
+// iso_hist (nullable) receives the value at index *iter_dev.
+int mean_to_iso(const float* x, long long n, float* mean_dev, const int* half_dev, float* iso_hist,
+                const int* iter_dev, DevBuf<double>& partial, cudaStream_t s);
+
+}  // namespace dwg

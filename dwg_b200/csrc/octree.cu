@@ -1,0 +1,494 @@
+// octree.cu -- GPU build of the octreeDWG topology and its FP64 moments.
+//
+// The reference builds the octree recursively on the CPU
+// (deps/libigl/include/igl/octree.cpp:171-335), precomputes the moments on the
+// CPU (deps/libigl/include/igl/fast_winding_number.cpp:9-120) and flattens the
+// result into pointer-chasing AoS nodes (src/TurboLibiGWN.cu:132-231).  Here:
+//   1. every point gets its octant path as a key, computed in FP64 with the
+//      same centre recursion and `>=` tests as octreeDWG;
+//   2. one stable radix sort groups points by key (the sorted order is the
+//      depth-first order of the leaves);
+//   3. a node exists for every run of equal key prefixes at depth d whose
+//      parent run holds more than one point; runs are found per level from
+//      the longest common prefix of neighbouring keys;
+//   4. nodes are numbered in depth-first pre-order, so each subtree is a
+//      contiguous node range and a contiguous point range.
+#include <cub/cub.cuh>
+
+#include "octree.cuh"
+
+namespace dwg {
+
+// ------------------------------------------------------------ bounding box --
+__global__ void k_bbox_partial(const float* __restrict__ P, long long n, float* __restrict__ part) {
+    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        for (int d = 0; d < 3; d++) {
+            float v = P[i * 3 + d];
+            mn[d] = fminf(mn[d], v);
+            mx[d] = fmaxf(mx[d], v);
+        }
+    }
+    typedef cub::BlockReduce<float, 256> BR;
+    __shared__ typename BR::TempStorage tmp;
+    for (int d = 0; d < 3; d++) {
+        float a = BR(tmp).Reduce(mn[d], cub::Min());
+        __syncthreads();
+        float b = BR(tmp).Reduce(mx[d], cub::Max());
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            part[blockIdx.x * 6 + d] = a;
+            part[blockIdx.x * 6 + 3 + d] = b;
+        }
+    }
+}
+
+__global__ void k_bbox_final(const float* __restrict__ part, int nb, float* __restrict__ out) {
+    typedef cub::BlockReduce<float, 256> BR;
+    __shared__ typename BR::TempStorage tmp;
+    for (int d = 0; d < 6; d++) {
+        float v = (d < 3) ? INFINITY : -INFINITY;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) {
+            float x = part[b * 6 + d];
+            v = (d < 3) ? fminf(v, x) : fmaxf(v, x);
+        }
+        float r = (d < 3) ? BR(tmp).Reduce(v, cub::Min()) : BR(tmp).Reduce(v, cub::Max());
+        __syncthreads();
+        if (threadIdx.x == 0) out[d] = r;
+    }
+}
+
+int bbox_device(const float* points_dev, long long n, float* out_dev, cudaStream_t s) {
+    static thread_local DevBuf<float> part;
+    const int nb = 256;
+    DWG_TRY(part.reserve(nb * 6));
+    k_bbox_partial<<<nb, 256, 0, s>>>(points_dev, n, part.ptr);
+    k_bbox_final<<<1, 256, 0, s>>>(part.ptr, nb, out_dev);
+    DWG_CHECK_LAUNCH();
+    return DWG_OK;
+}
+
+// root cube: AABB centre, width = largest extent, in FP64 (octree.cpp:306-316)
+__global__ void k_root(const float* __restrict__ bb, double* __restrict__ root) {
+    double w = 0;
+    for (int d = 0; d < 3; d++) {
+        double lo = bb[d], hi = bb[3 + d];
+        root[d] = (lo + hi) / 2.0;
+        if (hi - lo > w) w = hi - lo;
+    }
+    root[3] = w;
+}
+
+// ----------------------------------------------------------------- keys --
+// octant path: bit0 x >= cx, bit1 y >= cy, bit2 z >= cz (octree.cpp:200-221);
+// child centre = parent +/- (child width)/2 (octree.cpp:224-249,267-276)
+__global__ void k_keys(const float* __restrict__ P, int n, const double* __restrict__ root, int D,
+                       unsigned long long* __restrict__ keys, int* __restrict__ idx) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double px = P[(size_t)i * 3], py = P[(size_t)i * 3 + 1], pz = P[(size_t)i * 3 + 2];
+    double cx = root[0], cy = root[1], cz = root[2], w = root[3];
+    unsigned long long key = 0;
+    for (int d = 0; d < D; d++) {
+        double h = w / 2.0;
+        double hh = h / 2.0;
+        int o = (px >= cx ? 1 : 0) | (py >= cy ? 2 : 0) | (pz >= cz ? 4 : 0);
+        key = (key << 3) | (unsigned long long)o;
+        cx = cx + ((o & 1) ? hh : -hh);
+        cy = cy + ((o & 2) ? hh : -hh);
+        cz = cz + ((o & 4) ? hh : -hh);
+        w = h;
+    }
+    keys[i] = key;
+    idx[i] = i;
+}
+
+// longest common prefix (in octal digits) with the previous key; -1 at both ends
+__global__ void k_lcp(const unsigned long long* __restrict__ keys, int n, int D,
+                      signed char* __restrict__ lcp) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    int l = -1;
+    if (i > 0 && i < n) {
+        unsigned long long x = keys[i] ^ keys[i - 1];
+        if (x == 0)
+            l = D;
+        else {
+            int b = 63 - __clzll((long long)x);
+            l = D - 1 - b / 3;
+        }
+    }
+    lcp[i] = (signed char)l;
+}
+
+// a point is alone in its depth-d run iff d > max(lcp_i, lcp_{i+1}); it starts
+// the nodes at depths lcp_i+1 .. leafdepth_i
+__global__ void k_node_starts(const signed char* __restrict__ lcp, int n, int D,
+                              int* __restrict__ nstart) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    if (i == n) {
+        nstart[i] = 0;
+        return;
+    }
+    int a = lcp[i], b = lcp[i + 1];
+    int ld = min(D, max(a, b) + 1);
+    nstart[i] = max(0, ld - a);
+}
+
+__global__ void k_level_flags(const signed char* __restrict__ lcp, int n, int d, int* __restrict__ f) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) f[i] = lcp[i] < d ? 1 : 0;
+}
+
+__global__ void k_level_starts(const signed char* __restrict__ lcp, const int* __restrict__ rank, int n,
+                               int d, int* __restrict__ starts) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int f = lcp[i] < d ? 1 : 0;
+    if (f) starts[rank[i]] = i;
+    if (i == n - 1) starts[rank[i] + f] = n;
+}
+
+__global__ void k_level_nodes(const signed char* __restrict__ lcp, const int* __restrict__ rank,
+                              const int* __restrict__ starts, const int* __restrict__ node_base, int n,
+                              int d, int D, int4* __restrict__ info) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int a = lcp[i];
+    if (a >= d) return;
+    int ld = min(D, max(a, (int)lcp[i + 1]) + 1);
+    if (d > ld) return;
+    int node = node_base[i] + (d - a - 1);
+    int cnt = starts[rank[i] + 1] - i;
+    int skip = node_base[i + cnt];
+    int leaf = (cnt == 1 || d == D) ? kLeafFlag : 0;
+    info[node] = make_int4(i, cnt, skip, d | leaf);
+}
+
+__global__ void k_gather(const float* __restrict__ P, const float* __restrict__ A,
+                         const int* __restrict__ perm, int n, float4* __restrict__ pa,
+                         float4* __restrict__ nr, int* __restrict__ inv) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    int i = perm[j];
+    pa[j] = make_float4(P[(size_t)i * 3], P[(size_t)i * 3 + 1], P[(size_t)i * 3 + 2], A ? A[i] : 1.0f);
+    nr[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+    inv[i] = j;
+}
+
+__global__ void k_set_point_data(const float* __restrict__ N, const float* __restrict__ A,
+                                 const float* __restrict__ R, const int* __restrict__ perm, int n,
+                                 float4* __restrict__ pa, float4* __restrict__ nr) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    int i = perm[j];
+    if (A) pa[j].w = A[i];
+    float4 v = nr[j];
+    if (N) {
+        v.x = N[(size_t)i * 3];
+        v.y = N[(size_t)i * 3 + 1];
+        v.z = N[(size_t)i * 3 + 2];
+    }
+    if (R) v.w = R[i];
+    nr[j] = v;
+}
+
+__global__ void k_set_sorted_normals(const float* __restrict__ N, int n, float4* __restrict__ nr) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    float4 v = nr[j];
+    v.x = N[(size_t)j * 3];
+    v.y = N[(size_t)j * 3 + 1];
+    v.z = N[(size_t)j * 3 + 2];
+    nr[j] = v;
+}
+
+// ------------------------------------------------------------- moments --
+// one warp per node; lanes stride the node's contiguous point range and the
+// partial sums meet in a fixed shuffle tree (deterministic)
+__device__ __forceinline__ double warp_sum_d(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_max_d(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__global__ void k_centres(const int4* __restrict__ info, const float4* __restrict__ pa, int M,
+                          double* __restrict__ cm_d, double* __restrict__ r_d,
+                          float4* __restrict__ cmr) {
+    const int lane = threadIdx.x & 31;
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long v = warp; v < M; v += nwarps) {
+        int4 iv = info[v];
+        double sa = 0, sx = 0, sy = 0, sz = 0;
+        for (int j = iv.x + lane; j < iv.x + iv.y; j += 32) {
+            float4 p = pa[j];
+            double a = p.w;
+            sa += a;
+            sx += a * (double)p.x;
+            sy += a * (double)p.y;
+            sz += a * (double)p.z;
+        }
+        sa = warp_sum_d(sa);
+        sx = warp_sum_d(sx);
+        sy = warp_sum_d(sy);
+        sz = warp_sum_d(sz);
+        sa = __shfl_sync(0xffffffffu, sa, 0);
+        sx = __shfl_sync(0xffffffffu, sx, 0);
+        sy = __shfl_sync(0xffffffffu, sy, 0);
+        sz = __shfl_sync(0xffffffffu, sz, 0);
+        double cx = sa > 0 ? sx / sa : 0.0, cy = sa > 0 ? sy / sa : 0.0, cz = sa > 0 ? sz / sa : 0.0;
+        double rm = 0;
+        for (int j = iv.x + lane; j < iv.x + iv.y; j += 32) {
+            float4 p = pa[j];
+            double dx = (double)p.x - cx, dy = (double)p.y - cy, dz = (double)p.z - cz;
+            rm = fmax(rm, sqrt(dx * dx + dy * dy + dz * dz));
+        }
+        rm = warp_max_d(rm);
+        if (lane == 0) {
+            cm_d[v * 3] = cx;
+            cm_d[v * 3 + 1] = cy;
+            cm_d[v * 3 + 2] = cz;
+            r_d[v] = rm;
+            cmr[v] = make_float4((float)cx, (float)cy, (float)cz, (float)rm);
+        }
+    }
+}
+
+__global__ void k_ec(const int4* __restrict__ info, const float4* __restrict__ pa,
+                     const float4* __restrict__ nr, int M, double* __restrict__ ec_d,
+                     float4* __restrict__ ec) {
+    const int lane = threadIdx.x & 31;
+    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long v = warp; v < M; v += nwarps) {
+        int4 iv = info[v];
+        double ex = 0, ey = 0, ez = 0;
+        if (iv.y <= 32) {
+            if (lane < iv.y) {
+                float4 p = pa[iv.x + lane];
+                float4 q = nr[iv.x + lane];
+                double a = p.w;
+                ex = a * (double)q.x;
+                ey = a * (double)q.y;
+                ez = a * (double)q.z;
+            }
+        } else {
+            for (int j = iv.x + lane; j < iv.x + iv.y; j += 32) {
+                float a = pa[j].w;
+                float4 q = nr[j];
+                ex += (double)a * (double)q.x;
+                ey += (double)a * (double)q.y;
+                ez += (double)a * (double)q.z;
+            }
+        }
+        ex = warp_sum_d(ex);
+        ey = warp_sum_d(ey);
+        ez = warp_sum_d(ez);
+        if (lane == 0) {
+            ec_d[v * 3] = ex;
+            ec_d[v * 3 + 1] = ey;
+            ec_d[v * 3 + 2] = ez;
+            ec[v] = make_float4((float)ex, (float)ey, (float)ez, 0.f);
+        }
+    }
+}
+
+// ---------------------------------------------------------- leaf centres --
+__global__ void k_leaf_flags(const int4* __restrict__ info, int M, int min_count, int* __restrict__ f) {
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= M) return;
+    int4 iv = info[v];
+    f[v] = ((iv.w & kLeafFlag) && iv.y > min_count) ? 1 : 0;
+}
+
+// cell centre of a node, by the same FP64 recursion as the keys
+__global__ void k_leaf_centres(const int4* __restrict__ info, const int* __restrict__ f,
+                               const int* __restrict__ rank, int M,
+                               const unsigned long long* __restrict__ keys,
+                               const double* __restrict__ root, int D, float* __restrict__ out,
+                               int* __restrict__ out_node) {
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= M || !f[v]) return;
+    int4 iv = info[v];
+    int depth = iv.w & 0xff;
+    unsigned long long key = keys[iv.x];
+    double cx = root[0], cy = root[1], cz = root[2], w = root[3];
+    for (int d = 0; d < depth; d++) {
+        int o = (int)((key >> (3 * (D - 1 - d))) & 7ull);
+        double h = w / 2.0;
+        double hh = h / 2.0;
+        cx = cx + ((o & 1) ? hh : -hh);
+        cy = cy + ((o & 2) ? hh : -hh);
+        cz = cz + ((o & 4) ? hh : -hh);
+        w = h;
+    }
+    int r = rank[v];
+    out[(size_t)r * 3] = (float)cx;
+    out[(size_t)r * 3 + 1] = (float)cy;
+    out[(size_t)r * 3 + 2] = (float)cz;
+    out_node[r] = v;
+}
+
+// ------------------------------------------------------------- host side --
+template <typename F>
+static int cub_call(DevBuf<unsigned char>& scratch, F&& f) {
+    size_t bytes = 0;
+    cudaError_t e = f((void*)nullptr, bytes);
+    if (e != cudaSuccess) {
+        set_error("cub size query failed: %s", cudaGetErrorString(e));
+        return DWG_ERR_CUDA;
+    }
+    DWG_TRY(scratch.reserve(bytes + 256));
+    size_t have = scratch.n;
+    e = f((void*)scratch.ptr, have);
+    if (e != cudaSuccess) {
+        set_error("cub call failed: %s", cudaGetErrorString(e));
+        return DWG_ERR_CUDA;
+    }
+    return DWG_OK;
+}
+
+int octree_build(Octree& t, const float* P, int n, int D, const float* A, cudaStream_t s) {
+    DWG_REQUIRE(n >= 1, "octree: need at least one point (n=%d)", n);
+    DWG_REQUIRE(D >= 1 && D <= kMaxDepth, "octree: max_depth must be in [1, %d] (got %d)", kMaxDepth, D);
+    t.n = n;
+    t.max_depth = D;
+    DevBuf<float> bb;
+    DWG_TRY(bb.reserve(6));
+    DWG_TRY(bbox_device(P, n, bb.ptr, s));
+    DWG_TRY(t.root_dev.reserve(4));
+    k_root<<<1, 1, 0, s>>>(bb.ptr, t.root_dev.ptr);
+    DevBuf<unsigned long long> keys_in;
+    DevBuf<int> idx_in;
+    DWG_TRY(keys_in.reserve(n));
+    DWG_TRY(idx_in.reserve(n));
+    DWG_TRY(t.keys.reserve(n));
+    DWG_TRY(t.perm.reserve(n));
+    DWG_TRY(t.inv_perm.reserve(n));
+    k_keys<<<div_up(n, 256), 256, 0, s>>>(P, n, t.root_dev.ptr, D, keys_in.ptr, idx_in.ptr);
+    DWG_CHECK_LAUNCH();
+    unsigned long long* kin = keys_in.ptr;
+    unsigned long long* kout = t.keys.ptr;
+    int* vin = idx_in.ptr;
+    int* vout = t.perm.ptr;
+    DWG_TRY(cub_call(t.scratch, [&](void* tmp, size_t& bytes) {
+        return cub::DeviceRadixSort::SortPairs(tmp, bytes, kin, kout, vin, vout, n, 0, 3 * D, s);
+    }));
+    DevBuf<signed char> lcp;
+    DevBuf<int> nstart, node_base;
+    DWG_TRY(lcp.reserve(n + 1));
+    DWG_TRY(nstart.reserve(n + 1));
+    DWG_TRY(node_base.reserve(n + 1));
+    k_lcp<<<div_up(n + 1, 256), 256, 0, s>>>(t.keys.ptr, n, D, lcp.ptr);
+    k_node_starts<<<div_up(n + 1, 256), 256, 0, s>>>(lcp.ptr, n, D, nstart.ptr);
+    DWG_CHECK_LAUNCH();
+    int* ns = nstart.ptr;
+    int* nb = node_base.ptr;
+    DWG_TRY(cub_call(t.scratch, [&](void* tmp, size_t& bytes) {
+        return cub::DeviceScan::ExclusiveSum(tmp, bytes, ns, nb, n + 1, s);
+    }));
+    int M = 0;
+    DWG_CHECK_CUDA(cudaMemcpyAsync(&M, node_base.ptr + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+    DWG_CHECK_CUDA(cudaMemcpyAsync(t.root, t.root_dev.ptr, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    DWG_CHECK_CUDA(cudaStreamSynchronize(s));
+    t.M = M;
+    DWG_TRY(t.info.reserve(M));
+    DevBuf<int> flags, rank, starts;
+    DWG_TRY(flags.reserve(n));
+    DWG_TRY(rank.reserve(n));
+    DWG_TRY(starts.reserve(n + 1));
+    for (int d = 0; d <= D; d++) {
+        k_level_flags<<<div_up(n, 256), 256, 0, s>>>(lcp.ptr, n, d, flags.ptr);
+        int* fp = flags.ptr;
+        int* rp = rank.ptr;
+        DWG_TRY(cub_call(t.scratch, [&](void* tmp, size_t& bytes) {
+            return cub::DeviceScan::ExclusiveSum(tmp, bytes, fp, rp, n, s);
+        }));
+        k_level_starts<<<div_up(n, 256), 256, 0, s>>>(lcp.ptr, rank.ptr, n, d, starts.ptr);
+        k_level_nodes<<<div_up(n, 256), 256, 0, s>>>(lcp.ptr, rank.ptr, starts.ptr, node_base.ptr, n, d, D,
+                                                      t.info.ptr);
+        DWG_CHECK_LAUNCH();
+    }
+    DWG_TRY(t.pa.reserve(n));
+    DWG_TRY(t.nr.reserve(n));
+    k_gather<<<div_up(n, 256), 256, 0, s>>>(P, A, t.perm.ptr, n, t.pa.ptr, t.nr.ptr, t.inv_perm.ptr);
+    DWG_CHECK_LAUNCH();
+    DWG_TRY(t.cmr.reserve(M));
+    DWG_TRY(t.ec.reserve(M));
+    DWG_TRY(t.cm_d.reserve((size_t)M * 3));
+    DWG_TRY(t.r_d.reserve(M));
+    DWG_TRY(t.ec_d.reserve((size_t)M * 3));
+    DWG_TRY(t.work.reserve(2));
+    DWG_CHECK_CUDA(cudaMemsetAsync(t.work.ptr, 0, 2 * sizeof(unsigned int), s));
+    DWG_CHECK_CUDA(cudaMemsetAsync(t.ec.ptr, 0, sizeof(float4) * M, s));
+    DWG_CHECK_CUDA(cudaMemsetAsync(t.ec_d.ptr, 0, sizeof(double) * 3 * M, s));
+    DWG_TRY(octree_update_centres(t, s));
+    return DWG_OK;
+}
+
+int octree_set_point_data(Octree& t, const float* N, const float* A, const float* R, cudaStream_t s) {
+    if (!N && !A && !R) return DWG_OK;
+    k_set_point_data<<<div_up(t.n, 256), 256, 0, s>>>(N, A, R, t.perm.ptr, t.n, t.pa.ptr, t.nr.ptr);
+    DWG_CHECK_LAUNCH();
+    return DWG_OK;
+}
+
+int octree_set_sorted_normals(Octree& t, const float* N, cudaStream_t s) {
+    k_set_sorted_normals<<<div_up(t.n, 256), 256, 0, s>>>(N, t.n, t.nr.ptr);
+    DWG_CHECK_LAUNCH();
+    return DWG_OK;
+}
+
+static unsigned moment_blocks(int M) {
+    long long warps = M;
+    long long blocks = (warps * 32 + 255) / 256;
+    long long cap = (long long)num_sms() * 16;
+    return (unsigned)(blocks < cap ? (blocks > 0 ? blocks : 1) : cap);
+}
+
+int octree_update_centres(Octree& t, cudaStream_t s) {
+    k_centres<<<moment_blocks(t.M), 256, 0, s>>>(t.info.ptr, t.pa.ptr, t.M, t.cm_d.ptr, t.r_d.ptr, t.cmr.ptr);
+    DWG_CHECK_LAUNCH();
+    return DWG_OK;
+}
+
+int octree_update_normals(Octree& t, cudaStream_t s) {
+    k_ec<<<moment_blocks(t.M), 256, 0, s>>>(t.info.ptr, t.pa.ptr, t.nr.ptr, t.M, t.ec_d.ptr, t.ec.ptr);
+    DWG_CHECK_LAUNCH();
+    return DWG_OK;
+}
+
+int octree_leaf_centres(Octree& t, int min_count, DevBuf<float>& out_xyz, DevBuf<int>& out_node,
+                        int* num_leaves, cudaStream_t s) {
+    DevBuf<int> f, rank;
+    DWG_TRY(f.reserve(t.M));
+    DWG_TRY(rank.reserve(t.M));
+    k_leaf_flags<<<div_up(t.M, 256), 256, 0, s>>>(t.info.ptr, t.M, min_count, f.ptr);
+    int* fp = f.ptr;
+    int* rp = rank.ptr;
+    int M = t.M;
+    DWG_TRY(cub_call(t.scratch, [&](void* tmp, size_t& bytes) {
+        return cub::DeviceScan::ExclusiveSum(tmp, bytes, fp, rp, M, s);
+    }));
+    int last_rank = 0, last_flag = 0;
+    DWG_CHECK_CUDA(cudaMemcpyAsync(&last_rank, rank.ptr + M - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+    DWG_CHECK_CUDA(cudaMemcpyAsync(&last_flag, f.ptr + M - 1, sizeof(int), cudaMemcpyDeviceToHost, s));
+    DWG_CHECK_CUDA(cudaStreamSynchronize(s));
+    int L = last_rank + last_flag;
+    *num_leaves = L;
+    DWG_TRY(out_xyz.reserve((size_t)(L ? L : 1) * 3));
+    DWG_TRY(out_node.reserve(L ? L : 1));
+    k_leaf_centres<<<div_up(M, 256), 256, 0, s>>>(t.info.ptr, f.ptr, rank.ptr, M, t.keys.ptr, t.root_dev.ptr,
+                                                  t.max_depth, out_xyz.ptr, out_node.ptr);
+    DWG_CHECK_LAUNCH();
+    DWG_CHECK_CUDA(cudaStreamSynchronize(s));
+    return DWG_OK;
+}
+
+}  // namespace dwg

@@ -1,0 +1,61 @@
+// octree.cuh -- GPU octree with the topology of igl::octreeDWG
+// (deps/libigl/include/igl/octree.cpp:171-335).
+//
+// Layout in HBM (structure of arrays):
+//   points, sorted by their octant path (a 3*max_depth-bit key, stable):
+//     pa[i] = (x, y, z, area)  float4      nr[i] = (nx, ny, nz, radius) float4
+//     perm[i] = input index of sorted point i
+//   nodes, depth-first pre-order (a node's subtree is contiguous and its first
+//   child, if any, is the next node):
+//     info[v] = (pt_start, pt_count, skip, depth | LEAF)   int4
+//     cmr[v]  = (cm.x, cm.y, cm.z, R)                    float4 (rounded FP64)
+//     ec[v]   = (sum A n .x, .y, .z, 0)                  float4 (rounded FP64)
+//   skip[v] = index of the first node after v's subtree, so the children of v
+//   are v+1, skip[v+1], skip[skip[v+1]], ... while < skip[v].
+// Empty octants are not stored (the reference skips them at
+// src/TurboLibiGWN.cu:630).
+#pragma once
+
+#include "common.cuh"
+
+namespace dwg {
+
+constexpr int kLeafFlag = 1 << 8;
+constexpr int kMaxDepth = 21;
+
+struct Octree {
+    int n = 0;
+    int max_depth = 0;
+    int M = 0;
+    double root[4] = {0, 0, 0, 0};  // centre xyz, width (host copy)
+    DevBuf<double> root_dev;        // same on the device
+    DevBuf<unsigned long long> keys;  // sorted keys
+    DevBuf<int> perm;                 // sorted -> input
+    DevBuf<int> inv_perm;             // input -> sorted
+    DevBuf<float4> pa, nr;
+    DevBuf<int4> info;
+    DevBuf<float4> cmr, ec;
+    DevBuf<double> cm_d, r_d, ec_d;
+    DevBuf<unsigned char> scratch;  // CUB temporary storage
+    mutable DevBuf<unsigned int> work;  // [0] work counter of the persistent GWN kernel, [1] error flag
+};
+
+int octree_build(Octree& t, const float* points_dev, int n, int max_depth, const float* areas_dev,
+                 cudaStream_t s);
+// gather per-point arrays (input order) into sorted order; any may be null
+int octree_set_point_data(Octree& t, const float* normals_dev, const float* areas_dev,
+                          const float* radii_dev, cudaStream_t s);
+// the same from arrays already in sorted order (internal pipeline use)
+int octree_set_sorted_normals(Octree& t, const float* normals_sorted_dev, cudaStream_t s);
+// FP64 moments: sum A p / sum A, max |p - CM|, from pa (positions, areas)
+int octree_update_centres(Octree& t, cudaStream_t s);
+// FP64 sum A n from pa.w and nr.xyz
+int octree_update_normals(Octree& t, cudaStream_t s);
+// node centre of every node at the octreeDWG recursion (FP64), for leaf extraction
+int octree_leaf_centres(Octree& t, int min_count, DevBuf<float>& out_xyz, DevBuf<int>& out_node,
+                        int* num_leaves, cudaStream_t s);
+
+// bounding box of float3 points: out[0..2] = min, out[3..5] = max (device)
+int bbox_device(const float* points_dev, long long n, float* out_dev, cudaStream_t s);
+
+}  // namespace dwg

@@ -1,0 +1,566 @@
+// pipeline.cu -- DWG reconstruction on one GPU, every step on the device.
+//
+// Reference flow (include/DWGProcess.h:99-262,474-797; src/TurboDWG.cu:456-924):
+// CPU octree on the points, octree-leaf cell centres as the iteration's point
+// set, CPU moment precompute, then per iteration: mass-normal update,
+// screened GWN at the leaves and at the grid, mean iso value, marching cubes,
+// kNN of the triangle centroids, normal scatter / normalise, zero-normal
+// repair; finally a pass over all points at the final resolution.
+//
+// Here both octrees, their moments, the grids and the kNN structure are built
+// on the GPU once; one iteration is a fixed sequence of fixed-size launches
+// whose varying values (sigma, iso halving, triangle count, zero count) live
+// in device memory, so it can be captured once as a CUDA graph and replayed.
+#include <cub/cub.cuh>
+
+#include <cmath>
+#include <vector>
+
+#include "pipeline.cuh"
+
+namespace dwg {
+
+// Closed form of igl::voxel_grid(V, offset, s, 1) (deps/libigl/include/igl/voxel_grid.cpp:11-87)
+// in single precision; samples at origin + index * spacing.
+int voxel_grid_host(const float* P, int n, float offset, int s_res, cudaStream_t st, int res[3], float origin[3],
+                    float* spacing) {
+    DWG_REQUIRE(P && n >= 1, "voxel_grid: need points");
+    DWG_REQUIRE(s_res >= 4, "voxel_grid: resolution must be >= 4 (got %d)", s_res);
+    DevBuf<float> bb;
+    DWG_TRY(bb.reserve(6));
+    DWG_TRY(bbox_device(P, n, bb.ptr, st));
+    float b[6];
+    DWG_CHECK_CUDA(cudaMemcpyAsync(b, bb.ptr, sizeof(b), cudaMemcpyDeviceToHost, st));
+    DWG_CHECK_CUDA(cudaStreamSynchronize(st));
+    volatile float mn[3], mx[3], diag[3];
+    for (int d = 0; d < 3; ++d) {
+        mn[d] = b[d] - offset;
+        mx[d] = b[3 + d] + offset;
+        diag[d] = mx[d] - mn[d];
+    }
+    int si = 0;
+    for (int d = 1; d < 3; ++d)
+        if (diag[d] > diag[si]) si = d;
+    const float s_len = diag[si];
+    const float sf = (float)(s_res - 2);
+    for (int d = 0; d < 3; ++d) {
+        if (d == si) {
+            res[d] = s_res - 2;
+        } else {
+            volatile float v = sf * diag[d];
+            v = v / s_len;
+            res[d] = (int)std::ceil((float)v);
+        }
+        res[d] += 2;
+    }
+    volatile float Aa[3];
+    for (int d = 0; d < 3; ++d) {
+        volatile float ps = 1.0f / ((float)res[d] - 1.0f);
+        volatile float den = 1.0f - 2.0f * ps;
+        Aa[d] = diag[d] / den;
+    }
+    int ai = 0;
+    for (int d = 1; d < 3; ++d)
+        if (Aa[d] > Aa[ai]) ai = d;
+    volatile float h = Aa[ai] / ((float)res[ai] - 1.0f);
+    for (int d = 0; d < 3; ++d) {
+        volatile float c = (mn[d] + mx[d]) / 2.0f;
+        volatile float half = 0.5f * ((float)res[d] - 1.0f);
+        volatile float ext = half * h;
+        origin[d] = c - ext;
+    }
+    *spacing = h;
+    return DWG_OK;
+}
+
+// ---------------------------------------------------------------- kernels --
+__global__ void k_gather_xyz(const float* __restrict__ src, const int* __restrict__ perm, int n,
+                             float* __restrict__ dst) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    int i = perm[j];
+    dst[(size_t)j * 3] = src[(size_t)i * 3];
+    dst[(size_t)j * 3 + 1] = src[(size_t)i * 3 + 1];
+    dst[(size_t)j * 3 + 2] = src[(size_t)i * 3 + 2];
+}
+
+__global__ void k_fill(float* __restrict__ x, long long n, float v) {
+    long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) x[i] = v;
+}
+
+__global__ void k_sorted_xyz(const float4* __restrict__ pa, int n, float* __restrict__ out) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    float4 p = pa[j];
+    out[(size_t)j * 3] = p.x;
+    out[(size_t)j * 3 + 1] = p.y;
+    out[(size_t)j * 3 + 2] = p.z;
+}
+
+__global__ void k_set_nr(float4* __restrict__ nr, const float* __restrict__ N, const float* __restrict__ R, int n) {
+    int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    float4 v = nr[j];
+    if (N) {
+        v.x = N[(size_t)j * 3];
+        v.y = N[(size_t)j * 3 + 1];
+        v.z = N[(size_t)j * 3 + 2];
+    }
+    if (R) v.w = R[j];
+    nr[j] = v;
+}
+
+// SmoothNormalstoOctreeLeaves (include/DWGProcess.h:430-472): per leaf cell,
+// per component sum_j exp(-((p_jk - c_k)/W)^2 / 4) n_jk, FP64
+__global__ void k_smooth_leaves(const int4* __restrict__ info, const int* __restrict__ leaf_node, int L,
+                                const unsigned long long* __restrict__ keys, const double* __restrict__ root, int D,
+                                const float4* __restrict__ pa, const float4* __restrict__ nr,
+                                double* __restrict__ out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= L) return;
+    int4 iv = info[leaf_node[i]];
+    int depth = iv.w & 0xff;
+    unsigned long long key = keys[iv.x];
+    double c[3] = {root[0], root[1], root[2]}, w = root[3];
+    for (int d = 0; d < depth; ++d) {
+        int o = (int)((key >> (3 * (D - 1 - d))) & 7ull);
+        double h = w / 2.0, hh = h / 2.0;
+        c[0] += (o & 1) ? hh : -hh;
+        c[1] += (o & 2) ? hh : -hh;
+        c[2] += (o & 4) ? hh : -hh;
+        w = h;
+    }
+    double acc[3] = {0, 0, 0};
+    for (int j = iv.x; j < iv.x + iv.y; ++j) {
+        float4 p = pa[j];
+        float4 q = nr[j];
+        const double pv[3] = {p.x, p.y, p.z}, nv[3] = {q.x, q.y, q.z};
+        for (int k = 0; k < 3; ++k) {
+            double x = (pv[k] - c[k]) / w;
+            acc[k] += exp(-(x * x) / 4.0) * nv[k];
+        }
+    }
+    for (int k = 0; k < 3; ++k) out[(size_t)i * 3 + k] = acc[k];
+}
+
+__global__ void k_sumsq(const double* __restrict__ x, long long n, double* __restrict__ part) {
+    long long chunk = (n + 255) / 256;
+    long long b0 = blockIdx.x * chunk, b1 = b0 + chunk < n ? b0 + chunk : n;
+    double acc = 0;
+    for (long long i = b0 + threadIdx.x; i < b1; i += blockDim.x) acc += x[i] * x[i];
+    typedef cub::BlockReduce<double, 256> BR;
+    __shared__ typename BR::TempStorage tmp;
+    double t = BR(tmp).Sum(acc);
+    if (threadIdx.x == 0) part[blockIdx.x] = t;
+}
+
+// Eigen's normalized() over the whole L x 3 matrix (include/DWGProcess.h:537)
+__global__ void k_frobenius_apply(const double* __restrict__ part, const double* __restrict__ x, long long n,
+                                  const int* __restrict__ perm, float* __restrict__ out) {
+    __shared__ double norm;
+    if (threadIdx.x == 0) {
+        double t = 0;
+        for (int b = 0; b < 256; ++b) t += part[b];
+        norm = sqrt(t);
+    }
+    __syncthreads();
+    long long L = n / 3;
+    for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < L; j += (long long)gridDim.x * blockDim.x) {
+        long long i = perm[j];
+        for (int k = 0; k < 3; ++k) {
+            double v = x[i * 3 + k];
+            out[j * 3 + k] = (float)(norm > 0 ? v / norm : v);
+        }
+    }
+}
+
+// sigma schedule and iso halving (src/TurboDWG.cu:526-550), per iteration
+__global__ void k_iter_begin(const int* __restrict__ iter, const float* __restrict__ sigma_tab,
+                             const int* __restrict__ half_tab, float* __restrict__ cur_sigma,
+                             int* __restrict__ cur_half, unsigned long long* __restrict__ terms) {
+    int t = *iter;
+    *cur_sigma = sigma_tab[t];
+    *cur_half = half_tab[t];
+    *terms = 0;
+}
+
+__global__ void k_iter_end(int* __restrict__ iter, const unsigned long long* __restrict__ ntri, long long cap,
+                           const int* __restrict__ zc, const unsigned long long* __restrict__ terms,
+                           long long* __restrict__ tri_hist, int* __restrict__ zero_hist,
+                           unsigned long long* __restrict__ terms_hist) {
+    int t = *iter;
+    unsigned long long T = *ntri;
+    tri_hist[t] = (long long)T;
+    zero_hist[t] = *zc;
+    terms_hist[t] = *terms;
+    *iter = t + 1;
+}
+
+// ------------------------------------------------------------------ setup --
+Pipeline::~Pipeline() {
+    if (s) cudaStreamSynchronize(s);
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (ev) cudaEventDestroy(ev);
+    if (s) cudaStreamDestroy(s);
+}
+
+int Pipeline::join_in() {
+    DWG_CHECK_CUDA(cudaEventRecord(ev, caller));
+    DWG_CHECK_CUDA(cudaStreamWaitEvent(s, ev, 0));
+    return DWG_OK;
+}
+
+int Pipeline::join_out() {
+    DWG_CHECK_CUDA(cudaEventRecord(ev, s));
+    DWG_CHECK_CUDA(cudaStreamWaitEvent(caller, ev, 0));
+    return DWG_OK;
+}
+
+static float sigma_at(int t, float lambda) {
+    float s = lambda;
+    if (t < 4) s = 20.0f;
+    if (t > 0 && t % 7 == 0) s = 10.0f;
+    return s;
+}
+
+int Pipeline::ensure_hist(int total) {
+    if (total <= hist_cap) return DWG_OK;
+    int cap2 = total + 16;
+    std::vector<float> st(cap2);
+    std::vector<int> ht(cap2);
+    for (int t = 0; t < cap2; ++t) {
+        st[t] = sigma_at(t, prm.lambda);
+        ht[t] = (t % 5 == 0 && t != 0) ? 1 : 0;
+    }
+    // keep the history already recorded
+    std::vector<float> ih(hist_cap);
+    std::vector<long long> th(hist_cap);
+    std::vector<int> zh(hist_cap);
+    std::vector<unsigned long long> mh(hist_cap);
+    if (hist_cap) {
+        DWG_CHECK_CUDA(cudaMemcpyAsync(ih.data(), iso_hist.ptr, sizeof(float) * hist_cap, cudaMemcpyDeviceToHost, s));
+        DWG_CHECK_CUDA(cudaMemcpyAsync(th.data(), tri_hist.ptr, sizeof(long long) * hist_cap, cudaMemcpyDeviceToHost, s));
+        DWG_CHECK_CUDA(cudaMemcpyAsync(zh.data(), zero_hist.ptr, sizeof(int) * hist_cap, cudaMemcpyDeviceToHost, s));
+        DWG_CHECK_CUDA(cudaMemcpyAsync(mh.data(), terms_hist.ptr, sizeof(unsigned long long) * hist_cap,
+                                       cudaMemcpyDeviceToHost, s));
+        DWG_CHECK_CUDA(cudaStreamSynchronize(s));
+    }
+    // the captured graph holds the old table pointers
+    if (graph_exec) {
+        cudaGraphExecDestroy(graph_exec);
+        graph_exec = nullptr;
+    }
+    if (graph) {
+        cudaGraphDestroy(graph);
+        graph = nullptr;
+    }
+    DWG_TRY(sigma_tab.reserve(cap2));
+    DWG_TRY(half_tab.reserve(cap2));
+    DWG_TRY(iso_hist.reserve(cap2));
+    DWG_TRY(tri_hist.reserve(cap2));
+    DWG_TRY(zero_hist.reserve(cap2));
+    DWG_TRY(terms_hist.reserve(cap2));
+    DWG_CHECK_CUDA(cudaMemcpyAsync(sigma_tab.ptr, st.data(), sizeof(float) * cap2, cudaMemcpyHostToDevice, s));
+    DWG_CHECK_CUDA(cudaMemcpyAsync(half_tab.ptr, ht.data(), sizeof(int) * cap2, cudaMemcpyHostToDevice, s));
+    DWG_CHECK_CUDA(cudaMemsetAsync(iso_hist.ptr, 0, sizeof(float) * cap2, s));
+    DWG_CHECK_CUDA(cudaMemsetAsync(tri_hist.ptr, 0, sizeof(long long) * cap2, s));
+    DWG_CHECK_CUDA(cudaMemsetAsync(zero_hist.ptr, 0, sizeof(int) * cap2, s));
+    DWG_CHECK_CUDA(cudaMemsetAsync(terms_hist.ptr, 0, sizeof(unsigned long long) * cap2, s));
+    if (hist_cap) {
+        DWG_CHECK_CUDA(cudaMemcpyAsync(iso_hist.ptr, ih.data(), sizeof(float) * hist_cap, cudaMemcpyHostToDevice, s));
+        DWG_CHECK_CUDA(cudaMemcpyAsync(tri_hist.ptr, th.data(), sizeof(long long) * hist_cap, cudaMemcpyHostToDevice, s));
+        DWG_CHECK_CUDA(cudaMemcpyAsync(zero_hist.ptr, zh.data(), sizeof(int) * hist_cap, cudaMemcpyHostToDevice, s));
+        DWG_CHECK_CUDA(cudaMemcpyAsync(terms_hist.ptr, mh.data(), sizeof(unsigned long long) * hist_cap,
+                                       cudaMemcpyHostToDevice, s));
+    }
+    DWG_CHECK_CUDA(cudaStreamSynchronize(s));
+    hist_cap = cap2;
+    return DWG_OK;
+}
+
+int Pipeline::setup(const float* points_dev, const float* normals_dev, int n_points, const dwg_params& p,
+                    cudaStream_t stream) {
+    DWG_REQUIRE(points_dev && n_points >= 2, "pipeline: need at least 2 points (n=%d)", n_points);
+    DWG_REQUIRE(p.max_depth >= 1 && p.max_depth <= kMaxDepth, "pipeline: max_depth must be in [1, %d]", kMaxDepth);
+    DWG_REQUIRE(p.grid_reso >= 4 && p.final_reso >= 4, "pipeline: grid resolutions must be >= 4");
+    DWG_REQUIRE(p.knn_tri >= 1 && p.knn_tri <= 64 && p.knn_zero >= 1 && p.knn_zero <= 64 && p.kw >= 1 &&
+                    p.kw <= 64 && p.final_kw >= 1 && p.final_kw <= 64 && p.normal_kw >= 1 && p.normal_kw <= 64,
+                "pipeline: k values must be in [1, 64]");
+    DWG_REQUIRE(p.in_normal == 0 || p.in_normal == 1 || p.in_normal == 3, "pipeline: in_normal must be 0, 1 or 3");
+    DWG_REQUIRE(p.in_normal == 3 || normals_dev, "pipeline: in_normal %d needs input normals", p.in_normal);
+    prm = p;
+    caller = stream;
+    DWG_CHECK_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    DWG_CHECK_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    DWG_TRY(join_in());
+    n = n_points;
+    DWG_TRY(mc_upload_tables());
+    DWG_TRY(P.reserve((size_t)n * 3));
+    DWG_CHECK_CUDA(cudaMemcpyAsync(P.ptr, points_dev, sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s));
+    DWG_TRY(area_pts.reserve(n));
+    k_fill<<<div_up(n, 256), 256, 0, s>>>(area_pts.ptr, n, p.area);
+    DWG_CHECK_LAUNCH();
+    if (normals_dev) {
+        DWG_TRY(Nin.reserve((size_t)n * 3));
+        DWG_CHECK_CUDA(cudaMemcpyAsync(Nin.ptr, normals_dev, sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s));
+    }
+    // octree on the points (include/DWGProcess.h:227)
+    DWG_TRY(octree_build(t1, P.ptr, n, p.max_depth, area_pts.ptr, s));
+    // leaf cell centres with more than min_num points (GetOctreeLeaves, :383-428)
+    DevBuf<float> raw_pos;
+    DevBuf<int> raw_node;
+    DWG_TRY(octree_leaf_centres(t1, p.min_num, raw_pos, raw_node, &L, s));
+    DWG_REQUIRE(L >= 2, "pipeline: fewer than 2 octree leaves (%d)", L);
+    // octree on the leaves; its sorted order is the canonical leaf order
+    DWG_TRY(leaf_area.reserve(L));
+    k_fill<<<div_up(L, 256), 256, 0, s>>>(leaf_area.ptr, L, p.area);
+    DevBuf<float> raw_area;
+    DWG_TRY(raw_area.reserve(L));
+    k_fill<<<div_up(L, 256), 256, 0, s>>>(raw_area.ptr, L, p.area);
+    DWG_TRY(octree_build(t2, raw_pos.ptr, L, p.max_depth, raw_area.ptr, s));
+    DWG_TRY(leaf_pos.reserve((size_t)L * 3));
+    DWG_TRY(leaf_nrm.reserve((size_t)L * 3));
+    DWG_TRY(leaf_rad.reserve(L));
+    k_gather_xyz<<<div_up(L, 256), 256, 0, s>>>(raw_pos.ptr, t2.perm.ptr, L, leaf_pos.ptr);
+    k_fill<<<div_up(L, 256), 256, 0, s>>>(leaf_rad.ptr, L, p.screen);
+    DWG_CHECK_LAUNCH();
+    if (p.in_normal != 3) {
+        DWG_TRY(octree_set_point_data(t1, Nin.ptr, nullptr, nullptr, s));
+        DevBuf<double> sm, part;
+        DWG_TRY(sm.reserve((size_t)L * 3));
+        DWG_TRY(part.reserve(256));
+        k_smooth_leaves<<<div_up(L, 128), 128, 0, s>>>(t1.info.ptr, raw_node.ptr, L, t1.keys.ptr, t1.root_dev.ptr,
+                                                       t1.max_depth, t1.pa.ptr, t1.nr.ptr, sm.ptr);
+        k_sumsq<<<256, 256, 0, s>>>(sm.ptr, (long long)L * 3, part.ptr);
+        k_frobenius_apply<<<div_up(L, 256), 256, 0, s>>>(part.ptr, sm.ptr, (long long)L * 3, t2.perm.ptr,
+                                                         leaf_nrm.ptr);
+        DWG_CHECK_LAUNCH();
+        DWG_CHECK_CUDA(cudaStreamSynchronize(s));
+    }
+    // kNN structure over the leaves, radii (GetRadiiandAs, include/DWGProcess.h:283-343)
+    DWG_TRY(knn_build(kidx, leaf_pos.ptr, L, s));
+    if (p.use_radii) {
+        DevBuf<int> nb;
+        DWG_TRY(nb.reserve((size_t)L * p.kw));
+        KnnQuery q;
+        q.q = leaf_pos.ptr;
+        q.nq = L;
+        DWG_TRY(knn_query(kidx, q, p.kw, nb.ptr, s));
+        DWG_TRY(radii(leaf_pos.ptr, L, nb.ptr, p.kw, leaf_rad.ptr, s));
+        DWG_CHECK_CUDA(cudaStreamSynchronize(s));
+    }
+    // iteration grid around the points (include/DWGProcess.h:672)
+    DWG_TRY(voxel_grid_host(P.ptr, n, p.offset_1, p.grid_reso, s, gres, gorg, &gh));
+    if (p.in_normal == 3) DWG_TRY(gauss_map(leaf_pos.ptr, L, leaf_nrm.ptr, s));
+    k_set_nr<<<div_up(L, 256), 256, 0, s>>>(t2.nr.ptr, leaf_nrm.ptr, leaf_rad.ptr, L);
+    DWG_CHECK_LAUNCH();
+    // buffers of one iteration
+    long long ng = (long long)gres[0] * gres[1] * gres[2];
+    cap = ng / 2 > 1000000 ? ng / 2 : 1000000;  // src/TurboDWG.cu:466
+    DWG_TRY(field.reserve(ng));
+    DWG_TRY(wleaf.reserve(L));
+    DWG_TRY(cent.reserve((size_t)cap * 3));
+    DWG_TRY(tnrm.reserve((size_t)cap * 3));
+    DWG_TRY(ntri.reserve(1));
+    DWG_TRY(knn_buf.reserve((size_t)cap * p.knn_tri));
+    DWG_TRY(acc.reserve((size_t)L * 3));
+    DWG_CHECK_CUDA(cudaMemsetAsync(acc.ptr, 0, sizeof(long long) * 3 * L, s));
+    DWG_TRY(is_zero.reserve(L));
+    DWG_TRY(zero_count.reserve(1));
+    DWG_CHECK_CUDA(cudaMemsetAsync(zero_count.ptr, 0, sizeof(int), s));
+    DWG_TRY(iter_dev.reserve(1));
+    DWG_TRY(cur_half.reserve(1));
+    DWG_TRY(cur_sigma.reserve(1));
+    DWG_TRY(iso_dev.reserve(1));
+    DWG_TRY(terms_cur.reserve(1));
+    DWG_CHECK_CUDA(cudaMemsetAsync(iter_dev.ptr, 0, sizeof(int), s));
+    DWG_TRY(ensure_hist(p.total_iter > 0 ? p.total_iter : 1));
+    DWG_CHECK_CUDA(cudaStreamSynchronize(s));
+    return join_out();
+}
+
+// one DWG iteration, src/TurboDWG.cu:516-657
+int Pipeline::iterate_once() {
+    k_iter_begin<<<1, 1, 0, s>>>(iter_dev.ptr, sigma_tab.ptr, half_tab.ptr, cur_sigma.ptr, cur_half.ptr,
+                                 terms_cur.ptr);
+    DWG_CHECK_LAUNCH();
+    // UpdateMassNormals (:535)
+    k_set_nr<<<div_up(L, 256), 256, 0, s>>>(t2.nr.ptr, leaf_nrm.ptr, nullptr, L);
+    DWG_TRY(octree_update_normals(t2, s));
+    // screened GWN at the leaves and at the grid (:536-537)
+    dwg_gwn_params gp;
+    gp.beta = prm.beta;
+    gp.sigma = prm.lambda;
+    gp.screen = prm.screen;
+    gp.screened = 1;
+    gp.use_radii = prm.use_radii;
+    gp.precision = prm.precision;
+    GwnQuery ql;
+    ql.q = leaf_pos.ptr;
+    ql.nq = L;
+    DWG_TRY(gwn_eval(t2, ql, gp, wleaf.ptr, terms_cur.ptr, nullptr, s, cur_sigma.ptr));
+    GwnQuery qg;
+    for (int d = 0; d < 3; ++d) {
+        qg.res[d] = gres[d];
+        qg.origin[d] = gorg[d];
+    }
+    qg.spacing = gh;
+    DWG_TRY(gwn_eval(t2, qg, gp, field.ptr, terms_cur.ptr, nullptr, s, cur_sigma.ptr));
+    // mean iso value, halved every 5th iteration (:541-550)
+    DWG_TRY(mean_to_iso(wleaf.ptr, L, iso_dev.ptr, cur_half.ptr, iso_hist.ptr, iter_dev.ptr, partial, s));
+    // marching cubes at the iso value (:554)
+    McGrid g;
+    for (int d = 0; d < 3; ++d) {
+        g.res[d] = gres[d];
+        g.origin[d] = gorg[d];
+    }
+    g.spacing = gh;
+    DWG_TRY(mc_run(field.ptr, g, 0.f, iso_dev.ptr, nullptr, cent.ptr, tnrm.ptr, cap, ntri.ptr, mcws, s));
+    // k nearest leaves of every triangle centroid (:560-569)
+    KnnQuery q;
+    q.q = cent.ptr;
+    q.nq = cap;
+    q.nq_dev = ntri.ptr;
+    DWG_TRY(knn_query(kidx, q, prm.knn_tri, knn_buf.ptr, s));
+    // normal scatter + normalise (:571-583)
+    DWG_TRY(diffuse_normals(knn_buf.ptr, tnrm.ptr, cap, ntri.ptr, prm.knn_tri, L, leaf_nrm.ptr, acc.ptr,
+                            is_zero.ptr, zero_count.ptr, s));
+    // zero-normal repair when more than knn_zero points are zero (:585-644)
+    DWG_TRY(zero_repair(kidx, leaf_pos.ptr, L, leaf_nrm.ptr, is_zero.ptr, prm.knn_zero, prm.knn_zero, zws, s));
+    k_iter_end<<<1, 1, 0, s>>>(iter_dev.ptr, ntri.ptr, cap, zero_count.ptr, terms_cur.ptr, tri_hist.ptr,
+                               zero_hist.ptr, terms_hist.ptr);
+    DWG_CHECK_LAUNCH();
+    return DWG_OK;
+}
+
+int Pipeline::iterate(int n_iters) {
+    DWG_REQUIRE(!finalized, "pipeline: already finalized");
+    if (n_iters <= 0) return DWG_OK;
+    DWG_TRY(ensure_hist(iter + n_iters));
+    DWG_TRY(join_in());
+    for (int k = 0; k < n_iters; ++k) {
+        if (prm.use_graph && iter > 0) {
+            if (!graph_exec) {
+                DWG_CHECK_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+                int st = iterate_once();
+                cudaGraph_t gr = nullptr;
+                cudaError_t e = cudaStreamEndCapture(s, &gr);
+                if (st != DWG_OK) {
+                    if (gr) cudaGraphDestroy(gr);
+                    return st;
+                }
+                DWG_CHECK_CUDA(e);
+                graph = gr;
+                DWG_CHECK_CUDA(cudaGraphInstantiate(&graph_exec, graph, 0));
+            }
+            DWG_CHECK_CUDA(cudaGraphLaunch(graph_exec, s));
+        } else {
+            DWG_TRY(iterate_once());
+        }
+        ++iter;
+    }
+    return join_out();
+}
+
+// final pass, src/TurboDWG.cu:768-924
+int Pipeline::finalize() {
+    DWG_REQUIRE(!finalized, "pipeline: already finalized");
+    DWG_TRY(join_in());
+    dwg_gwn_params gp;
+    gp.beta = prm.beta;
+    gp.sigma = prm.lambda;
+    gp.screen = prm.screen;
+    gp.screened = 1;
+    gp.use_radii = prm.use_radii;
+    gp.precision = prm.precision;
+    DWG_TRY(final_iso.reserve(1));
+    DWG_TRY(final_ntri.reserve(1));
+    Octree* tree = nullptr;
+    const float* qpts = nullptr;
+    long long nqp = 0;
+    if (prm.use_leaves_generate == 1) {
+        // GenerateMesh(grid_points, ...) from the leaves (src/TurboDWG.cu:768-806)
+        DWG_TRY(voxel_grid_host(leaf_pos.ptr, L, 0.01f, prm.final_reso, s, fres, forg, &fh));
+        if (prm.use_radii) {
+            DevBuf<int> nb;
+            DWG_TRY(nb.reserve((size_t)L * prm.final_kw));
+            KnnQuery q;
+            q.q = leaf_pos.ptr;
+            q.nq = L;
+            DWG_TRY(knn_query(kidx, q, prm.final_kw, nb.ptr, s));
+            DWG_TRY(radii(leaf_pos.ptr, L, nb.ptr, prm.final_kw, leaf_rad.ptr, s));
+            DWG_CHECK_CUDA(cudaStreamSynchronize(s));
+        }
+        k_set_nr<<<div_up(L, 256), 256, 0, s>>>(t2.nr.ptr, leaf_nrm.ptr, leaf_rad.ptr, L);
+        DWG_CHECK_LAUNCH();
+        tree = &t2;
+        qpts = leaf_pos.ptr;
+        nqp = L;
+        DWG_TRY(point_nrm.reserve((size_t)n * 3));
+        DWG_CHECK_CUDA(cudaMemsetAsync(point_nrm.ptr, 0, sizeof(float) * 3 * n, s));
+    } else {
+        // GenerateMesh(cloud_points, ...) (src/TurboDWG.cu:808-924)
+        DWG_TRY(voxel_grid_host(P.ptr, n, prm.offset_2, prm.final_reso, s, fres, forg, &fh));
+        DWG_TRY(point_nrm.reserve((size_t)n * 3));
+        DWG_TRY(nb_final.reserve((size_t)n * prm.normal_kw));
+        KnnQuery q;
+        q.q = P.ptr;
+        q.nq = n;
+        DWG_TRY(knn_query(kidx, q, prm.normal_kw, nb_final.ptr, s));
+        DWG_TRY(load_normals(nb_final.ptr, prm.normal_kw, n, leaf_nrm.ptr, point_nrm.ptr, s));
+        DWG_TRY(pt_rad.reserve(n));
+        k_fill<<<div_up(n, 256), 256, 0, s>>>(pt_rad.ptr, n, prm.screen);
+        DWG_CHECK_LAUNCH();
+        if (prm.use_radii) {
+            KnnIndex pix;
+            DWG_TRY(knn_build(pix, P.ptr, n, s));
+            DevBuf<int> nb;
+            DWG_TRY(nb.reserve((size_t)n * prm.final_kw));
+            KnnQuery q2;
+            q2.q = P.ptr;
+            q2.nq = n;
+            DWG_TRY(knn_query(pix, q2, prm.final_kw, nb.ptr, s));
+            DWG_TRY(radii(P.ptr, n, nb.ptr, prm.final_kw, pt_rad.ptr, s));
+            DWG_CHECK_CUDA(cudaStreamSynchronize(s));
+        }
+        DWG_TRY(octree_set_point_data(t1, point_nrm.ptr, nullptr, pt_rad.ptr, s));
+        DWG_TRY(p_sorted.reserve((size_t)n * 3));
+        k_sorted_xyz<<<div_up(n, 256), 256, 0, s>>>(t1.pa.ptr, n, p_sorted.ptr);
+        DWG_CHECK_LAUNCH();
+        tree = &t1;
+        qpts = p_sorted.ptr;
+        nqp = n;
+    }
+    DWG_TRY(octree_update_normals(*tree, s));
+    DWG_TRY(wfin.reserve(nqp));
+    GwnQuery ql;
+    ql.q = qpts;
+    ql.nq = nqp;
+    DWG_TRY(gwn_eval(*tree, ql, gp, wfin.ptr, nullptr, nullptr, s));
+    long long ng = (long long)fres[0] * fres[1] * fres[2];
+    DWG_TRY(final_field.reserve(ng));
+    GwnQuery qg;
+    for (int d = 0; d < 3; ++d) {
+        qg.res[d] = fres[d];
+        qg.origin[d] = forg[d];
+    }
+    qg.spacing = fh;
+    DWG_TRY(gwn_eval(*tree, qg, gp, final_field.ptr, nullptr, nullptr, s));
+    DWG_TRY(mean_to_iso(wfin.ptr, nqp, final_iso.ptr, nullptr, nullptr, nullptr, partial, s));
+    final_cap = ng / 2 > 1000000 ? ng / 2 : 1000000;
+    DWG_TRY(tris.reserve((size_t)final_cap * 9));
+    McGrid g;
+    for (int d = 0; d < 3; ++d) {
+        g.res[d] = fres[d];
+        g.origin[d] = forg[d];
+    }
+    g.spacing = fh;
+    DWG_TRY(mc_run(final_field.ptr, g, 0.f, final_iso.ptr, tris.ptr, nullptr, nullptr, final_cap, final_ntri.ptr,
+                   mcws, s));
+    finalized = true;
+    return join_out();
+}
+
+}  // namespace dwg

@@ -1,0 +1,77 @@
+// pipeline.cuh -- the DWG reconstruction driver on one GPU.
+#pragma once
+
+#include "gwn.cuh"
+#include "knn.cuh"
+#include "mc.cuh"
+#include "normals.cuh"
+#include "octree.cuh"
+
+namespace dwg {
+
+struct Pipeline {
+    dwg_params prm;
+    cudaStream_t s = nullptr;       // the pipeline's own non-blocking stream
+    cudaStream_t caller = nullptr;  // the stream the caller passed
+    cudaEvent_t ev = nullptr;
+    int n = 0;  // points
+    int L = 0;  // leaves
+    DevBuf<float> P, Nin, area_pts;
+    Octree t1, t2;
+    KnnIndex kidx;  // on the leaves (canonical order)
+    // leaves, canonical order (depth-first order of the octree on the leaves)
+    DevBuf<float> leaf_pos, leaf_nrm, leaf_area, leaf_rad;
+    // iteration grid
+    int gres[3] = {0, 0, 0};
+    float gorg[3] = {0, 0, 0};
+    float gh = 0;
+    DevBuf<float> field, wleaf;
+    long long cap = 0;
+    DevBuf<float> cent, tnrm;
+    DevBuf<unsigned long long> ntri;
+    McWorkspace mcws;
+    DevBuf<int> knn_buf;
+    DevBuf<long long> acc;
+    DevBuf<unsigned char> is_zero;
+    DevBuf<int> zero_count;
+    ZeroRepairWs zws;
+    DevBuf<double> partial;
+    // per-iteration state on the device
+    DevBuf<int> iter_dev, half_tab, cur_half;
+    DevBuf<float> sigma_tab, cur_sigma, iso_dev;
+    DevBuf<unsigned long long> terms_cur;
+    DevBuf<float> iso_hist;
+    DevBuf<long long> tri_hist;
+    DevBuf<int> zero_hist;
+    DevBuf<unsigned long long> terms_hist;
+    int iter = 0;
+    int hist_cap = 0;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    // final pass
+    bool finalized = false;
+    int fres[3] = {0, 0, 0};
+    float forg[3] = {0, 0, 0};
+    float fh = 0;
+    DevBuf<float> final_field, point_nrm, tris, wfin, p_sorted, pt_rad;
+    DevBuf<int> nb_final;
+    DevBuf<unsigned long long> final_ntri;
+    DevBuf<float> final_iso;
+    long long final_cap = 0;
+
+    ~Pipeline();
+    int setup(const float* points_dev, const float* normals_dev, int n_points, const dwg_params& p,
+              cudaStream_t stream);
+    int iterate(int n_iters);
+    int iterate_once();
+    int finalize();
+    int ensure_hist(int total);
+    // order the pipeline stream after the caller's work, and back
+    int join_in();
+    int join_out();
+};
+
+int voxel_grid_host(const float* points_dev, int n, float offset, int s_res, cudaStream_t st, int res[3],
+                    float origin[3], float* spacing);
+
+}  // namespace dwg

@@ -1,0 +1,306 @@
+"""Python mirror of the reference's operator classes over the C ABI.
+
+Class and method names follow the reference (DWGTech/DWG):
+
+* ``TurboNormalInitialization.GaussMapInit``   -- include/TurboNormalInit.h:9-14
+* ``TurboLibiGWN`` (PreLibiGWN, UpdateMassNormals, UpdateGWNInfo,
+  TurboLibiGWNLaunch, TurboLibiScreenedGWNLaunch, EarseMemory)
+                                                 -- include/Turbo_GWN_l.h:24-69
+* ``TurboMC.TurboMarchingCubes``                 -- include/MarchingCubeCuda.h:35-44
+* ``GenerateKDTreeForDWG`` / ``CudaKNNWithKDTreeforDWG``
+                                                 -- include/TurboDWG.h:14-27
+* ``TurboDWG`` (the iteration and meshing driver) -- include/TurboDWG.h:29-74
+
+Eigen matrices and std::vector arguments of the reference become torch CUDA
+tensors of shape (n, 3) / (n,), float32; the CPU octree inputs (O_PI, O_CH,
+O_CM, O_R, O_EC) are replaced by a GPU octree built from the points.  Every
+call runs the CUDA library; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import capi
+
+
+def _req_cuda_f32(t, name, shape_last=None):
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError(f"{name} must be a CUDA tensor")
+    if t.dtype != torch.float32:
+        raise TypeError(f"{name} must be float32")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+    if shape_last is not None and (t.dim() != 2 or t.shape[1] != shape_last):
+        raise ValueError(f"{name} must have shape (n, {shape_last})")
+    return t
+
+
+class TurboNormalInitialization:
+    """Gauss-map normal initialisation (src/TurboNormalInit.cu:29-44)."""
+
+    def GaussMapInit(self, point_pos, point_normal, bound_upper=None, bound_lower=None, point_num=None):
+        _req_cuda_f32(point_pos, "point_pos", 3)
+        _req_cuda_f32(point_normal, "point_normal", 3)
+        n = point_pos.shape[0] if point_num is None else int(point_num)
+        if bound_upper is not None or bound_lower is not None:
+            # the reference passes the kd-tree bounds; they equal the bounding box
+            pass
+        capi.check(capi.load().dwg_gauss_map_init(capi.ptr(point_pos), n, capi.ptr(point_normal),
+                                                  capi.stream_ptr()))
+
+
+class TurboLibiGWN:
+    """Screened / plain generalised winding number with a GPU octree.
+
+    ``TurboLibiGWN(points, max_depth, areas)`` replaces the reference's
+    ``TurboLibiGWN(O_PI, O_CH, O_CM, O_R, O_EC)`` + ``PreLibiGWN``: the
+    octree (octreeDWG topology) and its moments are built on the GPU."""
+
+    def __init__(self, point_cloud=None, max_depth=10, areas=None):
+        self._h = C.c_void_p()
+        self.n = 0
+        if point_cloud is not None:
+            self.PreLibiGWN(point_cloud, max_depth, areas)
+
+    def PreLibiGWN(self, point_cloud, max_depth=10, areas=None):
+        _req_cuda_f32(point_cloud, "point_cloud", 3)
+        self.EarseMemory()
+        self.points = point_cloud
+        self.n = point_cloud.shape[0]
+        capi.check(capi.load().dwg_octree_build(capi.ptr(point_cloud), self.n, int(max_depth),
+                                                capi.ptr(areas), capi.stream_ptr(), C.byref(self._h)))
+
+    def num_nodes(self):
+        v = C.c_int()
+        capi.check(capi.load().dwg_octree_num_nodes(self._h, C.byref(v)))
+        return v.value
+
+    def UpdateMassNormals(self, i_Normals, i_As):
+        capi.check(capi.load().dwg_octree_update_normals(self._h, capi.ptr(i_Normals), capi.ptr(i_As),
+                                                         capi.stream_ptr()))
+
+    def UpdateGWNInfo(self, i_Normals, point_cloud=None, i_As=None):
+        capi.check(capi.load().dwg_octree_update_info(self._h, capi.ptr(i_Normals), capi.ptr(i_As),
+                                                      capi.stream_ptr()))
+
+    def _launch(self, query_points, i_Normals, i_As, radii, params, out_gwn, terms=None):
+        _req_cuda_f32(query_points, "query_points", 3)
+        nq = query_points.shape[0]
+        if out_gwn is None:
+            out_gwn = torch.empty(nq, dtype=torch.float32, device=query_points.device)
+        capi.check(capi.load().dwg_gwn_points(
+            self._h, capi.ptr(i_Normals), capi.ptr(i_As), capi.ptr(radii), capi.ptr(query_points), nq,
+            C.byref(params), capi.ptr(out_gwn), capi.ptr(terms), capi.stream_ptr()))
+        return out_gwn
+
+    def TurboLibiGWNLaunch(self, query_points, point_cloud=None, query_size=None, i_Normals=None, i_As=None,
+                           beta=2.3, out_gwn=None, precision=1):
+        """Plain GWN, sum A (p-q).n / (4 pi r^3 + 1e-8) (src/TurboLibiGWN.cu:328-511,899-910)."""
+        p = capi.gwn_params(beta=beta, sigma=0.0, screened=False, precision=precision)
+        return self._launch(query_points, i_Normals, i_As, None, p, out_gwn)
+
+    def TurboLibiScreenedGWNLaunch(self, query_points, point_cloud=None, query_size=None, i_Normals=None,
+                                   i_As=None, i_radii=None, beta=2.3, sigma=10.0, out_gwn=None, use_radii=False,
+                                   precision=1, screen=0.0015):
+        """Screened GWN (src/TurboLibiGWN.cu:513-812,912-922)."""
+        p = capi.gwn_params(beta=beta, sigma=sigma, screen=screen, screened=True, use_radii=use_radii,
+                            precision=precision)
+        return self._launch(query_points, i_Normals, i_As, i_radii if use_radii else None, p, out_gwn)
+
+    def grid(self, res, origin, spacing, i_Normals=None, i_As=None, beta=2.3, sigma=10.0, screened=True,
+             precision=1, out=None, terms=None, screen=0.0015):
+        """GWN at the closed-form grid origin + index * spacing (x fastest)."""
+        res = np.ascontiguousarray(res, np.int32)
+        org = np.ascontiguousarray(origin, np.float32)
+        n = int(np.prod(res.astype(np.int64)))
+        if out is None:
+            out = torch.empty(n, dtype=torch.float32, device="cuda")
+        p = capi.gwn_params(beta=beta, sigma=sigma, screen=screen, screened=screened, precision=precision)
+        capi.check(capi.load().dwg_gwn_grid(self._h, capi.ptr(i_Normals), capi.ptr(i_As), None, res.ctypes.data,
+                                            org.ctypes.data, float(spacing), C.byref(p), capi.ptr(out),
+                                            capi.ptr(terms), capi.stream_ptr()))
+        return out
+
+    def status(self):
+        """Sticky traversal error flags (0 = none); raises on a set flag."""
+        f = C.c_uint()
+        capi.check(capi.load().dwg_octree_status(self._h, C.byref(f)))
+        return f.value
+
+    def export(self):
+        """Node table (host numpy): depth, pt_start, pt_count, skip, cm, radius, ec, perm."""
+        M = self.num_nodes()
+        out = dict(depth=np.empty(M, np.int32), pt_start=np.empty(M, np.int32), pt_count=np.empty(M, np.int32),
+                   skip=np.empty(M, np.int32), cm=np.empty((M, 3), np.float64), radius=np.empty(M, np.float64),
+                   ec=np.empty((M, 3), np.float64), perm=np.empty(max(self.n, 1), np.int32))
+        capi.check(capi.load().dwg_octree_export(
+            self._h, *[out[k].ctypes.data for k in ("depth", "pt_start", "pt_count", "skip", "cm", "radius",
+                                                    "ec", "perm")]))
+        out["perm"] = out["perm"][: self.n]
+        return out
+
+    def EarseMemory(self):
+        if getattr(self, "_h", None) and self._h.value:
+            capi.load().dwg_octree_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.EarseMemory()
+        except Exception:
+            pass
+
+
+class TurboMC:
+    """Marching cubes (src/TurboMC.cu:572-638)."""
+
+    def TurboMarchingCubes(self, voxel_values, voxel_poses, res_x, res_y, res_z, threshold, iterations=0,
+                           mesh_path="", mesh_full_path="", mid_points=None, mid_normals=None, test_iter=999999,
+                           origin=None, spacing=None, tris=None, capacity=None):
+        """Returns the triangle count; writes a binary STL when
+        ``iterations == 123456`` (to mesh_full_path + '.stl') or when
+        ``iterations % test_iter == 0`` with test_iter != 999999, as the
+        reference does."""
+        res = np.array([res_x, res_y, res_z], np.int32)
+        ncell = (res_x - 1) * (res_y - 1) * (res_z - 1)
+        if capacity is None:
+            capacity = max(res_x * res_y * res_z // 2, 1000000)
+        want_stl = (test_iter != 999999 and iterations % test_iter == 0) or iterations == 123456
+        if want_stl and tris is None:
+            tris = torch.empty((capacity, 9), dtype=torch.float32, device=voxel_values.device)
+        org = np.ascontiguousarray(origin if origin is not None else [0, 0, 0], np.float32)
+        T = C.c_longlong()
+        cnt = torch.zeros(1, dtype=torch.int64, device=voxel_values.device)
+        rc = capi.load().dwg_marching_cubes(
+            capi.ptr(voxel_values), res.ctypes.data, capi.ptr(voxel_poses),
+            org.ctypes.data if voxel_poses is None else None, float(spacing or 0.0), float(threshold),
+            capi.ptr(tris), capi.ptr(mid_points), capi.ptr(mid_normals), int(capacity), capi.ptr(cnt),
+            C.byref(T), capi.stream_ptr())
+        capi.check(rc)
+        del ncell
+        if want_stl:
+            path = (mesh_full_path + ".stl") if iterations == 123456 else f"{mesh_path}{iterations}iter.stl"
+            host = tris[: T.value].cpu().numpy()
+            capi.check(capi.load().dwg_write_stl(path.encode(), host.ctypes.data, T.value))
+        return T.value
+
+
+class KnnIndex:
+    """GenerateKDTreeForDWG replacement (src/KNN_GWN.cu:183-212): a GPU index."""
+
+    def __init__(self, points):
+        _req_cuda_f32(points, "points", 3)
+        self.points = points
+        self._h = C.c_void_p()
+        capi.check(capi.load().dwg_knn_build(capi.ptr(points), points.shape[0], capi.stream_ptr(),
+                                             C.byref(self._h)))
+
+    def query(self, queries, k, out=None):
+        """CudaKNNWithKDTreeforDWG replacement (src/KNN_GWN.cu:490-715)."""
+        _req_cuda_f32(queries, "queries", 3)
+        if out is None:
+            out = torch.empty((queries.shape[0], k), dtype=torch.int32, device=queries.device)
+        capi.check(capi.load().dwg_knn_query(self._h, capi.ptr(queries), queries.shape[0], int(k), capi.ptr(out),
+                                             capi.stream_ptr()))
+        return out
+
+    def __del__(self):
+        try:
+            if self._h.value:
+                capi.load().dwg_knn_destroy(self._h)
+        except Exception:
+            pass
+
+
+def GenerateKDTreeForDWG(d_points, d_normals=None, points_size=None, bound_upper=None, bound_lower=None):
+    return KnnIndex(d_points)
+
+
+def CudaKNNWithKDTreeforDWG(d_points, numPoints, d_queries, numQueries, bound_upper, bound_lower, d_results, k,
+                            index=None):
+    ix = index if index is not None else KnnIndex(d_points[:numPoints])
+    ix.query(d_queries[:numQueries], k, out=d_results.view(numQueries, k))
+    return d_results
+
+
+def voxel_grid(points, offset, s):
+    """igl::voxel_grid(V, offset, s, 1) in closed form -> (res[3], origin[3], spacing)."""
+    _req_cuda_f32(points, "points", 3)
+    res = np.empty(3, np.int32)
+    org = np.empty(3, np.float32)
+    h = C.c_float()
+    capi.check(capi.load().dwg_voxel_grid(capi.ptr(points), points.shape[0], float(offset), int(s),
+                                          capi.stream_ptr(), res.ctypes.data, org.ctypes.data, C.byref(h)))
+    return res, org, np.float32(h.value)
+
+
+class TurboDWG:
+    """The DWG iteration + meshing driver (src/TurboDWG.cu:456-989), as one
+    GPU pipeline: ``TurboDWG(points, normals=None, **flags)``, then
+    ``TurboScreenedDWGLaunch(total_iters)`` and ``GenerateMesh()``."""
+
+    def __init__(self, points, normals=None, **flags):
+        _req_cuda_f32(points, "points", 3)
+        self.params = capi.default_params(**flags)
+        self.points = points
+        self._h = C.c_void_p()
+        capi.check(capi.load().dwg_pipeline_create(capi.ptr(points), capi.ptr(normals), points.shape[0],
+                                                   C.byref(self.params), capi.stream_ptr(), C.byref(self._h)))
+
+    def TurboScreenedDWGLaunch(self, total_iters=None):
+        n = self.params.total_iter if total_iters is None else int(total_iters)
+        capi.check(capi.load().dwg_pipeline_iterate(self._h, n))
+
+    def GenerateMesh(self):
+        capi.check(capi.load().dwg_pipeline_finalize(self._h))
+
+    def size(self, what):
+        v = C.c_longlong()
+        capi.check(capi.load().dwg_pipeline_size(self._h, what.encode(), C.byref(v)))
+        return v.value
+
+    def get(self, what):
+        sizes = {"leaf_pos": (self.size("leaves"), 3), "leaf_nrm": (self.size("leaves"), 3),
+                 "point_nrm": (self.size("points"), 3), "iso": (self.size("iterations"),),
+                 "field": (self.size("grid"),), "final_field": (self.size("final_grid"),),
+                 "final_iso": (1,), "grid_res": (3,), "final_res": (3,), "grid_origin": (4,),
+                 "final_origin": (4,)}
+        dtypes = {"tri_count": np.int64, "zero_count": np.int32, "terms": np.uint64, "grid_res": np.int32,
+                  "final_res": np.int32}
+        if what == "tris":
+            shape = (self.size("triangles"), 9)
+        elif what in ("tri_count", "zero_count", "terms"):
+            shape = (self.size("iterations"),)
+        else:
+            shape = sizes[what]
+        a = np.empty(shape, dtypes.get(what, np.float32))
+        if a.size:
+            capi.check(capi.load().dwg_pipeline_get(self._h, what.encode(), a.ctypes.data))
+        return a
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            capi.load().dwg_pipeline_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def reconstruct(points, normals=None, **flags):
+    """Full reconstruction on the GPU; returns a dict of host arrays."""
+    d = TurboDWG(points, normals, **flags)
+    d.TurboScreenedDWGLaunch()
+    d.GenerateMesh()
+    out = {k: d.get(k) for k in ("leaf_pos", "leaf_nrm", "iso", "tri_count", "zero_count", "terms", "tris",
+                                 "final_iso", "final_res")}
+    if not d.params.use_leaves_generate:
+        out["point_nrm"] = d.get("point_nrm")
+    d.close()
+    return out

@@ -1,0 +1,267 @@
+/*
+ * dwg_b200.h -- C ABI of the B200-native DWG reconstruction hot path.
+ *
+ * Conventions
+ *   - Pointers named *_dev are device pointers (cudaMalloc'd by the caller,
+ *     not managed memory); *_host are host pointers.  Point arrays are packed
+ *     xyz float triples (n * 3 floats).
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *     Calls enqueue work on it; results are valid once the stream has
+ *     completed, unless a function says it synchronises.
+ *   - Every function returns DWG_OK (0) or a negative status; the message of
+ *     the last error of the calling thread is available from dwg_last_error().
+ *   - Objects (octree, kNN index, pipeline) are owned by the library and freed
+ *     with their *_destroy function.  A handle must not be used from two host
+ *     threads at once.
+ */
+#ifndef DWG_B200_H
+#define DWG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DWG_OK 0
+#define DWG_ERR_INVALID (-1)   /* bad argument (null pointer, size, k > n ...) */
+#define DWG_ERR_CUDA (-2)      /* a CUDA runtime call failed */
+#define DWG_ERR_OVERFLOW (-3)  /* an output capacity was exceeded */
+#define DWG_ERR_NOMEM (-4)     /* device allocation failed */
+#define DWG_ERR_DEVICE (-5)    /* a kernel reported an error status */
+
+const char* dwg_last_error(void);
+/* library version string */
+const char* dwg_version(void);
+
+/* ------------------------------------------------------------------------
+ * Gauss-map initial normals: n_i = (p_i - c) / (|p_i - c| + 1e-8), with c the
+ * centre of the points' bounding box (computed on the device).
+ * Replaces TurboNormalInitialization::GaussMapInit
+ * (include/TurboNormalInit.h:13, src/TurboNormalInit.cu:29-44); the reference
+ * takes the bounds from its kd-tree build instead of computing them.
+ * ------------------------------------------------------------------------ */
+int dwg_gauss_map_init(const float* points_dev, int n, float* normals_dev, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Octree over a point set, rebuilt on the GPU.  Topology follows
+ * igl::octreeDWG (deps/libigl/include/igl/octree.cpp:171-335): a cube around
+ * the bounding box, a cell splits while it holds more than one point and its
+ * depth is below max_depth (1..21).  The CPU octree + TurboLibiGWN::PreLibiGWN
+ * flattening (src/TurboLibiGWN.cu:132-231) are replaced by this build.
+ * `areas_dev` fixes the mass centres / radii (fast_winding_number.cpp:9-120,
+ * computed in FP64); NULL means unit areas.
+ * ------------------------------------------------------------------------ */
+typedef struct dwg_octree dwg_octree;
+int dwg_octree_build(const float* points_dev, int n, int max_depth, const float* areas_dev,
+                     void* stream, dwg_octree** out);
+int dwg_octree_destroy(dwg_octree* tree);
+/* number of nodes (host query; synchronises the build stream once) */
+int dwg_octree_num_nodes(const dwg_octree* tree, int* num_nodes);
+/* Recompute the dipole moments sum(A_i n_i) per node, FP64.
+ * Replaces TurboLibiGWN::UpdateMassNormals (src/TurboLibiGWN.cu:924-952,1044-1052). */
+int dwg_octree_update_normals(dwg_octree* tree, const float* normals_dev, const float* areas_dev,
+                              void* stream);
+/* Recompute centres, radii and moments from new areas.
+ * Replaces TurboLibiGWN::UpdateGWNInfo (src/TurboLibiGWN.cu:954-1017,1054-1062). */
+int dwg_octree_update_info(dwg_octree* tree, const float* normals_dev, const float* areas_dev,
+                           void* stream);
+/* Sticky error word of the traversal kernels of this tree (synchronises):
+ * 0 = none; bit 0 stack overflow, bit 1 malformed node links, bit 2 leaf
+ * range outside the point array.  Any set bit makes the call return
+ * DWG_ERR_DEVICE. */
+int dwg_octree_status(const dwg_octree* tree, unsigned int* flags);
+/* Copy the node table to host memory (for checking).  Arrays may be NULL.
+ * Nodes are in depth-first pre-order; points are in the octree's sorted
+ * order, perm_host[i] = input index of sorted point i.
+ *   depth[M], pt_start[M], pt_count[M], skip[M] (index after the subtree),
+ *   cm[M*3] (FP64), radius[M] (FP64), ec[M*3] (FP64), perm[n] */
+int dwg_octree_export(const dwg_octree* tree, int* depth_host, int* pt_start_host,
+                      int* pt_count_host, int* skip_host, double* cm_host, double* radius_host,
+                      double* ec_host, int* perm_host);
+
+/* ------------------------------------------------------------------------
+ * Generalised winding number at query points, Barnes-Hut over `tree`.
+ * w(q) = sum over terms of A (sigma rho + 1) ((p - q).n) / (e^{sigma rho} 4 pi rho^3 + 1e-7)
+ * (screened, rho = max(|p-q|, s)), or A ((p - q).n) / (4 pi |p-q|^3 + 1e-8)
+ * (plain); far nodes (|CM - q| > beta R) contribute one dipole term.
+ * The opening decisions are the reference's, per query.
+ * Replaces TurboLibiGWN::TurboLibiScreenedGWNLaunch / TurboLibiGWNLaunch
+ * (include/Turbo_GWN_l.h:38-56, src/TurboLibiGWN.cu:814-922).
+ * normals/areas/radii are indexed like the points the tree was built from.
+ * ------------------------------------------------------------------------ */
+typedef struct {
+    float beta;      /* opening ratio, reference 2.3 */
+    float sigma;     /* screening coefficient (--lambda) */
+    float screen;    /* screen radius s when use_radii == 0, reference 0.0015 */
+    int screened;    /* 1 screened kernel, 0 plain kernel */
+    int use_radii;   /* 1: s = radii[i] for point terms (far field keeps `screen`) */
+    int precision;   /* 0 plain FP32 accumulation, 1 FP32 compensated (default) */
+} dwg_gwn_params;
+
+int dwg_gwn_points(dwg_octree* tree, const float* normals_dev, const float* areas_dev,
+                   const float* radii_dev, const float* queries_dev, long long num_queries,
+                   const dwg_gwn_params* params, float* out_dev, unsigned long long* terms_dev,
+                   void* stream);
+
+/* Same as dwg_gwn_points, writing the number of terms of every query to
+ * per_query_terms_dev (int32) -- a check that the opening decisions match
+ * a CPU restatement of the traversal, query by query. */
+int dwg_gwn_points_counted(dwg_octree* tree, const float* normals_dev, const float* areas_dev,
+                           const float* radii_dev, const float* queries_dev, long long num_queries,
+                           const dwg_gwn_params* params, float* out_dev, int* per_query_terms_dev,
+                           void* stream);
+
+/* Same sum at the samples of a regular grid: q(x,y,z) = origin + (x,y,z) * spacing,
+ * x fastest; out has res[0]*res[1]*res[2] values.  The reference materialises
+ * the grid positions (igl::voxel_grid + H2D copy); here they are closed-form. */
+int dwg_gwn_grid(dwg_octree* tree, const float* normals_dev, const float* areas_dev,
+                 const float* radii_dev, const int res[3], const float origin[3], float spacing,
+                 const dwg_gwn_params* params, float* out_dev, unsigned long long* terms_dev,
+                 void* stream);
+
+/* Closed-form igl::voxel_grid(V, offset, s, 1) (deps/libigl/include/igl/voxel_grid.cpp:11-87):
+ * resolution, origin and spacing of the padded grid around points_dev.
+ * Synchronises `stream` (the bounding box is read back). */
+int dwg_voxel_grid(const float* points_dev, int n, float offset, int s, void* stream, int res[3],
+                   float origin[3], float* spacing);
+
+/* ------------------------------------------------------------------------
+ * Marching cubes on a scalar grid (x fastest).  Corner, edge and case
+ * conventions of TurboMC::TurboMarchingCubes (src/TurboMC.cu:383-478,572-638);
+ * triangles are written in cell order (deterministic), each as 3 vertices
+ * (9 floats), plus centroid (3) and unit normal -cross/(|cross|+1e-8) (3).
+ * positions_dev (R^3 * 3 floats) may be NULL: then q = origin + idx*spacing.
+ * Output arrays may be NULL; at most `capacity` triangles are written.
+ * *num_tris_dev (device, unsigned long long) receives the full count T; when
+ * num_tris_host is non-NULL the call synchronises and stores T there, and
+ * returns DWG_ERR_OVERFLOW if T > capacity.
+ * ------------------------------------------------------------------------ */
+int dwg_marching_cubes(const float* field_dev, const int res[3], const float* positions_dev,
+                       const float origin[3], float spacing, float iso, float* tris_dev,
+                       float* centroids_dev, float* normals_dev, long long capacity,
+                       unsigned long long* num_tris_dev, long long* num_tris_host, void* stream);
+/* The generated case tables (edge mask [256], triangle edges [256*16], -1 padded). */
+int dwg_mc_tables(int* edge_table_host, signed char* tri_table_host);
+
+/* ------------------------------------------------------------------------
+ * k nearest neighbours.  Results ascend by the cukd candidate key
+ * (float bits of |p-q|^2) << 32 | index (include/cudaKDTree/cukd/knn.h:279-282),
+ * self included.  Replaces GenerateKDTreeForDWG + CudaKNNWithKDTreeforDWG
+ * (include/TurboDWG.h:14-27, src/KNN_GWN.cu:183-212,490-715) and the GWN
+ * variants (include/DWGProcess.h:20-30).  1 <= k <= 64, k <= n.
+ * ------------------------------------------------------------------------ */
+typedef struct dwg_knn_index dwg_knn_index;
+int dwg_knn_build(const float* points_dev, int n, void* stream, dwg_knn_index** out);
+int dwg_knn_destroy(dwg_knn_index* index);
+int dwg_knn_query(dwg_knn_index* index, const float* queries_dev, long long num_queries, int k,
+                  int* out_dev, void* stream);
+/* one-shot convenience: build, query, destroy */
+int dwg_knn(const float* points_dev, int n, const float* queries_dev, long long num_queries, int k,
+            int* out_dev, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Normal diffusion step: every triangle adds its normal to its k nearest
+ * points, sums are normalised; points whose sum has length < 1e-10 keep
+ * their normal and are flagged (is_zero_dev, may be NULL); *zero_count_dev
+ * receives their number.  Replaces ResetZero + UpdateNormals +
+ * NormalizeNormals (src/TurboDWG.cu:134-143,179-204,238-266,571-583).
+ * Sums are accumulated in 2^-40 fixed point so the result is independent of
+ * the order of the atomics.
+ * ------------------------------------------------------------------------ */
+int dwg_diffuse_normals(const int* knn_dev, const float* tri_normals_dev, long long num_tris, int k,
+                        int num_points, float* normals_dev, unsigned char* is_zero_dev,
+                        int* zero_count_dev, void* stream);
+/* Zero-normal repair: each flagged point gets the normalised sum of the
+ * normals of its k nearest unflagged points.  Replaces LoadZeroData +
+ * GenerateKDTreeForDWG + kNN + SimpleUpdateNonzeroNormals
+ * (src/TurboDWG.cu:145-177,322-359,585-644).  `index` must be built on the
+ * same points.  Runs only when the flagged count exceeds `min_zero` (10 in
+ * the reference), decided on the device. */
+int dwg_zero_repair(dwg_knn_index* index, float* normals_dev, const unsigned char* is_zero_dev,
+                    const int* zero_count_dev, int k, int min_zero, void* stream);
+/* Point normals = normalised mean of the normals of the k nearest leaves.
+ * Replaces LoadNormals (src/TurboDWG.cu:206-236,834-853). */
+int dwg_load_normals(const int* knn_dev, int k, long long num_queries,
+                     const float* leaf_normals_dev, float* out_dev, void* stream);
+/* r_i = clamp(sqrt(mean_j |p_i - p_j|^2), 0.0015, 0.015) over the k nearest
+ * (self included).  Replaces SimpleUpdateRadii / TurboDWG::UpdateRadii
+ * (src/TurboDWG.cu:361-391,674-691), with its per-neighbour offset initialised. */
+int dwg_radii(const float* points_dev, int n, const int* knn_dev, int k, float* radii_dev,
+              void* stream);
+
+/* ------------------------------------------------------------------------
+ * Full reconstruction (TurboIterative + TurboDWG::TurboScreenedDWGLaunch +
+ * TurboDWG::GenerateMesh, include/DWGProcess.h:474-797,
+ * src/TurboDWG.cu:456-924).  Parameters mirror the DWG_CUDA flags
+ * (src/main.cpp:19-39).
+ * ------------------------------------------------------------------------ */
+typedef struct {
+    int in_normal;          /* 0 random, 1 input, 3 Gauss map (default) */
+    int grid_reso;          /* --grid_reso (400) */
+    int final_reso;         /* --final_reso (500) */
+    int kw, final_kw, normal_kw; /* 10, 10, 10 */
+    int max_depth;          /* --max_depth (10) */
+    float lambda;           /* --lambda (10) */
+    int min_num;            /* --min_num (0) */
+    int use_radii;          /* --use_radii (0) */
+    float offset_1, offset_2; /* 0.05, 0.01 */
+    int use_leaves_generate; /* --use_leaves_generate (0) */
+    int total_iter;         /* --total_iter (40) */
+    float beta;             /* 2.3 */
+    float area;             /* 2e-6 */
+    float screen;           /* 0.0015 */
+    int knn_tri;            /* 15 */
+    int knn_zero;           /* 10 */
+    int precision;          /* dwg_gwn_params.precision */
+    int use_graph;          /* capture one iteration in a CUDA graph and replay it */
+} dwg_params;
+
+void dwg_params_default(dwg_params* p);
+
+typedef struct dwg_pipeline dwg_pipeline;
+/* points_dev: n normalised points; normals_dev: input normals (in_normal 0/1) or NULL. */
+int dwg_pipeline_create(const float* points_dev, const float* normals_dev, int n,
+                        const dwg_params* params, void* stream, dwg_pipeline** out);
+int dwg_pipeline_destroy(dwg_pipeline* p);
+/* run `n_iters` diffusion iterations (continuing the count) */
+int dwg_pipeline_iterate(dwg_pipeline* p, int n_iters);
+/* final meshing pass; the mesh stays on the device */
+int dwg_pipeline_finalize(dwg_pipeline* p);
+/* sizes: "leaves", "points", "triangles" (final mesh; synchronises),
+ * "iterations", "grid" (iteration grid samples), "final_grid" */
+int dwg_pipeline_size(dwg_pipeline* p, const char* what, long long* value);
+/* copy a result to host memory (synchronises): "leaf_pos" [L*3], "leaf_nrm" [L*3],
+ * "point_nrm" [N*3], "tris" [T*9], "iso" [iters], "tri_count" [iters] (int64),
+ * "zero_count" [iters] (int32), "field" [iteration grid], "final_field",
+ * "final_iso" [1], "terms" [iters] (uint64 pair evaluations per iteration),
+ * "grid_res" [3] (int32), "final_res" [3] (int32) */
+int dwg_pipeline_get(dwg_pipeline* p, const char* what, void* dst_host);
+/* device pointer of a pipeline array (no copy): "leaf_pos", "leaf_nrm",
+ * "point_nrm", "tris", "field", "final_field" */
+int dwg_pipeline_device_ptr(dwg_pipeline* p, const char* what, void** ptr);
+
+/* One call from host memory to host memory: create + iterate(total_iter) +
+ * finalize + copy of the mesh and point normals.  tris_host holds up to
+ * tri_capacity triangles; *num_tris receives the full count. */
+int dwg_reconstruct_host(const float* points_host, const float* normals_host, int n,
+                         const dwg_params* params, float* point_normals_host, float* tris_host,
+                         long long tri_capacity, long long* num_tris, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Host IO helpers (include/DWGProcess.h:53-97, src/TurboMC.cu:344-371,
+ * src/TurboDWG.cu:903-923).
+ * ------------------------------------------------------------------------ */
+/* Read "x y z [nx ny nz]" lines; returns the count in *n and malloc'd arrays
+ * (free with dwg_free_host).  When `normalize` is set, centre on the mean and
+ * divide by max 2|x| (FP64), as the reference reader does. */
+int dwg_read_xyz(const char* path, int normalize, float** points, float** normals, int* n);
+void dwg_free_host(void* p);
+int dwg_write_stl(const char* path, const float* tris_host, long long num_tris);
+int dwg_write_xyz(const char* path, const float* points_host, const float* normals_host, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DWG_B200_H */

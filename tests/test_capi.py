@@ -1,0 +1,127 @@
+"""CPU tests of the C ABI: the library loads, exports every symbol the header
+declares, rejects bad arguments before touching the GPU, generates the
+reference-pinned case table, and reads/writes the reference's file formats."""
+import ctypes as C
+import os
+import re
+import struct
+
+import numpy as np
+import pytest
+
+from dwg_b200 import capi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "dwg_b200.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"\b(dwg_[a-z0-9_]+)\s*\(", src)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol(dwg_lib):
+    names = declared_functions()
+    assert len(names) > 30
+    for n in names:
+        assert hasattr(dwg_lib, n), n
+    # and the binding covers them all
+    assert set(names) <= set(capi.exported_symbols())
+    assert dwg_lib.dwg_version().startswith(b"dwg_b200")
+
+
+def test_generated_table_matches_reference_fixture_and_oracle(dwg_lib, oracle_lib):
+    from tests.test_oracle import check_table_against_fixture
+    et = np.zeros(256, np.int32)
+    tt = np.zeros(256 * 16, np.int8)
+    assert dwg_lib.dwg_mc_tables(et.ctypes.data, tt.ctypes.data) == 0
+    tt = tt.reshape(256, 16)
+    check_table_against_fixture(et, tt)
+    oet, ott = oracle_lib.mc_tables()
+    assert np.array_equal(et, oet) and np.array_equal(tt, ott)
+
+
+def test_invalid_arguments_are_rejected(dwg_lib):
+    L = dwg_lib
+    h = C.c_void_p()
+    assert L.dwg_octree_build(None, 10, 8, None, None, C.byref(h)) == capi.DWG_ERR_INVALID
+    assert b"null" in L.dwg_last_error()
+    assert L.dwg_octree_build(1, 10, 8, None, None, None) == capi.DWG_ERR_INVALID
+    assert L.dwg_knn(1, 5, 1, 3, 0, 1, None) == capi.DWG_ERR_INVALID          # k = 0
+    assert L.dwg_knn(1, 5, 1, 3, 6, 1, None) == capi.DWG_ERR_INVALID          # k > n
+    assert b"k=6" in L.dwg_last_error()
+    assert L.dwg_pipeline_create(1, None, 100, None, None, C.byref(h)) == capi.DWG_ERR_INVALID
+    p = capi.default_params()
+    assert L.dwg_pipeline_create(None, None, 100, C.byref(p), None, C.byref(h)) == capi.DWG_ERR_INVALID
+    p.in_normal = 1  # needs input normals
+    assert L.dwg_pipeline_create(1, None, 100, C.byref(p), None, C.byref(h)) == capi.DWG_ERR_INVALID
+    assert L.dwg_mc_tables(None, None) == capi.DWG_ERR_INVALID
+
+
+def test_default_params_match_dwg_cuda_flags(dwg_lib):
+    # src/main.cpp:19-39 and the hard-coded constants of the reference
+    p = capi.default_params()
+    assert (p.in_normal, p.grid_reso, p.final_reso, p.kw, p.final_kw, p.normal_kw, p.max_depth) == \
+        (3, 400, 500, 10, 10, 10, 10)
+    assert p.lambda_ == 10.0 and p.min_num == 0 and p.use_radii == 0 and p.total_iter == 40
+    assert abs(p.offset_1 - 0.05) < 1e-7 and abs(p.offset_2 - 0.01) < 1e-7
+    assert abs(p.beta - 2.3) < 1e-6 and abs(p.area - 2e-6) < 1e-12 and abs(p.screen - 0.0015) < 1e-9
+    assert (p.knn_tri, p.knn_zero) == (15, 10)
+
+
+def test_read_xyz_normalises_like_the_reference(dwg_lib, tmp_path):
+    rng = np.random.default_rng(0)
+    P = rng.uniform(-3, 7, (50, 3))
+    N = rng.standard_normal((50, 3))
+    f = tmp_path / "c.xyz"
+    with open(f, "w") as fh:
+        for p, n in zip(P, N):
+            fh.write(" ".join(f"{v:.9f}" for v in (*p, *n)) + "\n")
+    pts = C.POINTER(C.c_float)()
+    nrm = C.POINTER(C.c_float)()
+    n = C.c_int()
+    assert dwg_lib.dwg_read_xyz(str(f).encode(), 1, C.byref(pts), C.byref(nrm), C.byref(n)) == 0
+    got = np.ctypeslib.as_array(pts, (n.value, 3)).copy()
+    gotn = np.ctypeslib.as_array(nrm, (n.value, 3)).copy()
+    dwg_lib.dwg_free_host(C.cast(pts, C.c_void_p))
+    dwg_lib.dwg_free_host(C.cast(nrm, C.c_void_p))
+    Pr = np.array([[float(f"{v:.9f}") for v in p] for p in P])
+    c = Pr.mean(0)
+    scale = np.max(2 * np.abs(Pr - c))
+    assert np.allclose(got, ((Pr - c) / scale).astype(np.float32), atol=1e-7)
+    assert np.abs(got).max() <= 0.5 + 1e-6
+    assert np.allclose(gotn, N, atol=1e-6)
+
+
+def test_read_xyz_rejects_malformed(dwg_lib, tmp_path):
+    f = tmp_path / "bad.xyz"
+    f.write_text("1 2 3\n4 5\n")
+    pts = C.POINTER(C.c_float)()
+    n = C.c_int()
+    assert dwg_lib.dwg_read_xyz(str(f).encode(), 1, C.byref(pts), None, C.byref(n)) == capi.DWG_ERR_INVALID
+    assert b"line 2" in dwg_lib.dwg_last_error()
+    f.write_text("1 2 nan\n")
+    assert dwg_lib.dwg_read_xyz(str(f).encode(), 1, C.byref(pts), None, C.byref(n)) == capi.DWG_ERR_INVALID
+    assert dwg_lib.dwg_read_xyz(b"/nonexistent/x.xyz", 1, C.byref(pts), None, C.byref(n)) == capi.DWG_ERR_INVALID
+
+
+def test_write_stl_binary_format(dwg_lib, tmp_path):
+    tris = np.array([[0, 0, 0, 1, 0, 0, 0, 1, 0], [0, 0, 0, 0, 0, 1, 1, 0, 0]], np.float32)
+    f = tmp_path / "m.stl"
+    assert dwg_lib.dwg_write_stl(str(f).encode(), tris.ctypes.data, 2) == 0
+    b = f.read_bytes()
+    assert len(b) == 80 + 4 + 2 * 50
+    assert struct.unpack("<I", b[80:84])[0] == 2
+    rec = struct.unpack("<12fH", b[84:134])
+    assert rec[:3] == (0.0, 0.0, 1.0)  # cross((1,0,0),(0,1,0))
+    assert rec[3:12] == tuple(tris[0])
+
+
+def test_write_xyz(dwg_lib, tmp_path):
+    P = np.array([[0.5, 1, 2]], np.float32)
+    N = np.array([[0, 0, 1]], np.float32)
+    f = tmp_path / "o.xyz"
+    assert dwg_lib.dwg_write_xyz(str(f).encode(), P.ctypes.data, N.ctypes.data, 1) == 0
+    assert [float(x) for x in f.read_text().split()] == [0.5, 1, 2, 0, 0, 1]

@@ -1,0 +1,243 @@
+"""GPU parity tests: every CUDA kernel against the CPU oracle on the same
+seeded inputs, called through the C ABI (ctypes)."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from dwg_b200 import capi, datasets as D, turbo  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+DEV = "cuda"
+
+
+def cu(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).to(DEV)
+
+
+def cloud(n=20000, kind="torus", seed=1):
+    if kind == "torus":
+        P, N = D.torus(n, seed=seed)
+    else:
+        P, N = D.sphere(n, seed=seed)
+    Pn, _, _ = D.normalize(P)
+    return Pn, N.astype(np.float32)
+
+
+def match_nodes(gpu, ot):
+    """map GPU node index -> oracle node index by (depth, first sorted point)"""
+    ost = ot.dfs_starts()
+    key = {(int(d), int(s)): i for i, (d, s, c) in enumerate(zip(ot.depth, ost, ot.counts)) if c > 0}
+    return np.array([key[(int(d), int(s))] for d, s in zip(gpu["depth"], gpu["pt_start"])])
+
+
+@pytest.fixture(scope="module")
+def torus_tree(dwg_lib, oracle_lib):
+    P, N = cloud(20000)
+    A = np.full(len(P), 2e-6, np.float32)
+    gt = turbo.TurboLibiGWN(cu(P), max_depth=8, areas=cu(A))
+    gt.UpdateMassNormals(cu(N), cu(A))
+    torch.cuda.synchronize()
+    ot = oracle_lib.Octree(P, 8)
+    return P, N, A, gt, ot
+
+
+def test_octree_topology_matches_octreeDWG(torus_tree):
+    P, N, A, gt, ot = torus_tree
+    g = gt.export()
+    # sorted point order == depth-first order of octreeDWG
+    assert np.array_equal(g["perm"], ot.dfs_order())
+    # same set of non-empty nodes with the same depth / point range / count
+    idx = match_nodes(g, ot)
+    assert len(idx) == int((ot.counts > 0).sum())
+    assert np.array_equal(g["pt_count"], ot.counts[idx])
+    # leaves are the same nodes
+    leaf_o = ot.children[idx, 0] == -1
+    leaf_g = (g["skip"] == np.arange(len(idx)) + 1)
+    assert np.array_equal(leaf_o, leaf_g)
+    # pre-order: every subtree is a contiguous node range
+    assert np.all(g["skip"] > np.arange(len(idx)))
+    assert g["skip"][0] == len(idx)
+
+
+def test_octree_moments_fp64(torus_tree):
+    P, N, A, gt, ot = torus_tree
+    g = gt.export()
+    idx = match_nodes(g, ot)
+    CM, R, EC = ot.moments(P, N, A)
+    assert np.allclose(g["cm"], CM[idx], rtol=0, atol=1e-14)
+    assert np.allclose(g["radius"], R[idx], rtol=0, atol=1e-14)
+    assert np.allclose(g["ec"], EC[idx], rtol=1e-12, atol=1e-18)
+
+
+def _oracle_gwn_with_gpu_moments(ot, g, idx, P, N, A, Q, **kw):
+    """oracle traversal fed the GPU's moments (so that the discrete opening
+    decisions are taken on identical float inputs)"""
+    M = ot.num_nodes
+    CM = np.zeros((M, 3))
+    R = np.zeros(M)
+    EC = np.zeros((M, 3))
+    CM[idx], R[idx], EC[idx] = g["cm"], g["radius"], g["ec"]
+    return ot.gwn(P, N, A, Q, moments=(CM, R, EC), **kw)
+
+
+@pytest.mark.parametrize("screened,sigma", [(True, 20.0), (True, 10.0), (False, 0.0)])
+@pytest.mark.parametrize("precision", [0, 1, 2])
+def test_gwn_points_same_sums_as_oracle(torus_tree, screened, sigma, precision, dwg_lib):
+    import ctypes as C
+    P, N, A, gt, ot = torus_tree
+    g = gt.export()
+    idx = match_nodes(g, ot)
+    rng = np.random.default_rng(7)
+    Q = np.concatenate([P[rng.choice(len(P), 3000, replace=False)],
+                        rng.uniform(-0.6, 0.6, (3000, 3)).astype(np.float32)])
+    w_ref, t_ref = _oracle_gwn_with_gpu_moments(ot, g, idx, P, N, A, Q, beta=2.3, sigma=sigma,
+                                                screened=screened)
+    out = torch.empty(len(Q), dtype=torch.float32, device=DEV)
+    terms = torch.empty(len(Q), dtype=torch.int32, device=DEV)
+    p = capi.gwn_params(beta=2.3, sigma=sigma, screened=screened, precision=precision)
+    capi.check(dwg_lib.dwg_gwn_points_counted(gt._h, None, None, None, capi.ptr(cu(Q)), len(Q), C.byref(p),
+                                              capi.ptr(out), capi.ptr(terms), None))
+    torch.cuda.synchronize()
+    assert gt.status() == 0
+    # identical opening decisions: the same number of terms per query
+    assert np.array_equal(terms.cpu().numpy(), t_ref)
+    w = out.cpu().numpy().astype(np.float64)
+    err = np.abs(w - w_ref)
+    scale = np.maximum(np.abs(w_ref), 1e-3 * np.abs(w_ref).max())
+    # FP32 terms vs FP64: relative error bound per precision mode
+    tol = {0: 2e-4, 1: 2e-5, 2: 2e-6}[precision]
+    assert np.max(err / scale) < tol, (precision, np.max(err / scale))
+
+
+def test_gwn_grid_matches_oracle(torus_tree, oracle_lib):
+    P, N, A, gt, ot = torus_tree
+    g = gt.export()
+    idx = match_nodes(g, ot)
+    res = np.array([21, 18, 13], np.int32)
+    org = np.array([-0.55, -0.5, -0.2], np.float32)
+    h = np.float32(0.05)
+    Q = oracle_lib.grid_points(res, org, h)
+    w_ref, _ = _oracle_gwn_with_gpu_moments(ot, g, idx, P, N, A, Q, beta=2.3, sigma=20.0, screened=True)
+    terms = torch.zeros(1, dtype=torch.int64, device=DEV)
+    w = gt.grid(res, org, h, beta=2.3, sigma=20.0, precision=1, terms=terms).cpu().numpy()
+    assert gt.status() == 0
+    assert np.max(np.abs(w - w_ref)) < 2e-5 * max(1e-3, np.abs(w_ref).max())
+    _, t_ref = _oracle_gwn_with_gpu_moments(ot, g, idx, P, N, A, Q, beta=2.3, sigma=20.0, screened=True)
+    assert int(terms.item()) == int(t_ref.sum())
+
+
+def test_marching_cubes_bit_exact(oracle_lib):
+    rng = np.random.default_rng(3)
+    res = np.array([37, 29, 33], np.int32)
+    org = np.array([-0.7, -0.5, -0.6], np.float32)
+    h = np.float32(0.037)
+    G = oracle_lib.grid_points(res, org, h)
+    f = np.zeros(len(G))
+    for _ in range(6):
+        c = rng.uniform(-0.5, 0.5, 3)
+        f += np.exp(-((G - c) ** 2).sum(1) / 0.02)
+    f = f.astype(np.float32)
+    iso = np.float32(0.37)
+    ref = oracle_lib.marching_cubes(f, res, org, h, iso)
+    T = ref["T"]
+    assert T > 1000
+    mc = turbo.TurboMC()
+    tris = torch.empty((T + 10, 9), dtype=torch.float32, device=DEV)
+    cen = torch.empty((T + 10, 3), dtype=torch.float32, device=DEV)
+    nrm = torch.empty((T + 10, 3), dtype=torch.float32, device=DEV)
+    n = mc.TurboMarchingCubes(cu(f), None, *res.tolist(), iso, mid_points=cen, mid_normals=nrm, tris=tris,
+                              origin=org, spacing=h, capacity=T + 10)
+    assert n == T
+    assert np.array_equal(tris[:T].cpu().numpy(), ref["tris"])
+    assert np.array_equal(cen[:T].cpu().numpy(), ref["centroids"])
+    assert np.array_equal(nrm[:T].cpu().numpy(), ref["normals"])
+
+
+def test_marching_cubes_overflow_reported(oracle_lib, dwg_lib):
+    import ctypes as C
+    res = np.array([16, 16, 16], np.int32)
+    org = np.zeros(3, np.float32)
+    G = oracle_lib.grid_points(res, org, np.float32(1 / 15))
+    f = (0.4 - np.linalg.norm(G - 0.5, axis=1)).astype(np.float32)
+    T_ref = oracle_lib.marching_cubes(f, res, org, np.float32(1 / 15), 0.0)["T"]
+    cap = T_ref // 2
+    cen = torch.empty((cap, 3), dtype=torch.float32, device=DEV)
+    T = C.c_longlong()
+    rc = dwg_lib.dwg_marching_cubes(capi.ptr(cu(f)), res.ctypes.data, None, org.ctypes.data, float(1 / 15), 0.0,
+                                    None, capi.ptr(cen), None, cap, None, C.byref(T), None)
+    assert rc == capi.DWG_ERR_OVERFLOW and T.value == T_ref
+
+
+def test_knn_matches_bruteforce_with_ties(oracle_lib):
+    rng = np.random.default_rng(4)
+    P = (rng.integers(0, 12, (3000, 3)) * 0.01).astype(np.float32)  # lattice: exact ties
+    Q = np.concatenate([(rng.integers(0, 12, (500, 3)) * 0.01 + 0.005).astype(np.float32),
+                        rng.uniform(-0.05, 0.16, (500, 3)).astype(np.float32)])
+    for k in (1, 10, 15, 16, 20, 64):
+        ref = oracle_lib.knn(P, Q, k)
+        ix = turbo.KnnIndex(cu(P))
+        got = ix.query(cu(Q), k).cpu().numpy()
+        assert np.array_equal(got, ref), k
+
+
+def test_knn_surface_cloud(oracle_lib):
+    P, _ = cloud(20000)
+    rng = np.random.default_rng(5)
+    Q = P[rng.choice(len(P), 2000, replace=False)] + rng.normal(0, 0.003, (2000, 3)).astype(np.float32)
+    ref = oracle_lib.knn(P, Q, 15)
+    got = turbo.KnnIndex(cu(P)).query(cu(Q), 15).cpu().numpy()
+    assert np.array_equal(got, ref)
+
+
+def test_diffusion_and_zero_repair_bit_exact(oracle_lib, dwg_lib):
+    import ctypes as C
+    rng = np.random.default_rng(6)
+    L, T, k = 4000, 9000, 15
+    Lpos = rng.uniform(-0.5, 0.5, (L, 3)).astype(np.float32)
+    knn = rng.integers(0, L // 2, (T, k)).astype(np.int32)  # upper half never hit -> zero normals
+    tn = rng.standard_normal((T, 3)).astype(np.float32)
+    tn /= np.linalg.norm(tn, axis=1, keepdims=True)
+    N0 = rng.standard_normal((L, 3)).astype(np.float32)
+    ref_n, ref_z, ref_c = oracle_lib.diffuse_normals(knn, tn, N0)
+    n_dev = cu(N0)
+    isz = torch.zeros(L, dtype=torch.uint8, device=DEV)
+    zc = torch.zeros(1, dtype=torch.int32, device=DEV)
+    capi.check(dwg_lib.dwg_diffuse_normals(capi.ptr(cu(knn)), capi.ptr(cu(tn)), T, k, L, capi.ptr(n_dev),
+                                           capi.ptr(isz), capi.ptr(zc), None))
+    torch.cuda.synchronize()
+    assert int(zc.item()) == ref_c and ref_c > 10
+    assert np.array_equal(isz.cpu().numpy().astype(bool), ref_z)
+    assert np.array_equal(n_dev.cpu().numpy(), ref_n)
+    rep = oracle_lib.zero_repair(Lpos, ref_n, ref_z, 10)
+    ix = turbo.KnnIndex(cu(Lpos))
+    capi.check(dwg_lib.dwg_zero_repair(ix._h, capi.ptr(n_dev), capi.ptr(isz), capi.ptr(zc), 10, 10, None))
+    torch.cuda.synchronize()
+    assert np.array_equal(n_dev.cpu().numpy(), rep)
+
+
+def test_gauss_map_load_normals_radii_bit_exact(oracle_lib, dwg_lib):
+    P, _ = cloud(5000, kind="sphere")
+    out = torch.empty((len(P), 3), dtype=torch.float32, device=DEV)
+    turbo.TurboNormalInitialization().GaussMapInit(cu(P), out)
+    torch.cuda.synchronize()
+    assert np.array_equal(out.cpu().numpy(), oracle_lib.gauss_map(P))
+    nb = oracle_lib.knn(P, P, 10)
+    got = torch.empty(len(P), dtype=torch.float32, device=DEV)
+    capi.check(dwg_lib.dwg_radii(capi.ptr(cu(P)), len(P), capi.ptr(cu(nb)), 10, capi.ptr(got), None))
+    torch.cuda.synchronize()
+    assert np.array_equal(got.cpu().numpy(), oracle_lib.radii(P, nb))
+    LN = oracle_lib.gauss_map(P)
+    ln = torch.empty((len(P), 3), dtype=torch.float32, device=DEV)
+    capi.check(dwg_lib.dwg_load_normals(capi.ptr(cu(nb)), 10, len(P), capi.ptr(cu(LN)), capi.ptr(ln), None))
+    torch.cuda.synchronize()
+    assert np.array_equal(ln.cpu().numpy(), oracle_lib.load_normals(nb, LN))
+
+
+def test_voxel_grid_matches_oracle(oracle_lib):
+    P, _ = cloud(3000)
+    for s in (16, 128, 257):
+        res, org, h = turbo.voxel_grid(cu(P), 0.05, s)
+        r2, o2, h2 = oracle_lib.voxel_grid(P, 0.05, s)
+        assert np.array_equal(res, r2) and np.array_equal(org, o2) and h == h2

@@ -1,0 +1,79 @@
+"""GPU pipeline (full DWG reconstruction) against the oracle's reconstruction
+on the same seeded cloud; and size-independent properties at larger sizes."""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+from dwg_b200 import datasets as D, turbo  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def cu(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+SMALL = dict(grid_reso=40, final_reso=40, total_iter=6, max_depth=7)
+
+
+@pytest.fixture(scope="module")
+def small_runs(oracle_lib):
+    P, N = D.sphere(3000, noise=0.002, seed=11)
+    Pn, _, _ = D.normalize(P)
+    ref = oracle_lib.reconstruct(Pn, **SMALL)
+    got = turbo.reconstruct(cu(Pn), **SMALL)
+    return Pn, ref, got
+
+
+def test_pipeline_leaves_identical(small_runs):
+    Pn, ref, got = small_runs
+    assert np.array_equal(got["leaf_pos"], ref["leaf_pos"])
+
+
+def test_pipeline_iso_and_counts_track_oracle(small_runs):
+    Pn, ref, got = small_runs
+    # FP32-compensated sums vs FP64: iso values agree to ~1e-6 relative
+    assert np.allclose(got["iso"], ref["iso"], rtol=1e-4, atol=1e-9)
+    # triangle counts: identical unless a grid value sits within rounding of the iso
+    assert np.all(np.abs(got["tri_count"] - ref["tri_count"]) <= 0.002 * ref["tri_count"] + 4)
+
+
+def test_pipeline_normals_agree_with_oracle(small_runs):
+    Pn, ref, got = small_runs
+    agree = np.sign((got["leaf_nrm"] * ref["leaf_nrm"]).sum(1))
+    assert agree.mean() > 0.99
+    pa = np.sign((got["point_nrm"] * ref["point_nrm"]).sum(1))
+    assert pa.mean() > 0.99
+
+
+def test_pipeline_mesh_close_to_oracle(small_runs):
+    Pn, ref, got = small_runs
+    a = got["tris"].reshape(-1, 3, 3).mean(1)
+    b = ref["tris"].reshape(-1, 3, 3).mean(1)
+    assert abs(len(a) - len(b)) <= 0.01 * len(b) + 4
+    from scipy.spatial import cKDTree
+    d1 = cKDTree(b).query(a)[0]
+    d2 = cKDTree(a).query(b)[0]
+    chamfer = d1.mean() + d2.mean()
+    h = 1.1 / 39
+    assert chamfer < 0.05 * h
+
+
+def test_pipeline_graph_replay_equals_eager(oracle_lib):
+    P, _ = D.torus(4000, seed=2)
+    Pn, _, _ = D.normalize(P)
+    a = turbo.reconstruct(cu(Pn), use_graph=1, **SMALL)
+    b = turbo.reconstruct(cu(Pn), use_graph=0, **SMALL)
+    for k in ("leaf_nrm", "iso", "tri_count", "zero_count", "tris", "point_nrm"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_pipeline_input_normals_mode(oracle_lib):
+    P, N = D.torus(4000, seed=3)
+    Pn, _, _ = D.normalize(P)
+    cfg = dict(SMALL, in_normal=1, total_iter=2)
+    ref = oracle_lib.reconstruct(Pn, normals=N, **cfg)
+    got = turbo.reconstruct(cu(Pn), cu(N), **cfg)
+    assert np.array_equal(got["leaf_pos"], ref["leaf_pos"])
+    assert np.allclose(got["iso"], ref["iso"], rtol=1e-4, atol=1e-9)
