@@ -17,21 +17,42 @@ constexpr int kGwnWarps = 8;
 constexpr int kGwnStack = 8 * (kMaxDepth + 1) + 8;
 constexpr float kFourPi = 12.566370614359172f;
 
+// MUFU approximations without the subnormal fix-up paths
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ex2_ftz(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_ftz(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// One term of the sum for offset (dx,dy,dz) = p - q and d = A (p - q).n.
+// Screened (src/TurboLibiGWN.cu:530-584): rho = max(|p-q|, s),
+// v = (sigma rho + 1) d / (e^{sigma rho} 4 pi rho^3 + 1e-7) with the sign of d,
+// skipped when |p-q| <= 1e-10.  Plain (:351-360): v = d / (4 pi |p-q|^3 + 1e-8).
+// PREC < 2 uses the MUFU approximations (sigma_l2e = sigma log2 e);
+// PREC 2 uses correctly rounded sqrt / division and expf.
 template <bool SCREENED, int PREC>
 __device__ __forceinline__ bool gwn_term(float dx, float dy, float dz, float d, float s, float sigma,
-                                         float& v) {
-    float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                                         float sigma_l2e, float& v) {
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
     if (SCREENED) {
-        float r = (PREC >= 2) ? sqrtf(r2) : r2 * rsqrtf(r2);
-        if (!(r > 1e-10f)) return false;
-        float rho = fmaxf(r, s);
-        float sr = sigma * rho;
-        float e = (PREC >= 2) ? expf(sr) : __expf(sr);
-        float r3 = rho * rho * rho;
-        float den = fmaf(e, kFourPi * r3, 1e-7f);
-        float num = fmaf(sigma, rho, 1.0f) * d;
-        float res = (PREC >= 2) ? __fdiv_rn(num, den) : __fdividef(num, den);
-        // sign of d = A (p - q).n, src/TurboLibiGWN.cu:550-584
+        if (!(r2 > 1e-20f)) return false;  // |p - q| <= 1e-10
+        const float r = (PREC >= 2) ? sqrtf(r2) : r2 * rsqrt_ftz(r2);
+        const float rho = fmaxf(r, s);
+        const float e = (PREC >= 2) ? expf(sigma * rho) : ex2_ftz(rho * sigma_l2e);
+        const float r3 = rho * rho * rho;
+        const float den = fmaf(e, kFourPi * r3, 1e-7f);
+        const float num = fmaf(sigma, rho, 1.0f) * d;
+        const float res = (PREC >= 2) ? __fdiv_rn(num, den) : num * rcp_ftz(den);
         v = copysignf(fabsf(res), d);
         return true;
     } else {
@@ -39,9 +60,9 @@ __device__ __forceinline__ bool gwn_term(float dx, float dy, float dz, float d, 
             v = 0.0f;
             return true;
         }
-        float r = (PREC >= 2) ? sqrtf(r2) : r2 * rsqrtf(r2);
-        float den = fmaf(kFourPi * r, r2, 1e-8f);
-        v = (PREC >= 2) ? __fdiv_rn(d, den) : __fdividef(d, den);
+        const float r = (PREC >= 2) ? sqrtf(r2) : r2 * rsqrt_ftz(r2);
+        const float den = fmaf(kFourPi * r, r2, 1e-8f);
+        v = (PREC >= 2) ? __fdiv_rn(d, den) : d * rcp_ftz(den);
         return true;
     }
 }
@@ -62,8 +83,9 @@ __device__ __forceinline__ void acc_add(float& s, float& c, float v) {
 
 struct GwnArgs {
     const int4* __restrict__ info;
-    const float4* __restrict__ cmr;
-    const float4* __restrict__ ec;
+    const float4* __restrict__ node_a;
+    const float4* __restrict__ node_b;
+    const float* __restrict__ node_r;
     const float4* __restrict__ pa;
     const float4* __restrict__ nr;
     float beta, sigma, screen;
@@ -83,12 +105,13 @@ struct GwnArgs {
 };
 
 template <bool GRID, bool SCREENED, int PREC>
-__global__ void __launch_bounds__(kGwnWarps * 32) k_gwn(GwnArgs a) {
+__global__ void __launch_bounds__(kGwnWarps * 32, 4) k_gwn(GwnArgs a) {
     __shared__ int2 stack[kGwnWarps][kGwnStack];
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
     const float sigma = a.sigma_dev ? *a.sigma_dev : a.sigma;
+    const float sigma_l2e = sigma * 1.4426950408889634f;
     unsigned long long my_terms = 0;
     for (;;) {
         unsigned g = 0;
@@ -130,7 +153,7 @@ __global__ void __launch_bounds__(kGwnWarps * 32) k_gwn(GwnArgs a) {
                 float d = p.w * fmaf(dx, nn.x, fmaf(dy, nn.y, dz * nn.z));
                 float sc = a.use_radii ? nn.w : a.screen;
                 float v;
-                if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, sc, sigma, v)) {
+                if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, sc, sigma, sigma_l2e, v)) {
                     acc_add<PREC>(s, c, v);
                     ++nterm;
                 }
@@ -154,35 +177,55 @@ __global__ void __launch_bounds__(kGwnWarps * 32) k_gwn(GwnArgs a) {
                 continue;
             }
             const bool act = (((unsigned)e.y) >> lane) & 1u;
-            const int end = a.info[e.x].z;
+            const int end = __float_as_int(a.node_b[e.x].w) & kMetaSkip;
             int ch = e.x + 1;
             while (ch < end) {
-                const int4 ic = a.info[ch];
+                const float4 na = a.node_a[ch];
+                const float4 nb = a.node_b[ch];
+                const int meta = __float_as_int(nb.w);
+                const int next = meta & kMetaSkip;
                 // structural guard: a child's subtree ends after it and within
-                // its parent's; a leaf's points lie inside the point array
-                if (ic.z <= ch || ic.z > end || end > a.num_nodes) {
+                // its parent's
+                if (next <= ch || next > end || end > a.num_nodes) {
                     if (lane == 0) atomicOr(&a.work[1], 2u);
                     break;
                 }
-                if (ic.w & kLeafFlag) {
-                    if (ic.x < 0 || ic.y < 0 || ic.x + ic.y > a.num_points) {
-                        if (lane == 0) atomicOr(&a.work[1], 4u);
-                    } else if (act) {
-                        leaf_points(ic.x, ic.y);
+                if (meta & kMetaLeaf) {
+                    if ((meta & kMetaSingle) && !a.use_radii) {
+                        // one point: its term is the node's (cm = p, ec = A n)
+                        if (act) {
+                            const float dx = na.x - qx, dy = na.y - qy, dz = na.z - qz;
+                            const float d = fmaf(dx, nb.x, fmaf(dy, nb.y, dz * nb.z));
+                            float v;
+                            if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, a.screen, sigma, sigma_l2e, v)) {
+                                acc_add<PREC>(s, c, v);
+                                ++nterm;
+                            }
+                        }
+                    } else {
+                        const int4 ic = a.info[ch];
+                        if (ic.x < 0 || ic.y < 0 || ic.x + ic.y > a.num_points) {
+                            if (lane == 0) atomicOr(&a.work[1], 4u);
+                        } else if (act) {
+                            leaf_points(ic.x, ic.y);
+                        }
                     }
                 } else {
                     bool near = false;
                     if (act) {
-                        const float4 cm = a.cmr[ch];
-                        // opening test in round-to-nearest single precision
-                        // (src/TurboLibiGWN.cu:636-644)
-                        float dx = __fsub_rn(cm.x, qx), dy = __fsub_rn(cm.y, qy), dz = __fsub_rn(cm.z, qz);
-                        float dist = __fsqrt_rn(sq3_rn(dx, dy, dz));
-                        if (dist > __fmul_rn(a.beta, cm.w)) {
-                            const float4 m = a.ec[ch];
-                            float d = fmaf(dx, m.x, fmaf(dy, m.y, dz * m.z));
+                        // opening test sqrt_rn(d2) > beta*R, d2 in round-to-nearest
+                        // single precision (src/TurboLibiGWN.cu:636-644), as a
+                        // comparison of d2 with the node's exact threshold
+                        const float dx = __fsub_rn(na.x, qx), dy = __fsub_rn(na.y, qy), dz = __fsub_rn(na.z, qz);
+                        const float d2 = sq3_rn(dx, dy, dz);
+                        const float thr = fabsf(na.w);
+                        bool far = d2 > thr;
+                        if (!far && d2 == thr && signbit(na.w))
+                            far = __fsqrt_rn(d2) > __fmul_rn(a.beta, a.node_r[ch]);
+                        if (far) {
+                            const float d = fmaf(dx, nb.x, fmaf(dy, nb.y, dz * nb.z));
                             float v;
-                            if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, a.screen, sigma, v)) {
+                            if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, a.screen, sigma, sigma_l2e, v)) {
                                 acc_add<PREC>(s, c, v);
                                 ++nterm;
                             }
@@ -200,7 +243,7 @@ __global__ void __launch_bounds__(kGwnWarps * 32) k_gwn(GwnArgs a) {
                         }
                     }
                 }
-                ch = ic.z;
+                ch = next;
             }
         }
         if (valid) {
@@ -251,8 +294,10 @@ int gwn_eval(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, float*
     DWG_REQUIRE(out != nullptr, "gwn: output is null");
     GwnArgs a;
     a.info = t.info.ptr;
-    a.cmr = t.cmr.ptr;
-    a.ec = t.ec.ptr;
+    DWG_TRY(octree_set_beta(const_cast<Octree&>(t), p.beta, s));
+    a.node_a = t.node_a.ptr;
+    a.node_b = t.node_b.ptr;
+    a.node_r = t.node_r.ptr;
     a.pa = t.pa.ptr;
     a.nr = t.nr.ptr;
     a.beta = p.beta;

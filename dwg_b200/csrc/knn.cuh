@@ -15,6 +15,10 @@ struct KnnIndex {
     DevBuf<int> cell_fill;
     DevBuf<float> bbox;
     DevBuf<unsigned char> scratch;
+    // query bucketing workspace (grown on demand; not thread safe)
+    int morton_shift = 0;
+    mutable DevBuf<int> q_key, q_order, q_hist, q_fill;
+    mutable DevBuf<unsigned char> q_scratch;
 };
 
 int knn_build(KnnIndex& ix, const float* points_dev, int n, cudaStream_t s);

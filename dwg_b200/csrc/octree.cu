@@ -219,7 +219,7 @@ __device__ __forceinline__ double warp_max_d(double v) {
 
 __global__ void k_centres(const int4* __restrict__ info, const float4* __restrict__ pa, int M,
                           double* __restrict__ cm_d, double* __restrict__ r_d,
-                          float4* __restrict__ cmr) {
+                          float4* __restrict__ node_a, float* __restrict__ node_r) {
     const int lane = threadIdx.x & 31;
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
@@ -255,48 +255,76 @@ __global__ void k_centres(const int4* __restrict__ info, const float4* __restric
             cm_d[v * 3 + 1] = cy;
             cm_d[v * 3 + 2] = cz;
             r_d[v] = rm;
-            cmr[v] = make_float4((float)cx, (float)cy, (float)cz, (float)rm);
+            node_a[v] = make_float4((float)cx, (float)cy, (float)cz, 0.f);
+            node_r[v] = (float)rm;
         }
     }
 }
 
-__global__ void k_ec(const int4* __restrict__ info, const float4* __restrict__ pa,
-                     const float4* __restrict__ nr, int M, double* __restrict__ ec_d,
-                     float4* __restrict__ ec) {
-    const int lane = threadIdx.x & 31;
-    const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
-    const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-    for (long long v = warp; v < M; v += nwarps) {
-        int4 iv = info[v];
-        double ex = 0, ey = 0, ez = 0;
-        if (iv.y <= 32) {
-            if (lane < iv.y) {
-                float4 p = pa[iv.x + lane];
-                float4 q = nr[iv.x + lane];
-                double a = p.w;
-                ex = a * (double)q.x;
-                ey = a * (double)q.y;
-                ez = a * (double)q.z;
-            }
-        } else {
-            for (int j = iv.x + lane; j < iv.x + iv.y; j += 32) {
-                float a = pa[j].w;
-                float4 q = nr[j];
-                ex += (double)a * (double)q.x;
-                ey += (double)a * (double)q.y;
-                ez += (double)a * (double)q.z;
-            }
+// sum A n per node, bottom-up one depth level at a time: a leaf sums its
+// points, an internal node its children (in octant order) -- every node's sum
+// has a fixed order, so the result is the same from run to run
+__global__ void k_ec_level(const int* __restrict__ nodes, int count, const int4* __restrict__ info,
+                           const float4* __restrict__ pa, const float4* __restrict__ nr,
+                           double* __restrict__ ec_d, float4* __restrict__ node_b) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int v = nodes[i];
+    const int4 iv = info[v];
+    double ex = 0, ey = 0, ez = 0;
+    if (iv.w & kLeafFlag) {
+        for (int j = iv.x; j < iv.x + iv.y; ++j) {
+            const double a = pa[j].w;
+            const float4 q = nr[j];
+            ex += a * (double)q.x;
+            ey += a * (double)q.y;
+            ez += a * (double)q.z;
         }
-        ex = warp_sum_d(ex);
-        ey = warp_sum_d(ey);
-        ez = warp_sum_d(ez);
-        if (lane == 0) {
-            ec_d[v * 3] = ex;
-            ec_d[v * 3 + 1] = ey;
-            ec_d[v * 3 + 2] = ez;
-            ec[v] = make_float4((float)ex, (float)ey, (float)ez, 0.f);
+    } else {
+        for (int c = v + 1; c < iv.z; c = info[c].z) {
+            ex += ec_d[(size_t)c * 3];
+            ey += ec_d[(size_t)c * 3 + 1];
+            ez += ec_d[(size_t)c * 3 + 2];
         }
     }
+    ec_d[(size_t)v * 3] = ex;
+    ec_d[(size_t)v * 3 + 1] = ey;
+    ec_d[(size_t)v * 3 + 2] = ez;
+    int meta = iv.z | ((iv.w & kLeafFlag) ? kMetaLeaf : 0) | (((iv.w & kLeafFlag) && iv.y == 1) ? kMetaSingle : 0);
+    node_b[v] = make_float4((float)ex, (float)ey, (float)ez, __int_as_float(meta));
+}
+
+// Open threshold of a node for opening ratio beta: with t = beta*R rounded,
+// sqrt_rn(d2) > t  <=>  d2 > B, B = (t + ulp(t)/2)^2 (exact in FP64), except
+// d2 == B, which rounds half to even and is decided by the exact test.  The
+// float stored is B rounded down, negated when B is itself a float.
+__global__ void k_node_thr(const float* __restrict__ node_r, int M, float beta, float4* __restrict__ node_a) {
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= M) return;
+    const float t = __fmul_rn(beta, node_r[v]);
+    float thr;
+    if (t == 0.f) {
+        thr = -0.0f;  // every d2 > 0 is far; d2 == 0 takes the exact test
+    } else {
+        const double hulp = ((double)nextafterf(t, INFINITY) - (double)t) * 0.5;
+        const double b = ((double)t + hulp) * ((double)t + hulp);
+        const float bf = __double2float_rd(b);
+        thr = ((double)bf == b) ? -bf : bf;
+    }
+    float4 a = node_a[v];
+    a.w = thr;
+    node_a[v] = a;
+}
+
+__global__ void k_depth_hist(const int4* __restrict__ info, int M, int* __restrict__ hist) {
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < M) atomicAdd(&hist[info[v].w & 0xff], 1);
+}
+
+__global__ void k_depth_scatter(const int4* __restrict__ info, int M, int* __restrict__ fill,
+                                int* __restrict__ nodes) {
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v < M) nodes[atomicAdd(&fill[info[v].w & 0xff], 1)] = v;
 }
 
 // ---------------------------------------------------------- leaf centres --
@@ -415,20 +443,40 @@ int octree_build(Octree& t, const float* P, int n, int D, const float* A, cudaSt
                                                       t.info.ptr);
         DWG_CHECK_LAUNCH();
     }
+    {
+        DevBuf<int> hist, fill;
+        DWG_TRY(hist.reserve(kMaxDepth + 2));
+        DWG_TRY(fill.reserve(kMaxDepth + 2));
+        DWG_TRY(t.level_nodes.reserve(M));
+        DWG_CHECK_CUDA(cudaMemsetAsync(hist.ptr, 0, sizeof(int) * (kMaxDepth + 2), s));
+        k_depth_hist<<<div_up(M, 256), 256, 0, s>>>(t.info.ptr, M, hist.ptr);
+        DWG_CHECK_LAUNCH();
+        int h[kMaxDepth + 2];
+        DWG_CHECK_CUDA(cudaMemcpyAsync(h, hist.ptr, sizeof(h), cudaMemcpyDeviceToHost, s));
+        DWG_CHECK_CUDA(cudaStreamSynchronize(s));
+        t.level_off[0] = 0;
+        for (int d = 0; d <= kMaxDepth; ++d) t.level_off[d + 1] = t.level_off[d] + (d <= D ? h[d] : 0);
+        DWG_CHECK_CUDA(cudaMemcpyAsync(fill.ptr, t.level_off, sizeof(int) * (kMaxDepth + 1), cudaMemcpyHostToDevice, s));
+        k_depth_scatter<<<div_up(M, 256), 256, 0, s>>>(t.info.ptr, M, fill.ptr, t.level_nodes.ptr);
+        DWG_CHECK_LAUNCH();
+        DWG_CHECK_CUDA(cudaStreamSynchronize(s));
+    }
     DWG_TRY(t.pa.reserve(n));
     DWG_TRY(t.nr.reserve(n));
     k_gather<<<div_up(n, 256), 256, 0, s>>>(P, A, t.perm.ptr, n, t.pa.ptr, t.nr.ptr, t.inv_perm.ptr);
     DWG_CHECK_LAUNCH();
-    DWG_TRY(t.cmr.reserve(M));
-    DWG_TRY(t.ec.reserve(M));
+    DWG_TRY(t.node_a.reserve(M));
+    DWG_TRY(t.node_b.reserve(M));
+    DWG_TRY(t.node_r.reserve(M));
     DWG_TRY(t.cm_d.reserve((size_t)M * 3));
     DWG_TRY(t.r_d.reserve(M));
     DWG_TRY(t.ec_d.reserve((size_t)M * 3));
     DWG_TRY(t.work.reserve(2));
     DWG_CHECK_CUDA(cudaMemsetAsync(t.work.ptr, 0, 2 * sizeof(unsigned int), s));
-    DWG_CHECK_CUDA(cudaMemsetAsync(t.ec.ptr, 0, sizeof(float4) * M, s));
+    DWG_CHECK_CUDA(cudaMemsetAsync(t.node_b.ptr, 0, sizeof(float4) * M, s));
     DWG_CHECK_CUDA(cudaMemsetAsync(t.ec_d.ptr, 0, sizeof(double) * 3 * M, s));
     DWG_TRY(octree_update_centres(t, s));
+    DWG_TRY(octree_update_normals(t, s));  // fills the node meta words
     return DWG_OK;
 }
 
@@ -453,13 +501,28 @@ static unsigned moment_blocks(int M) {
 }
 
 int octree_update_centres(Octree& t, cudaStream_t s) {
-    k_centres<<<moment_blocks(t.M), 256, 0, s>>>(t.info.ptr, t.pa.ptr, t.M, t.cm_d.ptr, t.r_d.ptr, t.cmr.ptr);
+    k_centres<<<moment_blocks(t.M), 256, 0, s>>>(t.info.ptr, t.pa.ptr, t.M, t.cm_d.ptr, t.r_d.ptr, t.node_a.ptr,
+                                                  t.node_r.ptr);
     DWG_CHECK_LAUNCH();
+    t.thr_beta = -1.f;
+    return DWG_OK;
+}
+
+int octree_set_beta(Octree& t, float beta, cudaStream_t s) {
+    if (t.thr_beta == beta) return DWG_OK;
+    k_node_thr<<<div_up(t.M, 256), 256, 0, s>>>(t.node_r.ptr, t.M, beta, t.node_a.ptr);
+    DWG_CHECK_LAUNCH();
+    t.thr_beta = beta;
     return DWG_OK;
 }
 
 int octree_update_normals(Octree& t, cudaStream_t s) {
-    k_ec<<<moment_blocks(t.M), 256, 0, s>>>(t.info.ptr, t.pa.ptr, t.nr.ptr, t.M, t.ec_d.ptr, t.ec.ptr);
+    for (int d = t.max_depth; d >= 0; --d) {
+        int cnt = t.level_off[d + 1] - t.level_off[d];
+        if (cnt <= 0) continue;
+        k_ec_level<<<div_up(cnt, 128), 128, 0, s>>>(t.level_nodes.ptr + t.level_off[d], cnt, t.info.ptr, t.pa.ptr,
+                                                     t.nr.ptr, t.ec_d.ptr, t.node_b.ptr);
+    }
     DWG_CHECK_LAUNCH();
     return DWG_OK;
 }

@@ -7,9 +7,13 @@
 //     perm[i] = input index of sorted point i
 //   nodes, depth-first pre-order (a node's subtree is contiguous and its first
 //   child, if any, is the next node):
-//     info[v] = (pt_start, pt_count, skip, depth | LEAF)   int4
-//     cmr[v]  = (cm.x, cm.y, cm.z, R)                    float4 (rounded FP64)
-//     ec[v]   = (sum A n .x, .y, .z, 0)                  float4 (rounded FP64)
+//     info[v]   = (pt_start, pt_count, skip, depth | LEAF)     int4
+//     node_a[v] = (cm.x, cm.y, cm.z, open threshold)          float4
+//     node_b[v] = (sum A n .x, .y, .z, meta)                  float4
+//     node_r[v] = R (max |p - cm|, rounded from FP64)         float
+//   meta = skip | LEAF_BIT | SINGLE_BIT (a leaf holding one point); the open
+//   threshold is the largest float T with sqrt_rn(d2) > beta*R <=> d2 > T for
+//   every float d2 != T, its sign bit set when d2 == T needs the exact test.
 //   skip[v] = index of the first node after v's subtree, so the children of v
 //   are v+1, skip[v+1], skip[skip[v+1]], ... while < skip[v].
 // Empty octants are not stored (the reference skips them at
@@ -22,6 +26,9 @@ namespace dwg {
 
 constexpr int kLeafFlag = 1 << 8;
 constexpr int kMaxDepth = 21;
+constexpr int kMetaSkip = (1 << 29) - 1;
+constexpr int kMetaLeaf = 1 << 29;
+constexpr int kMetaSingle = 1 << 30;
 
 struct Octree {
     int n = 0;
@@ -34,8 +41,13 @@ struct Octree {
     DevBuf<int> inv_perm;             // input -> sorted
     DevBuf<float4> pa, nr;
     DevBuf<int4> info;
-    DevBuf<float4> cmr, ec;
+    DevBuf<float4> node_a, node_b;
+    DevBuf<float> node_r;
+    float thr_beta = -1.f;  // beta the open thresholds were computed for (-1: none)
     DevBuf<double> cm_d, r_d, ec_d;
+    // node ids grouped by depth (level d = level_nodes[level_off[d] .. level_off[d+1]))
+    DevBuf<int> level_nodes;
+    int level_off[kMaxDepth + 2] = {0};
     DevBuf<unsigned char> scratch;  // CUB temporary storage
     mutable DevBuf<unsigned int> work;  // [0] work counter of the persistent GWN kernel, [1] error flag
 };
@@ -51,6 +63,8 @@ int octree_set_sorted_normals(Octree& t, const float* normals_sorted_dev, cudaSt
 int octree_update_centres(Octree& t, cudaStream_t s);
 // FP64 sum A n from pa.w and nr.xyz
 int octree_update_normals(Octree& t, cudaStream_t s);
+// open thresholds for the opening ratio beta (no-op when already current)
+int octree_set_beta(Octree& t, float beta, cudaStream_t s);
 // node centre of every node at the octreeDWG recursion (FP64), for leaf extraction
 int octree_leaf_centres(Octree& t, int min_count, DevBuf<float>& out_xyz, DevBuf<int>& out_node,
                         int* num_leaves, cudaStream_t s);
