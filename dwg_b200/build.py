@@ -17,6 +17,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libdwg_b200.so")
+CLI_SRC = os.path.join(HERE, "cli", "dwg_cuda.cpp")
+CLI = os.path.join(HERE, "bin", "DWG_CUDA")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [
@@ -82,7 +84,21 @@ def build(force: bool = False, jobs: int = 0, verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    build_cli(force)
     return LIB
+
+
+def build_cli(force: bool = False) -> str:
+    """DWG_CUDA command line tool, linked against libdwg_b200.so (rpath $ORIGIN/..)."""
+    os.makedirs(os.path.dirname(CLI), exist_ok=True)
+    deps = [CLI_SRC, LIB] + headers()
+    if force or _stale(CLI, deps):
+        cmd = [nvcc(), "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"), CLI_SRC, "-o", CLI,
+               "-L" + HERE, "-ldwg_b200", "-Xlinker", "-rpath,$ORIGIN/.."]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"DWG_CUDA build failed:\n{r.stdout}\n{r.stderr}")
+    return CLI
 
 
 def main():
