@@ -64,6 +64,7 @@ _SIGS = {
     "dwg_voxel_grid": (_i, [_vp, _i, _f, _i, _vp, _vp, _vp, _vp]),
     "dwg_marching_cubes": (_i, [_vp, _vp, _vp, _vp, _f, _f, _vp, _vp, _vp, _ll, _vp, _vp, _vp]),
     "dwg_mc_tables": (_i, [_vp, _vp]),
+    "dwg_marching_cubes_noalloc": (_i, [_vp, _vp, _vp, _vp, _f, _f, _vp, _vp, _vp, _ll, _vp, _vp]),
     "dwg_knn_build": (_i, [_vp, _i, _vp, C.POINTER(_vp)]),
     "dwg_knn_destroy": (_i, [_vp]),
     "dwg_knn_query": (_i, [_vp, _vp, _ll, _i, _vp, _vp]),

@@ -16,6 +16,8 @@
 // The case table is generated (mc_tables_host), not transcribed.
 #include <cub/cub.cuh>
 
+#include <mutex>
+
 #include "mc.cuh"
 
 namespace dwg {
@@ -343,3 +345,121 @@ int mc_run(const float* field, const McGrid& g, float iso, const float* iso_dev,
 }
 
 }  // namespace dwg
+
+// ----------------------------------------------------------------------------
+// Marching cubes without any device allocation.
+//
+// Some callers cannot allocate device memory when they mesh: a host that is
+// recording a CUDA graph in global capture mode (cudaMalloc is not permitted
+// while such a capture is open), a real-time loop that must not allocate after
+// start-up, or an application that owns every byte of device memory through
+// its own pool.  dwg_marching_cubes_noalloc serves them with the same two
+// kernels as dwg_marching_cubes; its scratch (per-block triangle counts, their
+// offsets and the total) lives in the file-scope device array below, which
+// every GPU that loads this library holds until the process exits.
+// ----------------------------------------------------------------------------
+namespace dwg {
+
+// 2^19 blocks of 256 cells: grids up to 134,217,728 cells (e.g. 512^3)
+constexpr long long kMcNoAllocMaxBlocks = 1ll << 19;
+constexpr long long kMcNoAllocMaxCells = kMcNoAllocMaxBlocks * kMcThreads;
+// [0, max) block counts, [max, 2 max) block offsets, then the 64-bit total
+static __device__ __align__(256) unsigned int g_mc_noalloc_scratch[2 * kMcNoAllocMaxBlocks + 64];
+
+// exclusive scan of the block counts by one block, in chunks, with a carry;
+// writes every offset and the total, so no slot has to start at zero
+constexpr int kMcScanThreads = 1024;
+__global__ void __launch_bounds__(kMcScanThreads)
+    k_mc_noalloc_scan(const unsigned int* __restrict__ counts, unsigned int* __restrict__ offs, long long nb,
+                      unsigned long long* __restrict__ total) {
+    typedef cub::BlockScan<unsigned long long, kMcScanThreads> BS;
+    __shared__ typename BS::TempStorage tmp;
+    __shared__ unsigned long long carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (long long base = 0; base < nb; base += kMcScanThreads) {
+        const long long i = base + threadIdx.x;
+        const unsigned long long v = i < nb ? counts[i] : 0ull;
+        unsigned long long ex, agg;
+        BS(tmp).ExclusiveSum(v, ex, agg);
+        if (i < nb) offs[i] = (unsigned int)(carry + ex);
+        __syncthreads();
+        if (threadIdx.x == 0) carry += agg;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *total = carry;
+}
+
+// device address of the scratch array, looked up once per device with that
+// device current (the host-side symbol is not a device address)
+static int mc_noalloc_scratch(unsigned int** out) {
+    static std::mutex mu;
+    static unsigned int* addr[64] = {nullptr};
+    int dev = 0;
+    DWG_CHECK_CUDA(cudaGetDevice(&dev));
+    DWG_REQUIRE(dev >= 0 && dev < 64, "marching_cubes_noalloc: device ordinal %d out of range", dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_mc_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            set_error("marching_cubes_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+            return DWG_ERR_CUDA;
+        }
+        addr[dev] = (unsigned int*)p;
+    }
+    *out = addr[dev];
+    return DWG_OK;
+}
+
+}  // namespace dwg
+
+extern "C" int dwg_marching_cubes_noalloc(const float* field_dev, const int res[3], const float* positions_dev,
+                                          const float origin[3], float spacing, float iso, float* tris_dev,
+                                          float* centroids_dev, float* normals_dev, long long capacity,
+                                          long long* num_tris_host, void* stream) {
+    using namespace dwg;
+    DWG_REQUIRE(field_dev && res && num_tris_host, "marching_cubes_noalloc: null field, resolution or count");
+    DWG_REQUIRE(origin || positions_dev, "marching_cubes_noalloc: grid undefined (no origin, no positions)");
+    DWG_REQUIRE(res[0] >= 2 && res[1] >= 2 && res[2] >= 2, "marching_cubes_noalloc: resolution must be >= 2");
+    DWG_REQUIRE(capacity >= 0, "marching_cubes_noalloc: negative capacity");
+    const long long ncell = (long long)(res[0] - 1) * (res[1] - 1) * (res[2] - 1);
+    DWG_REQUIRE(ncell <= kMcNoAllocMaxCells,
+                "marching_cubes_noalloc: %lld cells exceed the allocation-free limit of %lld cells; use "
+                "dwg_marching_cubes",
+                ncell, kMcNoAllocMaxCells);
+    DWG_TRY(mc_upload_tables());
+    unsigned int* scratch = nullptr;
+    DWG_TRY(mc_noalloc_scratch(&scratch));
+    unsigned int* counts = scratch;
+    unsigned int* offs = scratch + kMcNoAllocMaxBlocks;
+    unsigned long long* total = reinterpret_cast<unsigned long long*>(scratch + 2 * kMcNoAllocMaxBlocks);
+    cudaStream_t s = (cudaStream_t)stream;
+    McArgs a;
+    a.field = field_dev;
+    a.pos = positions_dev;
+    a.rx = res[0];
+    a.ry = res[1];
+    a.rz = res[2];
+    a.ncell = ncell;
+    a.ox = origin ? origin[0] : 0.f;
+    a.oy = origin ? origin[1] : 0.f;
+    a.oz = origin ? origin[2] : 0.f;
+    a.h = spacing;
+    a.iso = iso;
+    a.iso_dev = nullptr;
+    const long long nb = (ncell + kMcThreads - 1) / kMcThreads;
+    k_mc_count<<<(unsigned)nb, kMcThreads, 0, s>>>(a, counts);
+    k_mc_noalloc_scan<<<1, kMcScanThreads, 0, s>>>(counts, offs, nb, total);
+    k_mc_emit<<<(unsigned)nb, kMcThreads, 0, s>>>(a, offs, capacity, tris_dev, centroids_dev, normals_dev);
+    DWG_CHECK_LAUNCH();
+    unsigned long long T = 0;
+    DWG_CHECK_CUDA(cudaMemcpyAsync(&T, total, sizeof(T), cudaMemcpyDeviceToHost, s));
+    DWG_CHECK_CUDA(cudaStreamSynchronize(s));
+    *num_tris_host = (long long)T;
+    if ((long long)T > capacity) {
+        set_error("marching_cubes_noalloc: %llu triangles exceed capacity %lld", T, capacity);
+        return DWG_ERR_OVERFLOW;
+    }
+    return DWG_OK;
+}

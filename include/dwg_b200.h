@@ -145,6 +145,25 @@ int dwg_marching_cubes(const float* field_dev, const int res[3], const float* po
 /* The generated case tables (edge mask [256], triangle edges [256*16], -1 padded). */
 int dwg_mc_tables(int* edge_table_host, signed char* tri_table_host);
 
+/* Marching cubes that allocates no device memory.  No counterpart in the
+ * reference: it is for callers that cannot allocate while they mesh -- a host
+ * recording a CUDA graph in global capture mode (cudaMalloc is not allowed
+ * during such a capture), a real-time loop that must not allocate after
+ * start-up, or an application whose device memory all comes from its own pool.
+ * Same arguments, kernels and output as dwg_marching_cubes (the count is
+ * returned in *num_tris_host, required; the call synchronises `stream`).
+ * Its scratch is a static device array of the library (about 4 MB, held by
+ * every GPU that loads the library until the process exits), which limits the
+ * grid to 134,217,728 cells (e.g. 512^3); larger grids are rejected with
+ * DWG_ERR_INVALID before any GPU work.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  All calls share the array, so calls that
+ * overlap on the GPU (different streams or threads at once) race. */
+int dwg_marching_cubes_noalloc(const float* field_dev, const int res[3], const float* positions_dev,
+                               const float origin[3], float spacing, float iso, float* tris_dev,
+                               float* centroids_dev, float* normals_dev, long long capacity,
+                               long long* num_tris_host, void* stream);
+
 /* ------------------------------------------------------------------------
  * k nearest neighbours.  Results ascend by the cukd candidate key
  * (float bits of |p-q|^2) << 32 | index (include/cudaKDTree/cukd/knn.h:279-282),
