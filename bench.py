@@ -184,6 +184,7 @@ def run_ours(a, rank, world, local_rank):
         e1.record(stream)
         torch.cuda.synchronize()
         step_ms.append(e0.elapsed_time(e1))
+        print(f"step: {step_ms[-1]:.1f} ms", file=sys.stderr)
         lib.dwg_pipeline_destroy(h)
     barrier()
     torch.cuda.synchronize()
@@ -210,6 +211,7 @@ def run_ours(a, rank, world, local_rank):
         torch.cuda.synchronize()
         e2e_ms.append(e0.elapsed_time(e1))
         e2e_wall_ms.append((time.perf_counter() - t0) * 1e3)
+        print(f"e2e call {i}: {e2e_ms[-1]:.1f} ms (device), {e2e_wall_ms[-1]:.1f} ms (host)", file=sys.stderr)
     clk = clocks.stop()
 
     # kernel-level roofline: the screened GWN grid kernel on the iteration-0 state

@@ -5,6 +5,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -20,6 +21,39 @@ void set_error(const char* fmt, ...) {
     va_start(ap, fmt);
     vsnprintf(g_err, sizeof(g_err), fmt, ap);
     va_end(ap);
+}
+
+int pool_alloc(void** p, size_t bytes) {
+    static std::mutex mu;
+    static bool configured[64] = {false};
+    int dev = 0;
+    DWG_CHECK_CUDA(cudaGetDevice(&dev));
+    if (dev >= 0 && dev < 64) {
+        std::lock_guard<std::mutex> lock(mu);
+        if (!configured[dev]) {
+            cudaMemPool_t pool;
+            if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+                unsigned long long keep = ~0ull;
+                cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            }
+            configured[dev] = true;
+        }
+    }
+    cudaError_t e = cudaMallocAsync(p, bytes, cudaStreamLegacy);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
+    if (e != cudaSuccess) {
+        set_error("device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+        *p = nullptr;
+        return e == cudaErrorMemoryAllocation ? DWG_ERR_NOMEM : DWG_ERR_CUDA;
+    }
+    return DWG_OK;
+}
+
+void pool_free(void* p) {
+    if (!p) return;
+    // wait for every stream's use of the block, then return it to the pool
+    if (cudaDeviceSynchronize() != cudaSuccess) return;
+    cudaFreeAsync(p, cudaStreamLegacy);
 }
 
 }  // namespace dwg

@@ -46,6 +46,14 @@ struct Status {
     } while (0)
 
 // ------------------------------------------------------ device buffers --
+// Device memory comes from the device's stream-ordered pool, which keeps
+// freed blocks mapped (release threshold = unlimited): building and tearing
+// down a pipeline per cloud then costs no page-table work.  An allocation is
+// made complete before it is returned; a release first waits for the device
+// to finish its work, like cudaFree.
+int pool_alloc(void** p, size_t bytes);
+void pool_free(void* p);
+
 // Grow-only device buffer; owner frees.
 template <typename T>
 struct DevBuf {
@@ -53,21 +61,17 @@ struct DevBuf {
     size_t n = 0;
     int reserve(size_t count) {
         if (count <= n && ptr) return DWG_OK;
-        if (ptr) cudaFree(ptr);
-        ptr = nullptr;
-        n = 0;
+        release();
         size_t bytes = (count ? count : 1) * sizeof(T);
-        cudaError_t e = cudaMalloc(&ptr, bytes);
-        if (e != cudaSuccess) {
-            set_error("cudaMalloc(%zu bytes) failed: %s", bytes, cudaGetErrorString(e));
-            ptr = nullptr;
-            return DWG_ERR_NOMEM;
-        }
+        void* p = nullptr;
+        int st = pool_alloc(&p, bytes);
+        if (st != DWG_OK) return st;
+        ptr = (T*)p;
         n = count ? count : 1;
         return DWG_OK;
     }
     void release() {
-        if (ptr) cudaFree(ptr);
+        if (ptr) pool_free(ptr);
         ptr = nullptr;
         n = 0;
     }

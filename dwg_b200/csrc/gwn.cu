@@ -160,13 +160,75 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 4) k_gwn(GwnArgs a) {
             }
         };
 
-        const int4 root = a.info[0];
+        // one child record (level order): a single-point leaf is one term, a
+        // larger leaf is summed point by point, an internal node is a dipole
+        // term when far for this lane and is opened (pushed with the lanes
+        // that need it) otherwise
+        auto child = [&](int cidx, const float4& na, const float4& nb, bool act, int& sp) {
+            const unsigned meta = (unsigned)__float_as_int(nb.w);
+            if (meta & kMetaLeafBit) {
+                if ((meta & kMetaSingle) && !a.use_radii) {
+                    if (act) {
+                        const float dx = na.x - qx, dy = na.y - qy, dz = na.z - qz;
+                        const float d = fmaf(dx, nb.x, fmaf(dy, nb.y, dz * nb.z));
+                        float v;
+                        if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, a.screen, sigma, sigma_l2e, v)) {
+                            acc_add<PREC>(s, c, v);
+                            ++nterm;
+                        }
+                    }
+                } else {
+                    const int st = (int)(meta & kMetaIndex), cnt = __float_as_int(na.w);
+                    if (cnt < 0 || st + cnt > a.num_points) {
+                        if (lane == 0) atomicOr(&a.work[1], 4u);
+                    } else if (act) {
+                        leaf_points(st, cnt);
+                    }
+                }
+                return;
+            }
+            bool near = false;
+            if (act) {
+                // opening test sqrt_rn(d2) > beta*R, d2 in round-to-nearest
+                // single precision (src/TurboLibiGWN.cu:636-644), as a
+                // comparison of d2 with the node's exact threshold
+                const float dx = __fsub_rn(na.x, qx), dy = __fsub_rn(na.y, qy), dz = __fsub_rn(na.z, qz);
+                const float d2 = sq3_rn(dx, dy, dz);
+                const float thr = fabsf(na.w);
+                bool far = d2 > thr;
+                if (!far && d2 == thr && signbit(na.w)) far = __fsqrt_rn(d2) > __fmul_rn(a.beta, a.node_r[cidx]);
+                if (far) {
+                    const float d = fmaf(dx, nb.x, fmaf(dy, nb.y, dz * nb.z));
+                    float v;
+                    if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, a.screen, sigma, sigma_l2e, v)) {
+                        acc_add<PREC>(s, c, v);
+                        ++nterm;
+                    }
+                } else {
+                    near = true;
+                }
+            }
+            const unsigned nm = __ballot_sync(FULL, near);
+            if (nm) {
+                if (sp < kGwnStack) {
+                    if (lane == 0) stack[w][sp] = make_int2(cidx, (int)nm);
+                    ++sp;
+                } else if (lane == 0) {
+                    atomicOr(&a.work[1], 1u);
+                }
+            }
+        };
+
         int sp = 0;
-        if (root.w & kLeafFlag) {
-            if (valid && root.x >= 0 && root.y >= 0 && root.x + root.y <= a.num_points) leaf_points(root.x, root.y);
-        } else {
-            if (lane == 0) stack[w][0] = make_int2(0, (int)vm);
-            sp = 1;
+        {
+            const float4 ra = a.node_a[0], rb = a.node_b[0];
+            const unsigned rm = (unsigned)__float_as_int(rb.w);
+            if (rm & kMetaLeafBit) {
+                child(0, ra, rb, valid, sp);  // a leaf root is summed; nothing is pushed
+            } else {
+                if (lane == 0) stack[w][0] = make_int2(0, (int)vm);
+                sp = 1;
+            }
         }
         while (sp > 0) {
             __syncwarp();
@@ -177,73 +239,24 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 4) k_gwn(GwnArgs a) {
                 continue;
             }
             const bool act = (((unsigned)e.y) >> lane) & 1u;
-            const int end = __float_as_int(a.node_b[e.x].w) & kMetaSkip;
-            int ch = e.x + 1;
-            while (ch < end) {
-                const float4 na = a.node_a[ch];
-                const float4 nb = a.node_b[ch];
-                const int meta = __float_as_int(nb.w);
-                const int next = meta & kMetaSkip;
-                // structural guard: a child's subtree ends after it and within
-                // its parent's
-                if (next <= ch || next > end || end > a.num_nodes) {
-                    if (lane == 0) atomicOr(&a.work[1], 2u);
-                    break;
+            const unsigned pm = (unsigned)__float_as_int(a.node_b[e.x].w);
+            const int first = (int)(pm & kMetaIndex);
+            const int nch = (int)((pm >> 28) & 7u) + 1;
+            // structural guard: children come after the parent, inside the table
+            if ((pm & kMetaLeafBit) || first <= e.x || first + nch > a.num_nodes) {
+                if (lane == 0) atomicOr(&a.work[1], 2u);
+                continue;
+            }
+            float4 na = a.node_a[first], nb = a.node_b[first];
+            for (int j = 0; j < nch; ++j) {
+                float4 na2, nb2;
+                if (j + 1 < nch) {  // load the next sibling while this one is evaluated
+                    na2 = a.node_a[first + j + 1];
+                    nb2 = a.node_b[first + j + 1];
                 }
-                if (meta & kMetaLeaf) {
-                    if ((meta & kMetaSingle) && !a.use_radii) {
-                        // one point: its term is the node's (cm = p, ec = A n)
-                        if (act) {
-                            const float dx = na.x - qx, dy = na.y - qy, dz = na.z - qz;
-                            const float d = fmaf(dx, nb.x, fmaf(dy, nb.y, dz * nb.z));
-                            float v;
-                            if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, a.screen, sigma, sigma_l2e, v)) {
-                                acc_add<PREC>(s, c, v);
-                                ++nterm;
-                            }
-                        }
-                    } else {
-                        const int4 ic = a.info[ch];
-                        if (ic.x < 0 || ic.y < 0 || ic.x + ic.y > a.num_points) {
-                            if (lane == 0) atomicOr(&a.work[1], 4u);
-                        } else if (act) {
-                            leaf_points(ic.x, ic.y);
-                        }
-                    }
-                } else {
-                    bool near = false;
-                    if (act) {
-                        // opening test sqrt_rn(d2) > beta*R, d2 in round-to-nearest
-                        // single precision (src/TurboLibiGWN.cu:636-644), as a
-                        // comparison of d2 with the node's exact threshold
-                        const float dx = __fsub_rn(na.x, qx), dy = __fsub_rn(na.y, qy), dz = __fsub_rn(na.z, qz);
-                        const float d2 = sq3_rn(dx, dy, dz);
-                        const float thr = fabsf(na.w);
-                        bool far = d2 > thr;
-                        if (!far && d2 == thr && signbit(na.w))
-                            far = __fsqrt_rn(d2) > __fmul_rn(a.beta, a.node_r[ch]);
-                        if (far) {
-                            const float d = fmaf(dx, nb.x, fmaf(dy, nb.y, dz * nb.z));
-                            float v;
-                            if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, a.screen, sigma, sigma_l2e, v)) {
-                                acc_add<PREC>(s, c, v);
-                                ++nterm;
-                            }
-                        } else {
-                            near = true;
-                        }
-                    }
-                    const unsigned nm = __ballot_sync(FULL, near);
-                    if (nm) {
-                        if (sp < kGwnStack) {
-                            if (lane == 0) stack[w][sp] = make_int2(ch, (int)nm);
-                            ++sp;
-                        } else if (lane == 0) {
-                            atomicOr(&a.work[1], 1u);
-                        }
-                    }
-                }
-                ch = next;
+                child(first + j, na, nb, act, sp);
+                na = na2;
+                nb = nb2;
             }
         }
         if (valid) {

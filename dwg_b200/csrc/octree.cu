@@ -15,6 +15,8 @@
 //      contiguous node range and a contiguous point range.
 #include <cub/cub.cuh>
 
+#include <vector>
+
 #include "octree.cuh"
 
 namespace dwg {
@@ -218,7 +220,7 @@ __device__ __forceinline__ double warp_max_d(double v) {
 }
 
 __global__ void k_centres(const int4* __restrict__ info, const float4* __restrict__ pa, int M,
-                          double* __restrict__ cm_d, double* __restrict__ r_d,
+                          double* __restrict__ cm_d, double* __restrict__ r_d, const int* __restrict__ lvl_of,
                           float4* __restrict__ node_a, float* __restrict__ node_r) {
     const int lane = threadIdx.x & 31;
     const long long warp = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
@@ -255,8 +257,11 @@ __global__ void k_centres(const int4* __restrict__ info, const float4* __restric
             cm_d[v * 3 + 1] = cy;
             cm_d[v * 3 + 2] = cz;
             r_d[v] = rm;
-            node_a[v] = make_float4((float)cx, (float)cy, (float)cz, 0.f);
-            node_r[v] = (float)rm;
+            const int p = lvl_of[v];
+            // leaves keep their point count in .w (they have no open test)
+            node_a[p] = make_float4((float)cx, (float)cy, (float)cz,
+                                    (iv.w & kLeafFlag) ? __int_as_float(iv.y) : 0.f);
+            node_r[p] = (float)rm;
         }
     }
 }
@@ -264,12 +269,14 @@ __global__ void k_centres(const int4* __restrict__ info, const float4* __restric
 // sum A n per node, bottom-up one depth level at a time: a leaf sums its
 // points, an internal node its children (in octant order) -- every node's sum
 // has a fixed order, so the result is the same from run to run
-__global__ void k_ec_level(const int* __restrict__ nodes, int count, const int4* __restrict__ info,
+__global__ void k_ec_level(const int* __restrict__ nodes, int p0, int count, const int4* __restrict__ info,
                            const float4* __restrict__ pa, const float4* __restrict__ nr,
-                           double* __restrict__ ec_d, float4* __restrict__ node_b) {
+                           const int* __restrict__ meta, double* __restrict__ ec_d,
+                           float4* __restrict__ node_b) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
-    const int v = nodes[i];
+    const int p = p0 + i;
+    const int v = nodes[p];
     const int4 iv = info[v];
     double ex = 0, ey = 0, ez = 0;
     if (iv.w & kLeafFlag) {
@@ -290,17 +297,48 @@ __global__ void k_ec_level(const int* __restrict__ nodes, int count, const int4*
     ec_d[(size_t)v * 3] = ex;
     ec_d[(size_t)v * 3 + 1] = ey;
     ec_d[(size_t)v * 3 + 2] = ez;
-    int meta = iv.z | ((iv.w & kLeafFlag) ? kMetaLeaf : 0) | (((iv.w & kLeafFlag) && iv.y == 1) ? kMetaSingle : 0);
-    node_b[v] = make_float4((float)ex, (float)ey, (float)ez, __int_as_float(meta));
+    node_b[p] = make_float4((float)ex, (float)ey, (float)ez, __int_as_float(meta[p]));
+}
+
+// level-order position of every node and the traversal meta word
+__global__ void k_lvl_of(const int* __restrict__ level_nodes, int M, int* __restrict__ lvl_of) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < M) lvl_of[level_nodes[p]] = p;
+}
+
+__global__ void k_node_meta(const int4* __restrict__ info, const int* __restrict__ level_nodes,
+                            const int* __restrict__ lvl_of, int M, int* __restrict__ meta) {
+    int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= M) return;
+    const int v = level_nodes[p];
+    const int4 iv = info[v];
+    unsigned m;
+    if (iv.w & kLeafFlag) {
+        m = kMetaLeafBit | (iv.y == 1 ? (unsigned)kMetaSingle : 0u) | ((unsigned)iv.x & kMetaIndex);
+    } else {
+        int nch = 0;
+        for (int c = v + 1; c < iv.z && nch < 9; c = info[c].z) ++nch;
+        m = ((unsigned)lvl_of[v + 1] & kMetaIndex) | ((unsigned)(nch - 1) << 28);
+    }
+    meta[p] = (int)m;
+}
+
+__global__ void k_depth_key(const int4* __restrict__ info, int M, unsigned* __restrict__ key, int* __restrict__ id) {
+    int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= M) return;
+    key[v] = (unsigned)(info[v].w & 0xff);
+    id[v] = v;
 }
 
 // Open threshold of a node for opening ratio beta: with t = beta*R rounded,
 // sqrt_rn(d2) > t  <=>  d2 > B, B = (t + ulp(t)/2)^2 (exact in FP64), except
 // d2 == B, which rounds half to even and is decided by the exact test.  The
 // float stored is B rounded down, negated when B is itself a float.
-__global__ void k_node_thr(const float* __restrict__ node_r, int M, float beta, float4* __restrict__ node_a) {
+__global__ void k_node_thr(const float* __restrict__ node_r, const int* __restrict__ meta, int M, float beta,
+                           float4* __restrict__ node_a) {
     int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= M) return;
+    if ((unsigned)meta[v] & kMetaLeafBit) return;
     const float t = __fmul_rn(beta, node_r[v]);
     float thr;
     if (t == 0.f) {
@@ -316,16 +354,6 @@ __global__ void k_node_thr(const float* __restrict__ node_r, int M, float beta, 
     node_a[v] = a;
 }
 
-__global__ void k_depth_hist(const int4* __restrict__ info, int M, int* __restrict__ hist) {
-    int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v < M) atomicAdd(&hist[info[v].w & 0xff], 1);
-}
-
-__global__ void k_depth_scatter(const int4* __restrict__ info, int M, int* __restrict__ fill,
-                                int* __restrict__ nodes) {
-    int v = blockIdx.x * blockDim.x + threadIdx.x;
-    if (v < M) nodes[atomicAdd(&fill[info[v].w & 0xff], 1)] = v;
-}
 
 // ---------------------------------------------------------- leaf centres --
 __global__ void k_leaf_flags(const int4* __restrict__ info, int M, int min_count, int* __restrict__ f) {
@@ -444,20 +472,34 @@ int octree_build(Octree& t, const float* P, int n, int D, const float* A, cudaSt
         DWG_CHECK_LAUNCH();
     }
     {
-        DevBuf<int> hist, fill;
-        DWG_TRY(hist.reserve(kMaxDepth + 2));
-        DWG_TRY(fill.reserve(kMaxDepth + 2));
+        // level order: stable radix sort of the nodes by depth
+        DevBuf<unsigned> dkey, dkey2;
+        DevBuf<int> ids;
+        DWG_TRY(dkey.reserve(M));
+        DWG_TRY(dkey2.reserve(M));
+        DWG_TRY(ids.reserve(M));
         DWG_TRY(t.level_nodes.reserve(M));
-        DWG_CHECK_CUDA(cudaMemsetAsync(hist.ptr, 0, sizeof(int) * (kMaxDepth + 2), s));
-        k_depth_hist<<<div_up(M, 256), 256, 0, s>>>(t.info.ptr, M, hist.ptr);
+        DWG_TRY(t.lvl_of.reserve(M));
+        DWG_TRY(t.node_meta.reserve(M));
+        k_depth_key<<<div_up(M, 256), 256, 0, s>>>(t.info.ptr, M, dkey.ptr, ids.ptr);
         DWG_CHECK_LAUNCH();
-        int h[kMaxDepth + 2];
-        DWG_CHECK_CUDA(cudaMemcpyAsync(h, hist.ptr, sizeof(h), cudaMemcpyDeviceToHost, s));
+        unsigned* k0 = dkey.ptr;
+        unsigned* k1 = dkey2.ptr;
+        int* v0 = ids.ptr;
+        int* v1 = t.level_nodes.ptr;
+        DWG_TRY(cub_call(t.scratch, [&](void* tmp, size_t& bytes) {
+            return cub::DeviceRadixSort::SortPairs(tmp, bytes, k0, k1, v0, v1, M, 0, 5, s);
+        }));
+        std::vector<unsigned> h(M);
+        DWG_CHECK_CUDA(cudaMemcpyAsync(h.data(), dkey2.ptr, sizeof(unsigned) * M, cudaMemcpyDeviceToHost, s));
         DWG_CHECK_CUDA(cudaStreamSynchronize(s));
+        for (int d = 0; d <= kMaxDepth + 1; ++d) t.level_off[d] = M;
+        for (int p = M - 1; p >= 0; --p) t.level_off[h[p]] = p;
         t.level_off[0] = 0;
-        for (int d = 0; d <= kMaxDepth; ++d) t.level_off[d + 1] = t.level_off[d] + (d <= D ? h[d] : 0);
-        DWG_CHECK_CUDA(cudaMemcpyAsync(fill.ptr, t.level_off, sizeof(int) * (kMaxDepth + 1), cudaMemcpyHostToDevice, s));
-        k_depth_scatter<<<div_up(M, 256), 256, 0, s>>>(t.info.ptr, M, fill.ptr, t.level_nodes.ptr);
+        for (int d = kMaxDepth; d >= 0; --d)
+            if (t.level_off[d] > t.level_off[d + 1]) t.level_off[d] = t.level_off[d + 1];
+        k_lvl_of<<<div_up(M, 256), 256, 0, s>>>(t.level_nodes.ptr, M, t.lvl_of.ptr);
+        k_node_meta<<<div_up(M, 256), 256, 0, s>>>(t.info.ptr, t.level_nodes.ptr, t.lvl_of.ptr, M, t.node_meta.ptr);
         DWG_CHECK_LAUNCH();
         DWG_CHECK_CUDA(cudaStreamSynchronize(s));
     }
@@ -501,8 +543,8 @@ static unsigned moment_blocks(int M) {
 }
 
 int octree_update_centres(Octree& t, cudaStream_t s) {
-    k_centres<<<moment_blocks(t.M), 256, 0, s>>>(t.info.ptr, t.pa.ptr, t.M, t.cm_d.ptr, t.r_d.ptr, t.node_a.ptr,
-                                                  t.node_r.ptr);
+    k_centres<<<moment_blocks(t.M), 256, 0, s>>>(t.info.ptr, t.pa.ptr, t.M, t.cm_d.ptr, t.r_d.ptr, t.lvl_of.ptr,
+                                                  t.node_a.ptr, t.node_r.ptr);
     DWG_CHECK_LAUNCH();
     t.thr_beta = -1.f;
     return DWG_OK;
@@ -510,7 +552,7 @@ int octree_update_centres(Octree& t, cudaStream_t s) {
 
 int octree_set_beta(Octree& t, float beta, cudaStream_t s) {
     if (t.thr_beta == beta) return DWG_OK;
-    k_node_thr<<<div_up(t.M, 256), 256, 0, s>>>(t.node_r.ptr, t.M, beta, t.node_a.ptr);
+    k_node_thr<<<div_up(t.M, 256), 256, 0, s>>>(t.node_r.ptr, t.node_meta.ptr, t.M, beta, t.node_a.ptr);
     DWG_CHECK_LAUNCH();
     t.thr_beta = beta;
     return DWG_OK;
@@ -520,8 +562,8 @@ int octree_update_normals(Octree& t, cudaStream_t s) {
     for (int d = t.max_depth; d >= 0; --d) {
         int cnt = t.level_off[d + 1] - t.level_off[d];
         if (cnt <= 0) continue;
-        k_ec_level<<<div_up(cnt, 128), 128, 0, s>>>(t.level_nodes.ptr + t.level_off[d], cnt, t.info.ptr, t.pa.ptr,
-                                                     t.nr.ptr, t.ec_d.ptr, t.node_b.ptr);
+        k_ec_level<<<div_up(cnt, 128), 128, 0, s>>>(t.level_nodes.ptr, t.level_off[d], cnt, t.info.ptr, t.pa.ptr,
+                                                     t.nr.ptr, t.node_meta.ptr, t.ec_d.ptr, t.node_b.ptr);
     }
     DWG_CHECK_LAUNCH();
     return DWG_OK;

@@ -5,17 +5,23 @@
 //   points, sorted by their octant path (a 3*max_depth-bit key, stable):
 //     pa[i] = (x, y, z, area)  float4      nr[i] = (nx, ny, nz, radius) float4
 //     perm[i] = input index of sorted point i
-//   nodes, depth-first pre-order (a node's subtree is contiguous and its first
-//   child, if any, is the next node):
-//     info[v]   = (pt_start, pt_count, skip, depth | LEAF)     int4
-//     node_a[v] = (cm.x, cm.y, cm.z, open threshold)          float4
-//     node_b[v] = (sum A n .x, .y, .z, meta)                  float4
-//     node_r[v] = R (max |p - cm|, rounded from FP64)         float
-//   meta = skip | LEAF_BIT | SINGLE_BIT (a leaf holding one point); the open
-//   threshold is the largest float T with sqrt_rn(d2) > beta*R <=> d2 > T for
-//   every float d2 != T, its sign bit set when d2 == T needs the exact test.
-//   skip[v] = index of the first node after v's subtree, so the children of v
-//   are v+1, skip[v+1], skip[skip[v+1]], ... while < skip[v].
+//   nodes, numbered v in depth-first pre-order (a node's subtree is
+//   contiguous and its first child, if any, is the next node):
+//     info[v] = (pt_start, pt_count, skip, depth | LEAF)   int4
+//     skip[v] = index of the first node after v's subtree, so the children of
+//     v are v+1, skip[v+1], ... while < skip[v]
+//     cm_d, r_d, ec_d: FP64 moments, pre-order
+//   traversal records, numbered p in level order (by depth, then pre-order),
+//   where the children of a node are consecutive:
+//     node_a[p] = (cm.x, cm.y, cm.z, open threshold | leaf point count)  float4
+//     node_b[p] = (sum A n .x, .y, .z, meta)                             float4
+//     node_r[p] = R (max |p - cm|, rounded from FP64)                    float
+//     level_nodes[p] = v,  lvl_of[v] = p
+//   meta of an internal node: first child p (bits 0-27) | (children - 1) << 28;
+//   of a leaf: LEAF (bit 31) | SINGLE (bit 30, one point) | pt_start (bits 0-27).
+//   The open threshold is the largest float T with sqrt_rn(d2) > beta*R <=>
+//   d2 > T for every float d2 != T; its sign bit is set when d2 == T needs the
+//   exact test.
 // Empty octants are not stored (the reference skips them at
 // src/TurboLibiGWN.cu:630).
 #pragma once
@@ -26,9 +32,9 @@ namespace dwg {
 
 constexpr int kLeafFlag = 1 << 8;
 constexpr int kMaxDepth = 21;
-constexpr int kMetaSkip = (1 << 29) - 1;
-constexpr int kMetaLeaf = 1 << 29;
+constexpr int kMetaIndex = (1 << 28) - 1;
 constexpr int kMetaSingle = 1 << 30;
+constexpr unsigned kMetaLeafBit = 1u << 31;
 
 struct Octree {
     int n = 0;
@@ -45,8 +51,8 @@ struct Octree {
     DevBuf<float> node_r;
     float thr_beta = -1.f;  // beta the open thresholds were computed for (-1: none)
     DevBuf<double> cm_d, r_d, ec_d;
-    // node ids grouped by depth (level d = level_nodes[level_off[d] .. level_off[d+1]))
-    DevBuf<int> level_nodes;
+    // level order: level d = positions level_off[d] .. level_off[d+1]
+    DevBuf<int> level_nodes, lvl_of, node_meta;
     int level_off[kMaxDepth + 2] = {0};
     DevBuf<unsigned char> scratch;  // CUB temporary storage
     mutable DevBuf<unsigned int> work;  // [0] work counter of the persistent GWN kernel, [1] error flag
