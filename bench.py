@@ -167,7 +167,7 @@ def run_ours(a, rank, world, local_rank):
         capi.check(lib.dwg_pipeline_get(last, b"tri_count", tri_count.ctypes.data))
         final_tris = v.value
         lib.dwg_pipeline_destroy(last)
-    launches = count_launches(a)
+    census = kernel_census(one_step, lib, torch)
 
     # timed: device events per step, L2 flushed between steps
     clocks = ClockSampler(local_rank)
@@ -248,23 +248,49 @@ def run_ours(a, rank, world, local_rank):
         "e2e": {"value": total_pts / (ems * 1e-3) / 1e6, "unit": "Mpts/s", "ms_per_step": ems,
                 "host_wall_ms_per_step": float(np.mean(e2e_wall_ms)),
                 "h2d_bytes_per_step": a.points * 12, "d2h_bytes_per_step": int(ntri.value) * 36 + a.points * 12},
-        "gpu_launches": launches * a.steps,
+        "gpu_launches": census["per_step"] * a.steps if census else None,
+        "kernel_census": census,
         "roofline": roof,
         "clocks": clk,
     }
     return out
 
 
-def count_launches(a):
-    """Kernel launches of one step, by construction of the pipeline:
-    setup (two octree builds with (max_depth+1) level passes, leaves, kNN
-    build, grids) + per iteration (15) + final pass."""
-    D = WORKLOAD["max_depth"]
-    octree = 2 + 1 + 1 + 2 + 4 * (D + 1) + 1 + 1 + 1  # bbox(2), root, keys, sort~, lcp, starts, levels, gather, centres
-    setup = 2 * octree + 3 + 4 + 3 + 2 + 2 + 1
-    per_iter = 15
-    final = 2 + 2 + 1 + 2 + 2 + 4
-    return setup + per_iter * a.iters + final
+def kernel_census(one_step, lib, torch):
+    """Kernels of one (untimed) step, counted from CUPTI activity records
+    (graph replays included) by liblaunch_counter.so: per-step launch count
+    of this library's kernels (dwg:: and its CUB instantiations) and the
+    device-time share of the top ones."""
+    import ctypes as C
+
+    from dwg_b200 import build
+    try:
+        lc = C.CDLL(build.COUNTER)
+    except OSError as e:
+        print(f"kernel census unavailable: {e}", file=sys.stderr)
+        return None
+    lc.dwglc_report.argtypes = [C.c_char_p, C.c_int]
+    torch.cuda.synchronize()
+    if lc.dwglc_start() != 0:
+        print("kernel census unavailable: CUPTI refused activity tracing", file=sys.stderr)
+        return None
+    h = one_step()
+    torch.cuda.synchronize()
+    lc.dwglc_stop()
+    lib.dwg_pipeline_destroy(h)
+    n = lc.dwglc_report(None, 0)
+    buf = C.create_string_buffer(n)
+    lc.dwglc_report(buf, n)
+    rows = []
+    for line in buf.value.decode().splitlines():
+        name, cnt, ns = line.rsplit("\t", 2)
+        if "dwg::" in name or "cub::" in name:
+            rows.append((name, int(cnt), int(ns) / 1e6))
+    total_ms = sum(r[2] for r in rows)
+    rows.sort(key=lambda r: -r[2])
+    return {"per_step": sum(r[1] for r in rows), "kernel_ms_per_step": total_ms,
+            "top": [{"kernel": r[0][:80], "launches": r[1], "ms": round(r[2], 3),
+                     "share": round(r[2] / total_ms, 4) if total_ms else None} for r in rows[:6]]}
 
 
 def gwn_roofline(a, lib, capi, turbo, torch, dev, P):

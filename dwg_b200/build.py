@@ -19,6 +19,9 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libdwg_b200.so")
 CLI_SRC = os.path.join(HERE, "cli", "dwg_cuda.cpp")
 CLI = os.path.join(HERE, "bin", "DWG_CUDA")
+COUNTER_SRC = os.path.join(CSRC, "launch_counter.cpp")
+COUNTER = os.path.join(HERE, "liblaunch_counter.so")
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [
@@ -85,7 +88,20 @@ def build(force: bool = False, jobs: int = 0, verbose: bool = False) -> str:
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
     build_cli(force)
+    build_counter(force)
     return LIB
+
+
+def build_counter(force: bool = False) -> str:
+    """Kernel launch census used by bench.py (CUPTI activity records)."""
+    if force or _stale(COUNTER, [COUNTER_SRC]):
+        cupti_lib = os.path.join(CUDA_HOME, "targets", "x86_64-linux", "lib")
+        cmd = ["g++", "-O2", "-std=c++17", "-shared", "-fPIC", "-I" + os.path.join(CUDA_HOME, "include"),
+               COUNTER_SRC, "-o", COUNTER, "-L" + cupti_lib, "-lcupti", "-Wl,-rpath," + cupti_lib]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"launch counter build failed:\n{r.stdout}\n{r.stderr}")
+    return COUNTER
 
 
 def build_cli(force: bool = False) -> str:

@@ -28,7 +28,7 @@ class DwgError(RuntimeError):
 
 class GwnParams(C.Structure):
     _fields_ = [("beta", C.c_float), ("sigma", C.c_float), ("screen", C.c_float),
-                ("screened", C.c_int), ("use_radii", C.c_int), ("precision", C.c_int)]
+                ("screened", C.c_int), ("use_radii", C.c_int), ("precision", C.c_int), ("tile", C.c_int)]
 
 
 class Params(C.Structure):
@@ -39,7 +39,13 @@ class Params(C.Structure):
         ("offset_1", C.c_float), ("offset_2", C.c_float), ("use_leaves_generate", C.c_int),
         ("total_iter", C.c_int), ("beta", C.c_float), ("area", C.c_float), ("screen", C.c_float),
         ("knn_tri", C.c_int), ("knn_zero", C.c_int), ("precision", C.c_int), ("use_graph", C.c_int),
+        ("tile", C.c_int),
     ]
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("beta", C.c_float), ("tile", C.c_int), ("rms_err", C.c_float), ("max_err", C.c_float),
+                ("grid_ms", C.c_float), ("ref_ms", C.c_float)]
 
 
 # name -> (restype, argtypes)
@@ -81,6 +87,25 @@ _SIGS = {
     "dwg_pipeline_size": (_i, [_vp, C.c_char_p, C.POINTER(_ll)]),
     "dwg_pipeline_get": (_i, [_vp, C.c_char_p, _vp]),
     "dwg_pipeline_device_ptr": (_i, [_vp, C.c_char_p, C.POINTER(_vp)]),
+    "dwg_autotune": (_i, [_vp, _i, C.POINTER(Params), _f, _i, _i, _vp, C.POINTER(TuneResult)]),
+    "dwg_batch_create": (_i, [_vp, _vp, _i, _vp, _vp, C.POINTER(_vp)]),
+    "dwg_batch_destroy": (_i, [_vp]),
+    "dwg_batch_iterate": (_i, [_vp, _i]),
+    "dwg_batch_finalize": (_i, [_vp]),
+    "dwg_batch_cloud": (_i, [_vp, _i, C.POINTER(_vp)]),
+    "dwg_mlp_param_count": (_ll, []),
+    "dwg_mlp_create": (_i, [C.c_ulonglong, _vp, C.POINTER(_vp)]),
+    "dwg_mlp_destroy": (_i, [_vp]),
+    "dwg_mlp_set_params": (_i, [_vp, _vp, _ll]),
+    "dwg_mlp_get_params": (_i, [_vp, _vp, _ll]),
+    "dwg_mlp_load": (_i, [_vp, C.c_char_p]),
+    "dwg_mlp_save": (_i, [_vp, C.c_char_p]),
+    "dwg_mlp_features": (_i, [_vp, _i, _vp, _vp]),
+    "dwg_mlp_forward": (_i, [_vp, _vp, _ll, _vp, _vp]),
+    "dwg_mlp_gradients": (_i, [_vp, _vp, _vp, _ll, C.POINTER(_f), _vp, _ll, _vp]),
+    "dwg_mlp_train_step": (_i, [_vp, _vp, _vp, _ll, _f, C.POINTER(_f), _vp]),
+    "dwg_mlp_init_normals": (_i, [_vp, _vp, _i, _vp, _vp]),
+    "dwg_pipeline_create_learned": (_i, [_vp, _i, C.POINTER(Params), _vp, _vp, C.POINTER(_vp)]),
     "dwg_reconstruct_host": (_i, [_vp, _vp, _i, C.POINTER(Params), _vp, _vp, _ll, C.POINTER(_ll), _vp]),
     "dwg_read_xyz": (_i, [C.c_char_p, _i, C.POINTER(C.POINTER(_f)), C.POINTER(C.POINTER(_f)), C.POINTER(_i)]),
     "dwg_free_host": (None, [_vp]),
@@ -157,5 +182,6 @@ def default_params(**kw) -> Params:
     return p
 
 
-def gwn_params(beta=2.3, sigma=10.0, screen=0.0015, screened=True, use_radii=False, precision=1) -> GwnParams:
-    return GwnParams(beta, sigma, screen, int(screened), int(use_radii), int(precision))
+def gwn_params(beta=2.3, sigma=10.0, screen=0.0015, screened=True, use_radii=False, precision=1,
+               tile=0) -> GwnParams:
+    return GwnParams(beta, sigma, screen, int(screened), int(use_radii), int(precision), int(tile))

@@ -10,7 +10,8 @@
 #include <string>
 #include <vector>
 
-#include "pipeline.cuh"
+#include "batch.cuh"
+#include "tune.cuh"
 
 namespace dwg {
 
@@ -66,8 +67,11 @@ struct dwg_octree {
 struct dwg_knn_index {
     KnnIndex ix;
 };
-struct dwg_pipeline {
-    Pipeline p;
+struct dwg_batch {
+    Batch b;
+};
+struct dwg_mlp {
+    Mlp m;
 };
 
 #define S(stream) ((cudaStream_t)(stream))
@@ -396,6 +400,7 @@ void dwg_params_default(dwg_params* p) {
     p->knn_zero = 10;
     p->precision = 1;
     p->use_graph = 1;
+    p->tile = 0;
 }
 
 int dwg_pipeline_create(const float* points_dev, const float* normals_dev, int n, const dwg_params* params,
@@ -527,6 +532,201 @@ int dwg_pipeline_device_ptr(dwg_pipeline* p, const char* what, void** ptr) {
         return DWG_ERR_INVALID;
     }
     return DWG_OK;
+}
+
+int dwg_batch_create(const float* const* points_dev, const int* counts, int num_clouds, const dwg_params* params,
+                     void* stream, dwg_batch** out) {
+    API_GUARD({
+        DWG_REQUIRE(out && points_dev && counts && params && num_clouds >= 1, "batch_create: bad arguments");
+        *out = nullptr;
+        dwg_batch* o = new dwg_batch();
+        int st = o->b.setup(points_dev, counts, num_clouds, params, S(stream));
+        if (st != DWG_OK) {
+            delete o;
+            return st;
+        }
+        *out = o;
+        return DWG_OK;
+    })
+}
+
+int dwg_batch_destroy(dwg_batch* b) {
+    delete b;
+    return DWG_OK;
+}
+
+int dwg_batch_iterate(dwg_batch* b, int n_iters) {
+    API_GUARD({
+        DWG_REQUIRE(b, "batch_iterate: null batch");
+        return b->b.iterate(n_iters);
+    })
+}
+
+int dwg_batch_finalize(dwg_batch* b) {
+    API_GUARD({
+        DWG_REQUIRE(b, "batch_finalize: null batch");
+        return b->b.finalize();
+    })
+}
+
+int dwg_batch_cloud(dwg_batch* b, int index, dwg_pipeline** cloud) {
+    API_GUARD({
+        DWG_REQUIRE(b && cloud, "batch_cloud: null argument");
+        DWG_REQUIRE(index >= 0 && index < (int)b->b.clouds.size(), "batch_cloud: index %d out of range", index);
+        *cloud = b->b.clouds[index].get();
+        return DWG_OK;
+    })
+}
+
+int dwg_autotune(const float* points_dev, int n, const dwg_params* params, float tol, int samples, int warm_iters,
+                 void* stream, dwg_tune_result* out) {
+    API_GUARD({
+        DWG_REQUIRE(points_dev && params && out && n >= 2, "autotune: bad arguments");
+        return autotune(points_dev, n, *params, tol, samples, warm_iters, S(stream), out);
+    })
+}
+
+long long dwg_mlp_param_count(void) { return mlp_param_count(); }
+
+int dwg_mlp_create(unsigned long long seed, void* stream, dwg_mlp** out) {
+    API_GUARD({
+        DWG_REQUIRE(out, "mlp_create: out is null");
+        *out = nullptr;
+        dwg_mlp* o = new dwg_mlp();
+        int st = mlp_init(o->m, seed, S(stream));
+        if (st != DWG_OK) {
+            delete o;
+            return st;
+        }
+        *out = o;
+        return DWG_OK;
+    })
+}
+
+int dwg_mlp_destroy(dwg_mlp* m) {
+    delete m;
+    return DWG_OK;
+}
+
+int dwg_mlp_set_params(dwg_mlp* m, const float* params_host, long long count) {
+    API_GUARD({
+        DWG_REQUIRE(m && params_host, "mlp_set_params: null argument");
+        DWG_REQUIRE(count == mlp_param_count(), "mlp_set_params: count %lld != %lld", count, mlp_param_count());
+        return mlp_set_flat(m->m, params_host, 0);
+    })
+}
+
+int dwg_mlp_get_params(dwg_mlp* m, float* params_host, long long count) {
+    API_GUARD({
+        DWG_REQUIRE(m && params_host, "mlp_get_params: null argument");
+        DWG_REQUIRE(count == mlp_param_count(), "mlp_get_params: count %lld != %lld", count, mlp_param_count());
+        return mlp_get_flat(m->m, params_host, 0);
+    })
+}
+
+static const char kMlpMagic[8] = {'D', 'W', 'G', 'M', 'L', 'P', '0', '1'};
+
+int dwg_mlp_load(dwg_mlp* m, const char* path) {
+    API_GUARD({
+        DWG_REQUIRE(m && path, "mlp_load: null argument");
+        FILE* f = fopen(path, "rb");
+        DWG_REQUIRE(f, "mlp_load: cannot open %s", path);
+        char magic[8];
+        long long count = 0;
+        const long long want = mlp_param_count();
+        std::vector<float> buf((size_t)want);
+        bool ok = fread(magic, 1, 8, f) == 8 && memcmp(magic, kMlpMagic, 8) == 0 &&
+                  fread(&count, sizeof(count), 1, f) == 1 && count == want &&
+                  fread(buf.data(), sizeof(float), (size_t)want, f) == (size_t)want;
+        fclose(f);
+        DWG_REQUIRE(ok, "mlp_load: %s is not a parameter file of %lld floats", path, want);
+        for (float v : buf) DWG_REQUIRE(std::isfinite(v), "mlp_load: %s holds a non-finite parameter", path);
+        return mlp_set_flat(m->m, buf.data(), 0);
+    })
+}
+
+int dwg_mlp_save(dwg_mlp* m, const char* path) {
+    API_GUARD({
+        DWG_REQUIRE(m && path, "mlp_save: null argument");
+        const long long count = mlp_param_count();
+        std::vector<float> buf((size_t)count);
+        DWG_TRY(mlp_get_flat(m->m, buf.data(), 0));
+        FILE* f = fopen(path, "wb");
+        DWG_REQUIRE(f, "mlp_save: cannot create %s", path);
+        bool ok = fwrite(kMlpMagic, 1, 8, f) == 8 && fwrite(&count, sizeof(count), 1, f) == 1 &&
+                  fwrite(buf.data(), sizeof(float), (size_t)count, f) == (size_t)count;
+        ok = (fclose(f) == 0) && ok;
+        DWG_REQUIRE(ok, "mlp_save: write to %s failed", path);
+        return DWG_OK;
+    })
+}
+
+int dwg_mlp_features(const float* points_dev, int n, float* features_dev, void* stream) {
+    API_GUARD({
+        DWG_REQUIRE(points_dev && features_dev && n >= 2, "mlp_features: bad arguments (n=%d)", n);
+        KnnIndex ix;
+        DWG_TRY(knn_build(ix, points_dev, n, S(stream)));
+        return mlp_features(ix, points_dev, n, features_dev, S(stream));
+    })
+}
+
+int dwg_mlp_forward(dwg_mlp* m, const float* features_dev, long long n, float* out_dev, void* stream) {
+    API_GUARD({
+        DWG_REQUIRE(m && features_dev && out_dev && n >= 0, "mlp_forward: bad arguments");
+        DWG_TRY(mlp_forward(m->m, features_dev, n, out_dev, S(stream)));
+        DWG_CHECK_CUDA(cudaStreamSynchronize(S(stream)));
+        return DWG_OK;
+    })
+}
+
+int dwg_mlp_gradients(dwg_mlp* m, const float* features_dev, const float* targets_dev, long long n,
+                      float* loss_host, float* grads_host, long long count, void* stream) {
+    API_GUARD({
+        DWG_REQUIRE(m && features_dev && targets_dev && grads_host && n >= 1, "mlp_gradients: bad arguments");
+        DWG_REQUIRE(count == mlp_param_count(), "mlp_gradients: count %lld != %lld", count, mlp_param_count());
+        DWG_TRY(mlp_backward(m->m, features_dev, targets_dev, n, loss_host, S(stream)));
+        return mlp_get_grads_flat(m->m, grads_host, S(stream));
+    })
+}
+
+int dwg_mlp_train_step(dwg_mlp* m, const float* features_dev, const float* targets_dev, long long n, float lr,
+                       float* loss_host, void* stream) {
+    API_GUARD({
+        DWG_REQUIRE(m && features_dev && targets_dev && n >= 1, "mlp_train_step: bad arguments");
+        DWG_REQUIRE(lr > 0.f && std::isfinite(lr), "mlp_train_step: learning rate must be positive");
+        DWG_TRY(mlp_backward(m->m, features_dev, targets_dev, n, loss_host, S(stream)));
+        DWG_TRY(mlp_adam(m->m, lr, 0.9f, 0.999f, 1e-8f, S(stream)));
+        DWG_CHECK_CUDA(cudaStreamSynchronize(S(stream)));
+        return DWG_OK;
+    })
+}
+
+int dwg_mlp_init_normals(dwg_mlp* m, const float* points_dev, int n, float* normals_dev, void* stream) {
+    API_GUARD({
+        DWG_REQUIRE(m && points_dev && normals_dev && n >= 2, "mlp_init_normals: bad arguments (n=%d)", n);
+        KnnIndex ix;
+        DWG_TRY(knn_build(ix, points_dev, n, S(stream)));
+        return mlp_init_normals(m->m, ix, points_dev, n, normals_dev, S(stream));
+    })
+}
+
+int dwg_pipeline_create_learned(const float* points_dev, int n, const dwg_params* params, dwg_mlp* init,
+                                void* stream, dwg_pipeline** out) {
+    API_GUARD({
+        DWG_REQUIRE(out && params && init, "pipeline_create_learned: null argument");
+        DWG_REQUIRE(params->in_normal == 4, "pipeline_create_learned: params->in_normal must be 4");
+        *out = nullptr;
+        dwg_pipeline* o = new dwg_pipeline();
+        o->p.init_mlp = &init->m;
+        int st = o->p.setup(points_dev, nullptr, n, *params, S(stream));
+        o->p.init_mlp = nullptr;
+        if (st != DWG_OK) {
+            delete o;
+            return st;
+        }
+        *out = o;
+        return DWG_OK;
+    })
 }
 
 int dwg_reconstruct_host(const float* points_host, const float* normals_host, int n, const dwg_params* params,

@@ -39,9 +39,9 @@ struct Status {
         }                                   \
     } while (0)
 
-#define DWG_TRY(expr)              \
+#define DWG_TRY(...)               \
     do {                           \
-        int _s = (expr);           \
+        int _s = (__VA_ARGS__);    \
         if (_s != DWG_OK) return _s; \
     } while (0)
 

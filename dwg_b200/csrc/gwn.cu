@@ -11,6 +11,8 @@
 // with an optional compensated (two-sum) accumulator per lane.
 #include "gwn.cuh"
 
+#include <vector>
+
 namespace dwg {
 
 constexpr int kGwnWarps = 8;
@@ -41,9 +43,7 @@ __device__ __forceinline__ float rcp_ftz(float x) {
 // PREC < 2 uses the MUFU approximations (sigma_l2e = sigma log2 e);
 // PREC 2 uses correctly rounded sqrt / division and expf.
 template <bool SCREENED, int PREC>
-__device__ __forceinline__ bool gwn_term(float dx, float dy, float dz, float d, float s, float sigma,
-                                         float sigma_l2e, float& v) {
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+__device__ __forceinline__ bool gwn_term_r2(float r2, float d, float s, float sigma, float sigma_l2e, float& v) {
     if (SCREENED) {
         if (!(r2 > 1e-20f)) return false;  // |p - q| <= 1e-10
         const float r = (PREC >= 2) ? sqrtf(r2) : r2 * rsqrt_ftz(r2);
@@ -51,9 +51,11 @@ __device__ __forceinline__ bool gwn_term(float dx, float dy, float dz, float d, 
         const float e = (PREC >= 2) ? expf(sigma * rho) : ex2_ftz(rho * sigma_l2e);
         const float r3 = rho * rho * rho;
         const float den = fmaf(e, kFourPi * r3, 1e-7f);
-        const float num = fmaf(sigma, rho, 1.0f) * d;
-        const float res = (PREC >= 2) ? __fdiv_rn(num, den) : num * rcp_ftz(den);
-        v = copysignf(fabsf(res), d);
+        // the reference forces the sign of d onto the term
+        // (src/TurboLibiGWN.cu:550-584); den > 0, so |sigma rho + 1| d does
+        // that (an operand modifier, no extra instruction)
+        const float num = fabsf(fmaf(sigma, rho, 1.0f)) * d;
+        v = (PREC >= 2) ? __fdiv_rn(num, den) : num * rcp_ftz(den);
         return true;
     } else {
         if (r2 == 0.0f) {
@@ -65,6 +67,12 @@ __device__ __forceinline__ bool gwn_term(float dx, float dy, float dz, float d, 
         v = (PREC >= 2) ? __fdiv_rn(d, den) : d * rcp_ftz(den);
         return true;
     }
+}
+
+template <bool SCREENED, int PREC>
+__device__ __forceinline__ bool gwn_term(float dx, float dy, float dz, float d, float s, float sigma,
+                                         float sigma_l2e, float& v) {
+    return gwn_term_r2<SCREENED, PREC>(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), d, s, sigma, sigma_l2e, v);
 }
 
 template <int PREC>
@@ -79,6 +87,32 @@ __device__ __forceinline__ void acc_add(float& s, float& c, float v) {
         s = t;
         c = __fadd_rn(c, err);
     }
+}
+
+// brick shapes of 32 grid samples (x, y, z extents) a warp evaluates together
+template <int SHAPE>
+struct Brick;
+template <>
+struct Brick<0> {
+    static constexpr int X = 4, Y = 4, Z = 2;
+};
+template <>
+struct Brick<1> {
+    static constexpr int X = 8, Y = 4, Z = 1;
+};
+template <>
+struct Brick<2> {
+    static constexpr int X = 2, Y = 4, Z = 4;
+};
+template <>
+struct Brick<3> {
+    static constexpr int X = 8, Y = 2, Z = 2;
+};
+
+__host__ __device__ inline void brick_extent(int shape, int& x, int& y, int& z) {
+    x = shape == 1 || shape == 3 ? 8 : (shape == 2 ? 2 : 4);
+    y = shape == 3 ? 2 : 4;
+    z = shape == 1 ? 1 : (shape == 0 ? 2 : (shape == 2 ? 4 : 2));
 }
 
 struct GwnArgs {
@@ -104,7 +138,160 @@ struct GwnArgs {
     int num_nodes, num_points;
 };
 
-template <bool GRID, bool SCREENED, int PREC>
+// The sum for the 32 queries of group g (a brick of grid samples, or 32
+// consecutive points); returns this lane's term count.
+template <bool GRID, bool SCREENED, int PREC, int SHAPE>
+__device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g, int lane, int2* __restrict__ stk,
+                                         float sigma, float sigma_l2e) {
+    const unsigned FULL = 0xffffffffu;
+    bool valid;
+    float qx = 0.f, qy = 0.f, qz = 0.f;
+    long long qi;
+    if (GRID) {
+        using B = Brick<SHAPE>;
+        const long long bxi = (long long)(g % (unsigned long long)a.bx);
+        const unsigned long long t = g / (unsigned long long)a.bx;
+        const long long byi = (long long)(t % (unsigned long long)a.by);
+        const long long bzi = (long long)(t / (unsigned long long)a.by);
+        const long long x = bxi * B::X + (lane % B::X), y = byi * B::Y + ((lane / B::X) % B::Y),
+                        z = bzi * B::Z + lane / (B::X * B::Y);
+        valid = x < a.rx && y < a.ry && z < a.rz;
+        qi = x + (long long)a.rx * (y + (long long)a.ry * z);
+        qx = __fadd_rn(a.ox, __fmul_rn((float)x, a.h));
+        qy = __fadd_rn(a.oy, __fmul_rn((float)y, a.h));
+        qz = __fadd_rn(a.oz, __fmul_rn((float)z, a.h));
+    } else {
+        qi = (long long)g * 32 + lane;
+        valid = qi < a.nq;
+        if (valid) {
+            qx = a.q[qi * 3];
+            qy = a.q[qi * 3 + 1];
+            qz = a.q[qi * 3 + 2];
+        }
+    }
+    const unsigned vm = __ballot_sync(FULL, valid);
+    float s = 0.f, c = 0.f;
+    int nterm = 0;
+    auto leaf_points = [&](int start, int cnt) {
+        for (int j = start; j < start + cnt; ++j) {
+            float4 p = a.pa[j];
+            float4 nn = a.nr[j];
+            float dx = p.x - qx, dy = p.y - qy, dz = p.z - qz;
+            float d = p.w * fmaf(dx, nn.x, fmaf(dy, nn.y, dz * nn.z));
+            float sc = a.use_radii ? nn.w : a.screen;
+            float v;
+            if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, sc, sigma, sigma_l2e, v)) {
+                acc_add<PREC>(s, c, v);
+                ++nterm;
+            }
+        }
+    };
+
+    // one child record (level order): a single-point leaf is one term, a
+    // larger leaf is summed point by point, an internal node is a dipole
+    // term when far for this lane and is opened (pushed with the lanes
+    // that need it) otherwise
+    auto child = [&](int cidx, const float4& na, const float4& nb, bool act, int& sp) {
+        const unsigned meta = (unsigned)__float_as_int(nb.w);
+        if (meta & kMetaLeafBit) {
+            if ((meta & kMetaSingle) && !a.use_radii) {
+                if (act) {
+                    const float dx = na.x - qx, dy = na.y - qy, dz = na.z - qz;
+                    const float d = fmaf(dx, nb.x, fmaf(dy, nb.y, dz * nb.z));
+                    float v;
+                    if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, a.screen, sigma, sigma_l2e, v)) {
+                        acc_add<PREC>(s, c, v);
+                        ++nterm;
+                    }
+                }
+            } else {
+                const int st = (int)(meta & kMetaIndex), cnt = __float_as_int(na.w);
+                if (cnt < 0 || st + cnt > a.num_points) {
+                    if (lane == 0) atomicOr(&a.work[1], 4u);
+                } else if (act) {
+                    leaf_points(st, cnt);
+                }
+            }
+            return;
+        }
+        bool near = false;
+        if (act) {
+            // opening test sqrt_rn(d2) > beta*R, d2 in round-to-nearest
+            // single precision (src/TurboLibiGWN.cu:636-644), as one
+            // comparison of d2 with the node's exact threshold
+            const float dx = __fsub_rn(na.x, qx), dy = __fsub_rn(na.y, qy), dz = __fsub_rn(na.z, qz);
+            const float d2 = sq3_rn(dx, dy, dz);
+            if (d2 > na.w) {
+                const float d = fmaf(dx, nb.x, fmaf(dy, nb.y, dz * nb.z));
+                float v;
+                // the far-field distance is the one of the opening test
+                if (gwn_term_r2<SCREENED, PREC>(d2, d, a.screen, sigma, sigma_l2e, v)) {
+                    acc_add<PREC>(s, c, v);
+                    ++nterm;
+                }
+            } else {
+                near = true;
+            }
+        }
+        const unsigned nm = __ballot_sync(FULL, near);
+        if (nm) {
+            if (sp < kGwnStack) {
+                if (lane == 0) stk[sp] = make_int2(cidx, (int)nm);
+                ++sp;
+            } else if (lane == 0) {
+                atomicOr(&a.work[1], 1u);
+            }
+        }
+    };
+
+    int sp = 0;
+    {
+        const float4 ra = a.node_a[0], rb = a.node_b[0];
+        const unsigned rm = (unsigned)__float_as_int(rb.w);
+        if (rm & kMetaLeafBit) {
+            child(0, ra, rb, valid, sp);  // a leaf root is summed; nothing is pushed
+        } else {
+            if (lane == 0) stk[0] = make_int2(0, (int)vm);
+            sp = 1;
+        }
+    }
+    while (sp > 0) {
+        __syncwarp();
+        const int2 e = stk[--sp];
+        __syncwarp();
+        if (e.x < 0 || e.x >= a.num_nodes) {
+            if (lane == 0) atomicOr(&a.work[1], 2u);
+            continue;
+        }
+        const bool act = (((unsigned)e.y) >> lane) & 1u;
+        const unsigned pm = (unsigned)__float_as_int(a.node_b[e.x].w);
+        const int first = (int)(pm & kMetaIndex);
+        const int nch = (int)((pm >> 28) & 7u) + 1;
+        // structural guard: children come after the parent, inside the table
+        if ((pm & kMetaLeafBit) || first <= e.x || first + nch > a.num_nodes) {
+            if (lane == 0) atomicOr(&a.work[1], 2u);
+            continue;
+        }
+        float4 na = a.node_a[first], nb = a.node_b[first];
+        for (int j = 0; j < nch; ++j) {
+            float4 na2, nb2;
+            if (j + 1 < nch) {  // load the next sibling while this one is evaluated
+                na2 = a.node_a[first + j + 1];
+                nb2 = a.node_b[first + j + 1];
+            }
+            child(first + j, na, nb, act, sp);
+            na = na2;
+            nb = nb2;
+        }
+    }
+    if (valid) {
+        a.out[qi] = (PREC == 0) ? s : __fadd_rn(s, c);
+        if (a.per_query_terms) a.per_query_terms[qi] = nterm;
+    }
+    return nterm;
+}
+
+template <bool GRID, bool SCREENED, int PREC, int SHAPE>
 __global__ void __launch_bounds__(kGwnWarps * 32, 4) k_gwn(GwnArgs a) {
     __shared__ int2 stack[kGwnWarps][kGwnStack];
     const unsigned FULL = 0xffffffffu;
@@ -118,152 +305,7 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 4) k_gwn(GwnArgs a) {
         if (lane == 0) g = atomicAdd(&a.work[0], 1u);
         g = __shfl_sync(FULL, g, 0);
         if ((long long)g >= a.ngroups) break;
-        bool valid;
-        float qx = 0.f, qy = 0.f, qz = 0.f;
-        long long qi;
-        if (GRID) {
-            int bxi = (int)(g % (unsigned)a.bx);
-            unsigned t = g / (unsigned)a.bx;
-            int byi = (int)(t % (unsigned)a.by);
-            int bzi = (int)(t / (unsigned)a.by);
-            int x = bxi * 4 + (lane & 3), y = byi * 4 + ((lane >> 2) & 3), z = bzi * 2 + (lane >> 4);
-            valid = x < a.rx && y < a.ry && z < a.rz;
-            qi = (long long)x + (long long)a.rx * ((long long)y + (long long)a.ry * z);
-            qx = __fadd_rn(a.ox, __fmul_rn((float)x, a.h));
-            qy = __fadd_rn(a.oy, __fmul_rn((float)y, a.h));
-            qz = __fadd_rn(a.oz, __fmul_rn((float)z, a.h));
-        } else {
-            qi = (long long)g * 32 + lane;
-            valid = qi < a.nq;
-            if (valid) {
-                qx = a.q[qi * 3];
-                qy = a.q[qi * 3 + 1];
-                qz = a.q[qi * 3 + 2];
-            }
-        }
-        const unsigned vm = __ballot_sync(FULL, valid);
-        float s = 0.f, c = 0.f;
-        int nterm = 0;
-
-        auto leaf_points = [&](int start, int cnt) {
-            for (int j = start; j < start + cnt; ++j) {
-                float4 p = a.pa[j];
-                float4 nn = a.nr[j];
-                float dx = p.x - qx, dy = p.y - qy, dz = p.z - qz;
-                float d = p.w * fmaf(dx, nn.x, fmaf(dy, nn.y, dz * nn.z));
-                float sc = a.use_radii ? nn.w : a.screen;
-                float v;
-                if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, sc, sigma, sigma_l2e, v)) {
-                    acc_add<PREC>(s, c, v);
-                    ++nterm;
-                }
-            }
-        };
-
-        // one child record (level order): a single-point leaf is one term, a
-        // larger leaf is summed point by point, an internal node is a dipole
-        // term when far for this lane and is opened (pushed with the lanes
-        // that need it) otherwise
-        auto child = [&](int cidx, const float4& na, const float4& nb, bool act, int& sp) {
-            const unsigned meta = (unsigned)__float_as_int(nb.w);
-            if (meta & kMetaLeafBit) {
-                if ((meta & kMetaSingle) && !a.use_radii) {
-                    if (act) {
-                        const float dx = na.x - qx, dy = na.y - qy, dz = na.z - qz;
-                        const float d = fmaf(dx, nb.x, fmaf(dy, nb.y, dz * nb.z));
-                        float v;
-                        if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, a.screen, sigma, sigma_l2e, v)) {
-                            acc_add<PREC>(s, c, v);
-                            ++nterm;
-                        }
-                    }
-                } else {
-                    const int st = (int)(meta & kMetaIndex), cnt = __float_as_int(na.w);
-                    if (cnt < 0 || st + cnt > a.num_points) {
-                        if (lane == 0) atomicOr(&a.work[1], 4u);
-                    } else if (act) {
-                        leaf_points(st, cnt);
-                    }
-                }
-                return;
-            }
-            bool near = false;
-            if (act) {
-                // opening test sqrt_rn(d2) > beta*R, d2 in round-to-nearest
-                // single precision (src/TurboLibiGWN.cu:636-644), as a
-                // comparison of d2 with the node's exact threshold
-                const float dx = __fsub_rn(na.x, qx), dy = __fsub_rn(na.y, qy), dz = __fsub_rn(na.z, qz);
-                const float d2 = sq3_rn(dx, dy, dz);
-                const float thr = fabsf(na.w);
-                bool far = d2 > thr;
-                if (!far && d2 == thr && signbit(na.w)) far = __fsqrt_rn(d2) > __fmul_rn(a.beta, a.node_r[cidx]);
-                if (far) {
-                    const float d = fmaf(dx, nb.x, fmaf(dy, nb.y, dz * nb.z));
-                    float v;
-                    if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, a.screen, sigma, sigma_l2e, v)) {
-                        acc_add<PREC>(s, c, v);
-                        ++nterm;
-                    }
-                } else {
-                    near = true;
-                }
-            }
-            const unsigned nm = __ballot_sync(FULL, near);
-            if (nm) {
-                if (sp < kGwnStack) {
-                    if (lane == 0) stack[w][sp] = make_int2(cidx, (int)nm);
-                    ++sp;
-                } else if (lane == 0) {
-                    atomicOr(&a.work[1], 1u);
-                }
-            }
-        };
-
-        int sp = 0;
-        {
-            const float4 ra = a.node_a[0], rb = a.node_b[0];
-            const unsigned rm = (unsigned)__float_as_int(rb.w);
-            if (rm & kMetaLeafBit) {
-                child(0, ra, rb, valid, sp);  // a leaf root is summed; nothing is pushed
-            } else {
-                if (lane == 0) stack[w][0] = make_int2(0, (int)vm);
-                sp = 1;
-            }
-        }
-        while (sp > 0) {
-            __syncwarp();
-            const int2 e = stack[w][--sp];
-            __syncwarp();
-            if (e.x < 0 || e.x >= a.num_nodes) {
-                if (lane == 0) atomicOr(&a.work[1], 2u);
-                continue;
-            }
-            const bool act = (((unsigned)e.y) >> lane) & 1u;
-            const unsigned pm = (unsigned)__float_as_int(a.node_b[e.x].w);
-            const int first = (int)(pm & kMetaIndex);
-            const int nch = (int)((pm >> 28) & 7u) + 1;
-            // structural guard: children come after the parent, inside the table
-            if ((pm & kMetaLeafBit) || first <= e.x || first + nch > a.num_nodes) {
-                if (lane == 0) atomicOr(&a.work[1], 2u);
-                continue;
-            }
-            float4 na = a.node_a[first], nb = a.node_b[first];
-            for (int j = 0; j < nch; ++j) {
-                float4 na2, nb2;
-                if (j + 1 < nch) {  // load the next sibling while this one is evaluated
-                    na2 = a.node_a[first + j + 1];
-                    nb2 = a.node_b[first + j + 1];
-                }
-                child(first + j, na, nb, act, sp);
-                na = na2;
-                nb = nb2;
-            }
-        }
-        if (valid) {
-            a.out[qi] = (PREC == 0) ? s : __fadd_rn(s, c);
-            if (a.per_query_terms) a.per_query_terms[qi] = nterm;
-        }
-        my_terms += (unsigned long long)nterm;
+        my_terms += (unsigned long long)gwn_group<GRID, SCREENED, PREC, SHAPE>(a, g, lane, stack[w], sigma, sigma_l2e);
     }
     if (a.terms_total) {
         for (int o = 16; o > 0; o >>= 1) my_terms += __shfl_down_sync(FULL, my_terms, o);
@@ -271,33 +313,81 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 4) k_gwn(GwnArgs a) {
     }
 }
 
-template <bool GRID, bool SCREENED, int PREC>
+// Grid sums of many clouds in one persistent launch: the groups of all
+// clouds form one work list (prefix[c] = first group of cloud c), taken in
+// order by the warps of the grid, so that small clouds do not idle the GPU.
+template <bool SCREENED, int PREC, int SHAPE>
+__global__ void __launch_bounds__(kGwnWarps * 32, 4)
+    k_gwn_batch(const GwnArgs* __restrict__ table, const unsigned long long* __restrict__ prefix, int nclouds,
+                unsigned long long* __restrict__ work) {
+    __shared__ int2 stack[kGwnWarps][kGwnStack];
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    const unsigned long long total = prefix[nclouds];
+    for (;;) {
+        unsigned long long g = 0;
+        if (lane == 0) g = atomicAdd(work, 1ull);
+        g = __shfl_sync(FULL, g, 0);
+        if (g >= total) break;
+        int lo = 0, hi = nclouds - 1;  // last cloud with prefix <= g
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (prefix[mid] <= g) lo = mid;
+            else hi = mid - 1;
+        }
+        const GwnArgs& a = table[lo];
+        const float sigma = a.sigma_dev ? *a.sigma_dev : a.sigma;
+        int nt = gwn_group<true, SCREENED, PREC, SHAPE>(a, g - prefix[lo], lane, stack[w], sigma,
+                                                       sigma * 1.4426950408889634f);
+        if (a.terms_total) {
+            for (int o = 16; o > 0; o >>= 1) nt += __shfl_down_sync(FULL, nt, o);
+            if (lane == 0 && nt) atomicAdd(a.terms_total, (unsigned long long)nt);
+        }
+    }
+}
+
+template <typename K>
+static int blocks_for(K kernel) {
+    int bps = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kernel, kGwnWarps * 32, 0);
+    return bps > 0 ? bps : 1;
+}
+
+template <bool GRID, bool SCREENED, int PREC, int SHAPE>
 static int launch(const GwnArgs& a, cudaStream_t s) {
     static int blocks_per_sm = 0;
-    if (!blocks_per_sm) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k_gwn<GRID, SCREENED, PREC>,
-                                                      kGwnWarps * 32, 0);
-        if (blocks_per_sm <= 0) blocks_per_sm = 1;
-    }
+    if (!blocks_per_sm) blocks_per_sm = blocks_for(k_gwn<GRID, SCREENED, PREC, SHAPE>);
     long long want = (a.ngroups + kGwnWarps - 1) / kGwnWarps;
     long long grid = (long long)num_sms() * blocks_per_sm;
     if (want < grid) grid = want > 0 ? want : 1;
-    k_gwn<GRID, SCREENED, PREC><<<(unsigned)grid, kGwnWarps * 32, 0, s>>>(a);
+    k_gwn<GRID, SCREENED, PREC, SHAPE><<<(unsigned)grid, kGwnWarps * 32, 0, s>>>(a);
     DWG_CHECK_LAUNCH();
     return DWG_OK;
+}
+
+template <bool GRID, bool SCREENED, int PREC>
+static int launch_shape(const GwnArgs& a, int shape, cudaStream_t s) {
+    if (!GRID) return launch<GRID, SCREENED, PREC, 0>(a, s);
+    switch (shape) {
+        case 1: return launch<GRID, SCREENED, PREC, 1>(a, s);
+        case 2: return launch<GRID, SCREENED, PREC, 2>(a, s);
+        case 3: return launch<GRID, SCREENED, PREC, 3>(a, s);
+        default: return launch<GRID, SCREENED, PREC, 0>(a, s);
+    }
 }
 
 template <bool GRID>
 static int dispatch(const GwnArgs& a, const dwg_gwn_params& p, cudaStream_t s) {
     const int prec = p.precision < 0 ? 0 : (p.precision > 2 ? 2 : p.precision);
     if (p.screened) {
-        if (prec == 0) return launch<GRID, true, 0>(a, s);
-        if (prec == 1) return launch<GRID, true, 1>(a, s);
-        return launch<GRID, true, 2>(a, s);
+        if (prec == 0) return launch_shape<GRID, true, 0>(a, p.tile, s);
+        if (prec == 1) return launch_shape<GRID, true, 1>(a, p.tile, s);
+        return launch_shape<GRID, true, 2>(a, p.tile, s);
     }
-    if (prec == 0) return launch<GRID, false, 0>(a, s);
-    if (prec == 1) return launch<GRID, false, 1>(a, s);
-    return launch<GRID, false, 2>(a, s);
+    if (prec == 0) return launch_shape<GRID, false, 0>(a, p.tile, s);
+    if (prec == 1) return launch_shape<GRID, false, 1>(a, p.tile, s);
+    return launch_shape<GRID, false, 2>(a, p.tile, s);
 }
 
 int gwn_eval(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, float* out,
@@ -347,11 +437,120 @@ int gwn_eval(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, float*
     a.oy = q.origin[1];
     a.oz = q.origin[2];
     a.h = q.spacing;
-    a.bx = (q.res[0] + 3) / 4;
-    a.by = (q.res[1] + 3) / 4;
-    a.ngroups = (long long)a.bx * a.by * ((q.res[2] + 1) / 2);
+    DWG_REQUIRE(p.tile >= 0 && p.tile <= 3, "gwn: tile must be in [0, 3]");
+    int ex, ey, ez;
+    brick_extent(p.tile, ex, ey, ez);
+    a.bx = (q.res[0] + ex - 1) / ex;
+    a.by = (q.res[1] + ey - 1) / ey;
+    a.ngroups = (long long)a.bx * a.by * ((q.res[2] + ez - 1) / ez);
     DWG_REQUIRE(a.ngroups < (1ll << 32), "gwn: grid too large");
     return dispatch<true>(a, p, s);
+}
+
+// ------------------------------------------------------------- batches --
+static void fill_args(GwnArgs& a, const Octree& t, const GwnBatchItem& it, const dwg_gwn_params& p) {
+    a.info = t.info.ptr;
+    a.node_a = t.node_a.ptr;
+    a.node_b = t.node_b.ptr;
+    a.node_r = t.node_r.ptr;
+    a.pa = t.pa.ptr;
+    a.nr = t.nr.ptr;
+    a.beta = p.beta;
+    a.sigma = p.sigma;
+    a.sigma_dev = it.sigma_dev;
+    a.screen = p.screen;
+    a.use_radii = p.use_radii;
+    a.q = nullptr;
+    a.rx = it.res[0];
+    a.ry = it.res[1];
+    a.rz = it.res[2];
+    a.nq = (long long)a.rx * a.ry * a.rz;
+    a.ox = it.origin[0];
+    a.oy = it.origin[1];
+    a.oz = it.origin[2];
+    a.h = it.spacing;
+    int ex, ey, ez;
+    brick_extent(p.tile, ex, ey, ez);
+    a.bx = (a.rx + ex - 1) / ex;
+    a.by = (a.ry + ey - 1) / ey;
+    a.ngroups = (long long)a.bx * a.by * ((a.rz + ez - 1) / ez);
+    a.out = it.out;
+    a.terms_total = it.terms_total;
+    a.per_query_terms = nullptr;
+    a.work = t.work.ptr;  // error word at [1]
+    a.num_nodes = t.M;
+    a.num_points = t.n;
+}
+
+struct GwnBatchImpl {
+    DevBuf<GwnArgs> table;
+    DevBuf<unsigned long long> prefix, work;
+    int n = 0;
+    dwg_gwn_params p{};
+};
+
+GwnBatch::~GwnBatch() { delete impl; }
+
+int gwn_batch_prepare(GwnBatch& b, const GwnBatchItem* items, int n, const dwg_gwn_params& p, cudaStream_t s) {
+    DWG_REQUIRE(items && n >= 1, "gwn batch: no clouds");
+    DWG_REQUIRE(p.screened, "gwn batch: screened sums only");
+    DWG_REQUIRE(p.tile >= 0 && p.tile <= 3, "gwn batch: tile must be in [0, 3]");
+    if (!b.impl) b.impl = new GwnBatchImpl();
+    GwnBatchImpl& B = *b.impl;
+    std::vector<GwnArgs> host((size_t)n);
+    std::vector<unsigned long long> pre((size_t)n + 1, 0);
+    for (int i = 0; i < n; ++i) {
+        DWG_REQUIRE(items[i].tree && items[i].tree->M > 0 && items[i].out, "gwn batch: cloud %d is incomplete", i);
+        DWG_REQUIRE(items[i].res[0] > 0 && items[i].res[1] > 0 && items[i].res[2] > 0,
+                    "gwn batch: cloud %d has a bad grid", i);
+        DWG_TRY(octree_set_beta(*items[i].tree, items[i].beta > 0.f ? items[i].beta : p.beta, s));
+        fill_args(host[i], *items[i].tree, items[i], p);
+        pre[i + 1] = pre[i] + (unsigned long long)host[i].ngroups;
+    }
+    DWG_TRY(B.table.reserve(n));
+    DWG_TRY(B.prefix.reserve(n + 1));
+    DWG_TRY(B.work.reserve(1));
+    DWG_CHECK_CUDA(cudaMemcpyAsync(B.table.ptr, host.data(), sizeof(GwnArgs) * n, cudaMemcpyHostToDevice, s));
+    DWG_CHECK_CUDA(cudaMemcpyAsync(B.prefix.ptr, pre.data(), sizeof(unsigned long long) * (n + 1),
+                                   cudaMemcpyHostToDevice, s));
+    DWG_CHECK_CUDA(cudaStreamSynchronize(s));  // host vectors go out of scope
+    B.n = n;
+    B.p = p;
+    b.groups = pre[n];
+    return DWG_OK;
+}
+
+template <bool SCREENED, int PREC, int SHAPE>
+static int launch_batch(GwnBatchImpl& B, unsigned long long groups, cudaStream_t s) {
+    static int bps = 0;
+    if (!bps) bps = blocks_for(k_gwn_batch<SCREENED, PREC, SHAPE>);
+    long long want = (long long)((groups + kGwnWarps - 1) / kGwnWarps);
+    long long grid = (long long)num_sms() * bps;
+    if (want < grid) grid = want > 0 ? want : 1;
+    k_gwn_batch<SCREENED, PREC, SHAPE><<<(unsigned)grid, kGwnWarps * 32, 0, s>>>(B.table.ptr, B.prefix.ptr, B.n,
+                                                                                 B.work.ptr);
+    DWG_CHECK_LAUNCH();
+    return DWG_OK;
+}
+
+template <int PREC>
+static int launch_batch_shape(GwnBatchImpl& B, unsigned long long groups, cudaStream_t s) {
+    switch (B.p.tile) {
+        case 1: return launch_batch<true, PREC, 1>(B, groups, s);
+        case 2: return launch_batch<true, PREC, 2>(B, groups, s);
+        case 3: return launch_batch<true, PREC, 3>(B, groups, s);
+        default: return launch_batch<true, PREC, 0>(B, groups, s);
+    }
+}
+
+int gwn_batch_launch(GwnBatch& b, cudaStream_t s) {
+    DWG_REQUIRE(b.impl && b.impl->n > 0, "gwn batch: not prepared");
+    GwnBatchImpl& B = *b.impl;
+    DWG_CHECK_CUDA(cudaMemsetAsync(B.work.ptr, 0, sizeof(unsigned long long), s));
+    const int prec = B.p.precision < 0 ? 0 : (B.p.precision > 2 ? 2 : B.p.precision);
+    if (prec == 0) return launch_batch_shape<0>(B, b.groups, s);
+    if (prec == 1) return launch_batch_shape<1>(B, b.groups, s);
+    return launch_batch_shape<2>(B, b.groups, s);
 }
 
 }  // namespace dwg

@@ -22,4 +22,32 @@ int gwn_eval(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, float*
              unsigned long long* terms_total, int* per_query_terms, cudaStream_t s,
              const float* sigma_dev = nullptr);
 
+// Grid sums of many clouds in one persistent launch (screened).  prepare()
+// records the clouds' octrees, grids and outputs once (host work, not
+// capturable); launch() is two stream operations and can be captured in a
+// CUDA graph and replayed while the octrees' moments change in place.
+struct GwnBatchItem {
+    Octree* tree = nullptr;
+    int res[3] = {0, 0, 0};
+    float origin[3] = {0, 0, 0};
+    float spacing = 0;
+    float* out = nullptr;
+    unsigned long long* terms_total = nullptr;  // nullable
+    const float* sigma_dev = nullptr;           // nullable: p.sigma
+    float beta = 0.f;                           // opening ratio of this cloud (0: p.beta)
+};
+
+struct GwnBatchImpl;
+struct GwnBatch {
+    GwnBatchImpl* impl = nullptr;
+    unsigned long long groups = 0;
+    GwnBatch() = default;
+    GwnBatch(const GwnBatch&) = delete;
+    GwnBatch& operator=(const GwnBatch&) = delete;
+    ~GwnBatch();
+};
+
+int gwn_batch_prepare(GwnBatch& b, const GwnBatchItem* items, int n, const dwg_gwn_params& p, cudaStream_t s);
+int gwn_batch_launch(GwnBatch& b, cudaStream_t s);
+
 }  // namespace dwg

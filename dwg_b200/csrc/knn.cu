@@ -13,6 +13,7 @@
 #include <cub/cub.cuh>
 
 #include <climits>
+#include <vector>
 
 #include "knn.cuh"
 #include "octree.cuh"
@@ -47,6 +48,73 @@ __global__ void k_knn_scatter(const float* __restrict__ P, int n, const int* __r
     if (i >= n) return;
     int slot = atomicAdd(&fill[cell_of[i]], 1);
     pts[slot] = make_float4(P[(size_t)i * 3], P[(size_t)i * 3 + 1], P[(size_t)i * 3 + 2], __int_as_float(i));
+}
+
+// level 1 of the occupancy pyramid from the cell ranges
+__global__ void k_pyr_first(const int* __restrict__ cell_start, int G0, int G1, int G2, int D0, int D1, int D2,
+                            unsigned char* __restrict__ occ) {
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= (long long)D0 * D1 * D2) return;
+    const int i = (int)(c % D0), j = (int)((c / D0) % D1), k = (int)(c / ((long long)D0 * D1));
+    unsigned char o = 0;
+    for (int t = 0; t < 8; ++t) {
+        const int x = 2 * i + (t & 1), y = 2 * j + ((t >> 1) & 1), z = 2 * k + (t >> 2);
+        if (x >= G0 || y >= G1 || z >= G2) continue;
+        const long long f = x + (long long)G0 * (y + (long long)G1 * z);
+        o |= cell_start[f + 1] > cell_start[f] ? 1 : 0;
+    }
+    occ[c] = o;
+}
+
+// level l >= 2 from level l - 1
+__global__ void k_pyr_next(const unsigned char* __restrict__ prev, int P0, int P1, int P2, int D0, int D1, int D2,
+                           unsigned char* __restrict__ occ) {
+    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= (long long)D0 * D1 * D2) return;
+    const int i = (int)(c % D0), j = (int)((c / D0) % D1), k = (int)(c / ((long long)D0 * D1));
+    unsigned char o = 0;
+    for (int t = 0; t < 8; ++t) {
+        const int x = 2 * i + (t & 1), y = 2 * j + ((t >> 1) & 1), z = 2 * k + (t >> 2);
+        if (x >= P0 || y >= P1 || z >= P2) continue;
+        o |= prev[x + (long long)P0 * (y + (long long)P1 * z)];
+    }
+    occ[c] = o;
+}
+
+static int build_pyramid(KnnIndex& ix, cudaStream_t s) {
+    ix.levels = 0;
+    int d[3] = {ix.G[0], ix.G[1], ix.G[2]};
+    ix.ldim[0][0] = d[0];
+    ix.ldim[0][1] = d[1];
+    ix.ldim[0][2] = d[2];
+    long long total = 0;
+    int L = 0;
+    while (d[0] > 1 || d[1] > 1 || d[2] > 1) {
+        DWG_REQUIRE(L + 1 < KnnIndex::kMaxLevels, "knn: grid too large for the occupancy pyramid");
+        ++L;
+        for (int t = 0; t < 3; ++t) {
+            d[t] = (d[t] + 1) / 2;
+            ix.ldim[L][t] = d[t];
+        }
+        ix.loff[L] = total;
+        total += (long long)d[0] * d[1] * d[2];
+    }
+    if (L == 0) return DWG_OK;
+    DWG_TRY(ix.occ.reserve(total));
+    for (int l = 1; l <= L; ++l) {
+        const int* D = ix.ldim[l];
+        const long long m = (long long)D[0] * D[1] * D[2];
+        if (l == 1)
+            k_pyr_first<<<div_up(m, 256), 256, 0, s>>>(ix.cell_start.ptr, ix.G[0], ix.G[1], ix.G[2], D[0], D[1], D[2],
+                                                       ix.occ.ptr + ix.loff[1]);
+        else
+            k_pyr_next<<<div_up(m, 256), 256, 0, s>>>(ix.occ.ptr + ix.loff[l - 1], ix.ldim[l - 1][0],
+                                                      ix.ldim[l - 1][1], ix.ldim[l - 1][2], D[0], D[1], D[2],
+                                                      ix.occ.ptr + ix.loff[l]);
+        DWG_CHECK_LAUNCH();
+    }
+    ix.levels = L;
+    return DWG_OK;
 }
 
 int knn_build(KnnIndex& ix, const float* P, int n, cudaStream_t s) {
@@ -110,6 +178,7 @@ int knn_build(KnnIndex& ix, const float* P, int n, cudaStream_t s) {
                                    cudaMemcpyDeviceToDevice, s));
     k_knn_scatter<<<div_up(n, 256), 256, 0, s>>>(P, n, cell_of.ptr, ix.cell_fill.ptr, ix.pts.ptr);
     DWG_CHECK_LAUNCH();
+    DWG_TRY(build_pyramid(ix, s));
     DWG_CHECK_CUDA(cudaStreamSynchronize(s));
     return DWG_OK;
 }
@@ -133,6 +202,11 @@ struct KnnArgs {
     int* __restrict__ q_key;
     int* __restrict__ q_hist;
     int morton_shift;
+    // occupancy pyramid
+    const unsigned char* __restrict__ occ;
+    int levels;
+    int ldim[KnnIndex::kMaxLevels][3];
+    long long loff[KnnIndex::kMaxLevels];
 };
 
 __device__ __forceinline__ long long knn_count(const KnnArgs& a) {
@@ -207,6 +281,14 @@ struct TopK {
         mx = ~0ull;
         mpos = 0;
     }
+    // k slots holding the key T: only keys below T enter, and T must bound
+    // the k-th key from above so that every slot is replaced
+    __device__ __forceinline__ void init_bound(int k, unsigned long long T) {
+#pragma unroll
+        for (int q = 0; q < KMAX; ++q) e[q] = q < k ? T : 0ull;
+        mx = T;
+        mpos = 0;
+    }
     // replace the maximum by v (v < mx) and find the new maximum
     __device__ __forceinline__ void replace_max(unsigned long long v) {
 #pragma unroll
@@ -253,6 +335,77 @@ struct TopK {
         }
     }
 };
+
+// Exact continuation of a query's search over the occupancy pyramid, after
+// the Chebyshev shells 0 and 1 around its cell (cx, cy, cz) were scanned.
+// Depth-first from the 1x1x1 top level, the children of a node in the order
+// of their octant's distance from the query's octant (same octant, then the
+// three face neighbours, the three edge neighbours, the opposite one); a
+// node is skipped when it is empty or its (eps-widened) box is farther than
+// the current k-th candidate.  The walk is stackless: a 4-bit child counter
+// per level in one 64-bit word and the current node's coordinates.
+template <int KMAX>
+__device__ __forceinline__ void knn_pyramid(const KnnArgs& a, float qx, float qy, float qz, int cx, int cy, int cz,
+                                            TopK<KMAX>& top) {
+    const unsigned long long NONE = ~0ull;
+    const float h = a.g.h;
+    const float eps = 1e-4f * h + 1e-6f;
+    const int top_l = a.levels;
+    int lvl = top_l, ci = 0, cj = 0, ck = 0;
+    unsigned long long ctr = 0;
+    for (;;) {
+        const int sh = 4 * lvl;
+        const int c = (int)((ctr >> sh) & 15ull);
+        if (c == 8) {
+            if (lvl == top_l) break;
+            ctr &= ~(15ull << sh);
+            ++lvl;
+            ci >>= 1;
+            cj >>= 1;
+            ck >>= 1;
+            continue;
+        }
+        ctr += 1ull << sh;
+        // octant of the query about the node's midpoint
+        const int half = 1 << (lvl - 1);
+        const float mx = a.g.lo0 + (float)((ci << lvl) + half) * h;
+        const float my = a.g.lo1 + (float)((cj << lvl) + half) * h;
+        const float mz = a.g.lo2 + (float)((ck << lvl) + half) * h;
+        const int qo = (qx >= mx ? 1 : 0) | (qy >= my ? 2 : 0) | (qz >= mz ? 4 : 0);
+        const int oc = qo ^ (int)((0x76534210u >> (4 * c)) & 7u);
+        const int nl = lvl - 1;
+        const int ni = (ci << 1) | (oc & 1), nj = (cj << 1) | ((oc >> 1) & 1), nk = (ck << 1) | (oc >> 2);
+        if (ni >= a.ldim[nl][0] || nj >= a.ldim[nl][1] || nk >= a.ldim[nl][2]) continue;
+        const float kd2 = top.mx == NONE ? INFINITY : __uint_as_float((unsigned)(top.mx >> 32)) * 1.00001f;
+        const float x0 = a.g.lo0 + (float)(ni << nl) * h - eps, x1 = a.g.lo0 + (float)((ni + 1) << nl) * h + eps;
+        const float y0 = a.g.lo1 + (float)(nj << nl) * h - eps, y1 = a.g.lo1 + (float)((nj + 1) << nl) * h + eps;
+        const float z0 = a.g.lo2 + (float)(nk << nl) * h - eps, z1 = a.g.lo2 + (float)((nk + 1) << nl) * h + eps;
+        const float ddx = fmaxf(0.f, fmaxf(x0 - qx, qx - x1));
+        const float ddy = fmaxf(0.f, fmaxf(y0 - qy, qy - y1));
+        const float ddz = fmaxf(0.f, fmaxf(z0 - qz, qz - z1));
+        if (ddx * ddx + ddy * ddy + ddz * ddz > kd2) continue;
+        if (nl == 0) {
+            if (abs(ni - cx) <= 1 && abs(nj - cy) <= 1 && abs(nk - cz) <= 1) continue;  // scanned already
+            const int cell = ni + a.g.G0 * (nj + a.g.G1 * nk);
+            const int e = a.cell_start[cell + 1];
+            for (int t = a.cell_start[cell]; t < e; ++t) {
+                const float4 pp = a.pts[t];
+                const int id = __float_as_int(pp.w);
+                if (a.exclude && a.exclude[id]) continue;
+                const float d2 = sq3_rn(__fsub_rn(pp.x, qx), __fsub_rn(pp.y, qy), __fsub_rn(pp.z, qz));
+                const unsigned long long v = ((unsigned long long)__float_as_uint(d2) << 32) | (unsigned)id;
+                if (v < top.mx) top.replace_max(v);
+            }
+            continue;
+        }
+        const int* D = a.ldim[nl];
+        if (!a.occ[a.loff[nl] + ni + (long long)D[0] * (nj + (long long)D[1] * nk)]) continue;
+        lvl = nl;
+        ci = ni;
+        cj = nj;
+        ck = nk;
+    }
+}
 
 // One thread per query; queries are processed in the order of their coarse
 // Morton bucket so that neighbouring threads search neighbouring cells.  A
@@ -329,6 +482,10 @@ __global__ void __launch_bounds__(128) k_knn_thread(KnnArgs a) {
                 bd -= eps;
                 if (bd > 0.f && __uint_as_float((unsigned)(top.mx >> 32)) < bd * bd * 0.9999f) break;
             }
+            if (r == 1 && a.levels > 0) {
+                knn_pyramid<KMAX>(a, qx, qy, qz, cx, cy, cz, top);
+                break;
+            }
         }
         top.sort();
         // slots >= k hold 0 (below every key) and sort first; results start at KMAX - k
@@ -337,6 +494,361 @@ __global__ void __launch_bounds__(128) k_knn_thread(KnnArgs a) {
             const int o = t - (KMAX - k);
             if (o >= 0) a.out[qi * k + o] = top.e[t] == NONE ? -1 : (int)(unsigned)(top.e[t] & 0xffffffffu);
         }
+    }
+}
+
+// ------------------------------------------------------ cell-grouped path --
+// Queries with k <= 16 and no exclusion are grouped by the grid cell they fall
+// in (clamped to the grid).  For cell c with centre x_c, kb[c] bounds the
+// distance from x_c to its 16th nearest point from above, and m_c is the
+// largest |q - x_c| over the cell's queries.  By the triangle inequality the
+// k nearest points of every such query lie within R_c = kb[c] + 2 m_c of x_c,
+// so one warp gathers that candidate set once (occupancy pyramid, then
+// cells, then points, all 32 lanes in step) into shared memory and every lane
+// then ranks the same candidates for its own query: no divergence, one search
+// per cell instead of one per query.  A cell whose candidate set does not fit
+// (or has no finite bound) sends its queries to the per-thread search.
+constexpr int kCqWarps = 2;
+constexpr int kCqNodes = 2048;  // frontier capacity per warp (ping-pong pair, shared memory)
+constexpr int kCqCands = 4096;  // candidate capacity per warp (global scratch, one slot per warp)
+constexpr int kCqChunk = 256;   // candidates staged in shared memory at a time
+
+__device__ __forceinline__ float cell_mid(float lo, int i, float h) { return lo + ((float)i + 0.5f) * h; }
+
+// kb from the 3x3x3 block around each cell: the 16th smallest distance, or
+// +inf when the block holds fewer than 16 points
+__global__ void k_kb_local(KnnGrid g, const int* __restrict__ cell_start, const float4* __restrict__ pts,
+                           float* __restrict__ kb) {
+    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= (long long)g.G0 * g.G1 * g.G2) return;
+    const int i = (int)(c % g.G0), j = (int)((c / g.G0) % g.G1), k = (int)(c / ((long long)g.G0 * g.G1));
+    const float x = cell_mid(g.lo0, i, g.h), y = cell_mid(g.lo1, j, g.h), z = cell_mid(g.lo2, k, g.h);
+    float d[kKnnBoundK];
+#pragma unroll
+    for (int t = 0; t < kKnnBoundK; ++t) d[t] = INFINITY;
+    float mx = INFINITY;
+    int mpos = 0, cnt = 0;
+    for (int dz = -1; dz <= 1; ++dz) {
+        const int zz = k + dz;
+        if (zz < 0 || zz >= g.G2) continue;
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int yy = j + dy;
+            if (yy < 0 || yy >= g.G1) continue;
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int xx = i + dx;
+                if (xx < 0 || xx >= g.G0) continue;
+                const int cc = xx + g.G0 * (yy + g.G1 * zz);
+                const int e = cell_start[cc + 1];
+                for (int t = cell_start[cc]; t < e; ++t) {
+                    const float4 p = pts[t];
+                    const float ex = p.x - x, ey = p.y - y, ez = p.z - z;
+                    const float d2 = ex * ex + ey * ey + ez * ez;
+                    ++cnt;
+                    if (d2 < mx) {
+#pragma unroll
+                        for (int q = 0; q < kKnnBoundK; ++q)
+                            if (q == mpos) d[q] = d2;
+                        mx = d[0];
+                        mpos = 0;
+#pragma unroll
+                        for (int q = 1; q < kKnnBoundK; ++q)
+                            if (d[q] > mx) {
+                                mx = d[q];
+                                mpos = q;
+                            }
+                    }
+                }
+            }
+        }
+    }
+    kb[c] = cnt >= kKnnBoundK ? sqrtf(mx) * 1.00002f + 1e-7f : INFINITY;
+}
+
+// one min-plus pass with the 26 neighbours at distance `step` cells:
+// kb[c] <= kb[c'] + |x_c - x_c'| (triangle inequality); len1..3 are the
+// neighbour distances rounded up
+__global__ void k_kb_jfa(KnnGrid g, const float* __restrict__ in, float* __restrict__ out, int step, float len1,
+                         float len2, float len3) {
+    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= (long long)g.G0 * g.G1 * g.G2) return;
+    const int i = (int)(c % g.G0), j = (int)((c / g.G0) % g.G1), k = (int)(c / ((long long)g.G0 * g.G1));
+    float v = in[c];
+    for (int dz = -1; dz <= 1; ++dz) {
+        const int zz = k + dz * step;
+        if (zz < 0 || zz >= g.G2) continue;
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int yy = j + dy * step;
+            if (yy < 0 || yy >= g.G1) continue;
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int xx = i + dx * step;
+                if (xx < 0 || xx >= g.G0) continue;
+                const int nz = (dx != 0) + (dy != 0) + (dz != 0);
+                if (nz == 0) continue;
+                const float len = nz == 1 ? len1 : (nz == 2 ? len2 : len3);
+                v = fminf(v, __fadd_ru(in[xx + (long long)g.G0 * (yy + (long long)g.G1 * zz)], len));
+            }
+        }
+    }
+    out[c] = v;
+}
+
+static int build_kbound(const KnnIndex& ix, cudaStream_t s) {
+    const long long ncell = (long long)ix.G[0] * ix.G[1] * ix.G[2];
+    KnnGrid g{ix.G[0], ix.G[1], ix.G[2], ix.lo[0], ix.lo[1], ix.lo[2], ix.h, ix.inv_h};
+    DWG_TRY(ix.kb.reserve(ncell));
+    DWG_TRY(ix.kb_tmp.reserve(ncell));
+    k_kb_local<<<div_up(ncell, 128), 128, 0, s>>>(g, ix.cell_start.ptr, ix.pts.ptr, ix.kb.ptr);
+    DWG_CHECK_LAUNCH();
+    const int gmax = max(ix.G[0], max(ix.G[1], ix.G[2]));
+    int step = 1;
+    while (step * 2 < gmax) step *= 2;
+    std::vector<int> steps;
+    for (int st = step; st >= 1; st /= 2) steps.push_back(st);
+    steps.push_back(1);
+    steps.push_back(1);
+    float* a = ix.kb.ptr;
+    float* b = ix.kb_tmp.ptr;
+    for (int st : steps) {
+        const double hs = (double)st * (double)ix.h;
+        const float l1 = nextafterf((float)hs, INFINITY);
+        const float l2 = nextafterf((float)(hs * 1.4142135623730951), INFINITY);
+        const float l3 = nextafterf((float)(hs * 1.7320508075688772), INFINITY);
+        k_kb_jfa<<<div_up(ncell, 256), 256, 0, s>>>(g, a, b, st, l1, l2, l3);
+        DWG_CHECK_LAUNCH();
+        std::swap(a, b);
+    }
+    if (a != ix.kb.ptr)
+        DWG_CHECK_CUDA(cudaMemcpyAsync(ix.kb.ptr, a, sizeof(float) * ncell, cudaMemcpyDeviceToDevice, s));
+    ix.kb_ready = true;
+    return DWG_OK;
+}
+
+// cell of every query, queries per cell, largest |q - x_c| per cell
+__global__ void k_cq_key(KnnArgs a, int* __restrict__ key, int* __restrict__ count, unsigned int* __restrict__ mbits) {
+    if (a.gate_count && *a.gate_count <= a.gate_min) return;
+    const long long nq = knn_count(a);
+    for (long long qi = blockIdx.x * (long long)blockDim.x + threadIdx.x; qi < nq;
+         qi += (long long)gridDim.x * blockDim.x) {
+        float qx, qy, qz;
+        knn_load_query(a, qi, qx, qy, qz);
+        const int cx = cell_coord(qx, a.g.lo0, a.g.inv_h, a.g.G0);
+        const int cy = cell_coord(qy, a.g.lo1, a.g.inv_h, a.g.G1);
+        const int cz = cell_coord(qz, a.g.lo2, a.g.inv_h, a.g.G2);
+        const int c = cx + a.g.G0 * (cy + a.g.G1 * cz);
+        const float ex = qx - cell_mid(a.g.lo0, cx, a.g.h), ey = qy - cell_mid(a.g.lo1, cy, a.g.h),
+                    ez = qz - cell_mid(a.g.lo2, cz, a.g.h);
+        const float m = sqrtf(ex * ex + ey * ey + ez * ez) * 1.00002f + 1e-7f;
+        key[qi] = c;
+        atomicAdd(&count[c], 1);
+        atomicMax(&mbits[c], __float_as_uint(m));  // non-negative floats order as their bits
+    }
+}
+
+__global__ void k_cq_active(const int* __restrict__ count, long long ncell, int* __restrict__ active,
+                            int* __restrict__ nactive) {
+    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= ncell || count[c] == 0) return;
+    active[atomicAdd(nactive, 1)] = (int)c;
+}
+
+__global__ void k_cq_scatter(KnnArgs a, const int* __restrict__ key, int* __restrict__ fill, int* __restrict__ order) {
+    if (a.gate_count && *a.gate_count <= a.gate_min) return;
+    const long long nq = knn_count(a);
+    for (long long qi = blockIdx.x * (long long)blockDim.x + threadIdx.x; qi < nq;
+         qi += (long long)gridDim.x * blockDim.x)
+        order[atomicAdd(&fill[key[qi]], 1)] = (int)qi;
+}
+
+// is the node (ni, nj, nk) of level l non-empty and within R of (x, y, z)?
+__device__ __forceinline__ bool cq_node_hit(const KnnArgs& a, int l, int ni, int nj, int nk, float x, float y,
+                                            float z, float R2, float eps) {
+    const int* D = a.ldim[l];
+    if (ni < 0 || nj < 0 || nk < 0 || ni >= D[0] || nj >= D[1] || nk >= D[2]) return false;
+    const float h = a.g.h;
+    const float x0 = a.g.lo0 + (float)(ni << l) * h - eps, x1 = a.g.lo0 + (float)((ni + 1) << l) * h + eps;
+    const float y0 = a.g.lo1 + (float)(nj << l) * h - eps, y1 = a.g.lo1 + (float)((nj + 1) << l) * h + eps;
+    const float z0 = a.g.lo2 + (float)(nk << l) * h - eps, z1 = a.g.lo2 + (float)((nk + 1) << l) * h + eps;
+    const float ddx = fmaxf(0.f, fmaxf(x0 - x, x - x1));
+    const float ddy = fmaxf(0.f, fmaxf(y0 - y, y - y1));
+    const float ddz = fmaxf(0.f, fmaxf(z0 - z, z - z1));
+    if (ddx * ddx + ddy * ddy + ddz * ddz > R2) return false;
+    if (l == 0) {
+        const int c = ni + a.g.G0 * (nj + a.g.G1 * nk);
+        return a.cell_start[c + 1] > a.cell_start[c];
+    }
+    return a.occ[a.loff[l] + ni + (long long)D[0] * (nj + (long long)D[1] * nk)] != 0;
+}
+
+template <int KMAX>
+__global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const int* __restrict__ active,
+                                                             const int* __restrict__ misc,
+                                                             const int* __restrict__ cstart,
+                                                             const int* __restrict__ ccount,
+                                                             const unsigned int* __restrict__ mbits,
+                                                             const float* __restrict__ kb,
+                                                             const int* __restrict__ order,
+                                                             int* __restrict__ work, int* __restrict__ fb,
+                                                             float4* __restrict__ cand_scratch) {
+    __shared__ int nodes[kCqWarps][2][kCqNodes];
+    __shared__ float4 stage[kCqWarps][kCqChunk];
+    if (a.gate_count && *a.gate_count <= a.gate_min) return;
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned below = (1u << lane) - 1u;
+    const int nactive = misc[0];
+    const unsigned long long NONE = ~0ull;
+    const float h = a.g.h;
+    const float eps = 1e-4f * h + 1e-6f;
+    const int k = a.k;
+    float4* cand = cand_scratch + (size_t)(blockIdx.x * kCqWarps + w) * kCqCands;
+    for (;;) {
+        int wi = 0;
+        if (lane == 0) wi = atomicAdd(&work[0], 1);
+        wi = __shfl_sync(FULL, wi, 0);
+        if (wi >= nactive) break;
+        const int c = active[wi];
+        const int ci = c % a.g.G0, cj = (c / a.g.G0) % a.g.G1, ck = c / (a.g.G0 * a.g.G1);
+        const float x = cell_mid(a.g.lo0, ci, h), y = cell_mid(a.g.lo1, cj, h), z = cell_mid(a.g.lo2, ck, h);
+        const int qs = cstart[c], qn = ccount[c];
+        float R = (kb[c] + 2.0f * __uint_as_float(mbits[c])) * 1.00002f + 1e-6f * h;
+        bool ok = isfinite(R);
+        int ncand = 0;
+        if (ok) {
+            const float R2 = R * R;
+            // the ball's box in cells
+            const int x0 = cell_coord(x - R, a.g.lo0, a.g.inv_h, a.g.G0), x1 = cell_coord(x + R, a.g.lo0, a.g.inv_h, a.g.G0);
+            const int y0 = cell_coord(y - R, a.g.lo1, a.g.inv_h, a.g.G1), y1 = cell_coord(y + R, a.g.lo1, a.g.inv_h, a.g.G1);
+            const int z0 = cell_coord(z - R, a.g.lo2, a.g.inv_h, a.g.G2), z1 = cell_coord(z + R, a.g.lo2, a.g.inv_h, a.g.G2);
+            // coarsest-enough level: at most 2048 nodes cover the box
+            int l = 0;
+            for (;;) {
+                const long long nn = (long long)((x1 >> l) - (x0 >> l) + 1) * ((y1 >> l) - (y0 >> l) + 1) *
+                                     ((z1 >> l) - (z0 >> l) + 1);
+                if (nn <= 2048 || l >= a.levels) break;
+                ++l;
+            }
+            const int bx = (x1 >> l) - (x0 >> l) + 1, by = (y1 >> l) - (y0 >> l) + 1, bz = (z1 >> l) - (z0 >> l) + 1;
+            const int tot = bx * by * bz;
+            int* cur = nodes[w][0];
+            int* nxt = nodes[w][1];
+            int nf = 0;
+            // stage A: the nodes of level l covering the box
+            for (int b = 0; b < tot; b += 32) {
+                const int t = b + lane;
+                bool keep = false;
+                int id = 0;
+                if (t < tot) {
+                    const int ni = (x0 >> l) + t % bx, nj = (y0 >> l) + (t / bx) % by, nk = (z0 >> l) + t / (bx * by);
+                    keep = cq_node_hit(a, l, ni, nj, nk, x, y, z, R2, eps);
+                    id = ni + a.ldim[l][0] * (nj + a.ldim[l][1] * nk);
+                }
+                const unsigned bal = __ballot_sync(FULL, keep);
+                const int pos = nf + __popc(bal & below);
+                if (keep && pos < kCqNodes) cur[pos] = id;
+                nf += __popc(bal);
+            }
+            ok = nf <= kCqNodes;
+            // stage B: down to the cells
+            for (int lv = l; lv >= 1 && ok; --lv) {
+                __syncwarp();
+                const int* D = a.ldim[lv];
+                int nn = 0;
+                for (int b = 0; b < nf * 8; b += 32) {
+                    const int t = b + lane;
+                    bool keep = false;
+                    int id = 0;
+                    if (t < nf * 8) {
+                        const int node = cur[t >> 3], oc = t & 7;
+                        const int ni = node % D[0], nj = (node / D[0]) % D[1], nk = node / (D[0] * D[1]);
+                        const int ui = 2 * ni + (oc & 1), uj = 2 * nj + ((oc >> 1) & 1), uk = 2 * nk + (oc >> 2);
+                        keep = cq_node_hit(a, lv - 1, ui, uj, uk, x, y, z, R2, eps);
+                        id = ui + a.ldim[lv - 1][0] * (uj + a.ldim[lv - 1][1] * uk);
+                    }
+                    const unsigned bal = __ballot_sync(FULL, keep);
+                    const int pos = nn + __popc(bal & below);
+                    if (keep && pos < kCqNodes) nxt[pos] = id;
+                    nn += __popc(bal);
+                }
+                ok = nn <= kCqNodes;
+                int* tmp = cur;
+                cur = nxt;
+                nxt = tmp;
+                nf = nn;
+            }
+            __syncwarp();
+            // stage C: the points of those cells within R of the centre
+            for (int b = 0; b < nf && ok; b += 32) {
+                const int t = b + lane;
+                int s0 = 0, cnt = 0;
+                if (t < nf) {
+                    const int cell = cur[t];
+                    s0 = a.cell_start[cell];
+                    cnt = a.cell_start[cell + 1] - s0;
+                }
+                const int mx = __reduce_max_sync(FULL, cnt);
+                for (int j = 0; j < mx; ++j) {
+                    bool keep = false;
+                    float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (j < cnt) {
+                        p = a.pts[s0 + j];
+                        const float ex = p.x - x, ey = p.y - y, ez = p.z - z;
+                        keep = ex * ex + ey * ey + ez * ez <= R2;
+                    }
+                    const unsigned bal = __ballot_sync(FULL, keep);
+                    const int pos = ncand + __popc(bal & below);
+                    if (keep && pos < kCqCands) cand[pos] = p;
+                    ncand += __popc(bal);
+                }
+                ok = ncand <= kCqCands;
+            }
+            __syncwarp();
+        }
+        if (!ok) {  // the per-thread search takes this cell's queries
+            for (int t = lane; t < qn; t += 32) fb[atomicAdd(&work[1], 1)] = order[qs + t];
+            continue;
+        }
+        __threadfence_block();  // the candidates written above, visible to the whole warp
+        __syncwarp();
+        // stage D: every lane ranks the same candidates for its own query,
+        // starting from the bound kb[c] + |q - x_c| on its 16th distance
+        const float kbc = kb[c];
+        for (int base = 0; base < qn; base += 32) {
+            const bool has = base + lane < qn;
+            long long qi = 0;
+            float qx = x, qy = y, qz = z;
+            if (has) {
+                qi = order[qs + base + lane];
+                knn_load_query(a, qi, qx, qy, qz);
+            }
+            const float ex = qx - x, ey = qy - y, ez = qz - z;
+            const float rq = (kbc + sqrtf(ex * ex + ey * ey + ez * ez) * 1.00002f) * 1.00002f + 1e-7f;
+            const unsigned long long T = ((unsigned long long)__float_as_uint(rq * rq * 1.00002f) << 32) | 0xffffffffull;
+            TopK<KMAX> top;
+            top.init_bound(k, T);
+            for (int c0 = 0; c0 < ncand; c0 += kCqChunk) {
+                // stage the next chunk of candidates in shared memory (coalesced)
+                const int cn = ncand - c0 < kCqChunk ? ncand - c0 : kCqChunk;
+                __syncwarp();
+                for (int t = lane; t < cn; t += 32) stage[w][t] = cand[c0 + t];
+                __syncwarp();
+                for (int t = 0; t < cn; ++t) {
+                    const float4 pp = stage[w][t];
+                    const float d2 = sq3_rn(__fsub_rn(pp.x, qx), __fsub_rn(pp.y, qy), __fsub_rn(pp.z, qz));
+                    const unsigned long long v = ((unsigned long long)__float_as_uint(d2) << 32) |
+                                                 (unsigned)__float_as_int(pp.w);
+                    if (v < top.mx) top.replace_max(v);
+                }
+            }
+            top.sort();
+            if (has) {
+#pragma unroll
+                for (int t = 0; t < KMAX; ++t) {
+                    const int o = t - (KMAX - k);
+                    if (o >= 0) a.out[qi * k + o] = top.e[t] == NONE ? -1 : (int)(unsigned)(top.e[t] & 0xffffffffu);
+                }
+            }
+        }
+        __syncwarp();
     }
 }
 
@@ -354,6 +866,58 @@ static int knn_launch(const KnnArgs& a, long long nq, cudaStream_t s) {
     k_knn_thread<KMAX><<<(unsigned)blocks, 128, 0, s>>>(a);
     DWG_CHECK_LAUNCH();
     return DWG_OK;
+}
+
+// queries grouped by cell (k <= 16, no exclusion), see k_knn_cells
+static int knn_query_cells(const KnnIndex& ix, const KnnArgs& a0, long long nq, cudaStream_t s) {
+    if (!ix.kb_ready) DWG_TRY(build_kbound(ix, s));
+    const long long ncell = (long long)ix.G[0] * ix.G[1] * ix.G[2];
+    DWG_TRY(ix.c_count.reserve(ncell + 1));
+    DWG_TRY(ix.c_start.reserve(ncell + 1));
+    DWG_TRY(ix.c_fill.reserve(ncell + 1));
+    DWG_TRY(ix.c_m.reserve(ncell));
+    DWG_TRY(ix.c_active.reserve(ncell));
+    DWG_TRY(ix.c_misc.reserve(4));
+    DWG_TRY(ix.q_key.reserve(nq));
+    DWG_TRY(ix.q_order.reserve(nq));
+    DWG_TRY(ix.c_fb.reserve(nq));
+    DWG_CHECK_CUDA(cudaMemsetAsync(ix.c_count.ptr, 0, sizeof(int) * (ncell + 1), s));
+    DWG_CHECK_CUDA(cudaMemsetAsync(ix.c_m.ptr, 0, sizeof(unsigned int) * ncell, s));
+    DWG_CHECK_CUDA(cudaMemsetAsync(ix.c_misc.ptr, 0, sizeof(int) * 4, s));
+    KnnArgs a = a0;
+    long long blocks = (nq + 255) / 256;
+    const long long cap = (long long)num_sms() * 8;
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    k_cq_key<<<(unsigned)blocks, 256, 0, s>>>(a, ix.q_key.ptr, ix.c_count.ptr, ix.c_m.ptr);
+    DWG_CHECK_LAUNCH();
+    size_t bytes = 0;
+    int* cin = ix.c_count.ptr;
+    int* cout = ix.c_start.ptr;
+    DWG_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, cin, cout, (int)(ncell + 1), s));
+    DWG_TRY(ix.c_scratch.reserve(bytes + 256));
+    bytes = ix.c_scratch.n;
+    DWG_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(ix.c_scratch.ptr, bytes, cin, cout, (int)(ncell + 1), s));
+    DWG_CHECK_CUDA(cudaMemcpyAsync(ix.c_fill.ptr, ix.c_start.ptr, sizeof(int) * (ncell + 1), cudaMemcpyDeviceToDevice, s));
+    k_cq_active<<<div_up(ncell, 256), 256, 0, s>>>(ix.c_count.ptr, ncell, ix.c_active.ptr, ix.c_misc.ptr);
+    k_cq_scatter<<<(unsigned)blocks, 256, 0, s>>>(a, ix.q_key.ptr, ix.c_fill.ptr, ix.q_order.ptr);
+    DWG_CHECK_LAUNCH();
+    static int bps = 0;
+    if (!bps) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_knn_cells<16>, kCqWarps * 32, 0);
+        if (bps <= 0) bps = 1;
+    }
+    const long long grid = (long long)num_sms() * bps;
+    DWG_TRY(ix.c_cand.reserve((size_t)grid * kCqWarps * kCqCands));
+    k_knn_cells<16><<<(unsigned)grid, kCqWarps * 32, 0, s>>>(
+        a, ix.c_active.ptr, ix.c_misc.ptr, ix.c_start.ptr, ix.c_count.ptr, ix.c_m.ptr, ix.kb.ptr, ix.q_order.ptr,
+        ix.c_misc.ptr + 1, ix.c_fb.ptr, ix.c_cand.ptr);
+    DWG_CHECK_LAUNCH();
+    // the queries of cells whose candidate sets did not fit
+    KnnArgs f = a;
+    f.order = ix.c_fb.ptr;
+    f.nq_dev_i32 = ix.c_misc.ptr + 2;
+    return knn_launch<16>(f, nq, s);
 }
 
 constexpr int kKnnBuckets = 1 << 15;
@@ -379,6 +943,14 @@ int knn_query(const KnnIndex& ix, const KnnQuery& q, int k, int* out, cudaStream
     a.k = k;
     a.out = out;
     a.morton_shift = ix.morton_shift;
+    a.occ = ix.occ.ptr;
+    a.levels = ix.levels;
+    for (int l = 0; l < KnnIndex::kMaxLevels; ++l) {
+        a.loff[l] = ix.loff[l];
+        for (int t = 0; t < 3; ++t) a.ldim[l][t] = ix.ldim[l][t];
+    }
+    a.order = nullptr;
+    if (k <= kKnnBoundK && !q.exclude && ix.n >= kKnnBoundK && q.use_cells) return knn_query_cells(ix, a, q.nq, s);
     // bucket the queries spatially (counting sort on device counts, no host sync)
     DWG_TRY(ix.q_key.reserve(q.nq));
     DWG_TRY(ix.q_order.reserve(q.nq));

@@ -15,6 +15,22 @@ struct KnnIndex {
     DevBuf<int> cell_fill;
     DevBuf<float> bbox;
     DevBuf<unsigned char> scratch;
+    // occupancy pyramid: level l >= 1 halves the grid (rounding up) and flags
+    // the cells whose 2x2x2 children hold a point; top level is 1x1x1
+    static constexpr int kMaxLevels = 16;
+    int levels = 0;  // top level index (0: no pyramid)
+    int ldim[kMaxLevels][3] = {};
+    long long loff[kMaxLevels] = {};
+    DevBuf<unsigned char> occ;
+    // kb[c] >= distance from the centre of cell c to its kKnnBoundK-th
+    // nearest point (built on the first cell-grouped query)
+    mutable DevBuf<float> kb, kb_tmp;
+    mutable bool kb_ready = false;
+    // workspace of the cell-grouped queries
+    mutable DevBuf<int> c_count, c_start, c_fill, c_active, c_misc, c_fb;
+    mutable DevBuf<unsigned int> c_m;
+    mutable DevBuf<unsigned char> c_scratch;
+    mutable DevBuf<float4> c_cand;  // per-warp candidate slots of the cell-grouped kernel
     // query bucketing workspace (grown on demand; not thread safe)
     int morton_shift = 0;
     mutable DevBuf<int> q_key, q_order, q_hist, q_fill;
@@ -22,6 +38,8 @@ struct KnnIndex {
 };
 
 int knn_build(KnnIndex& ix, const float* points_dev, int n, cudaStream_t s);
+
+constexpr int kKnnBoundK = 16;  // queries with k <= 16 and no exclusion use cell grouping
 
 struct KnnQuery {
     const float* q = nullptr;              // packed xyz, or ...
@@ -33,6 +51,7 @@ struct KnnQuery {
     const unsigned char* exclude = nullptr;  // skip candidates with exclude[idx] != 0
     const int* gate_count = nullptr;       // run only when *gate_count > gate_min
     int gate_min = 0;
+    bool use_cells = true;                 // allow the cell-grouped search (k <= 16)
 };
 
 // out[j*k + i] = index of the i-th nearest; -1 when fewer than k candidates

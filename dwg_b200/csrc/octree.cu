@@ -330,24 +330,33 @@ __global__ void k_depth_key(const int4* __restrict__ info, int M, unsigned* __re
     id[v] = v;
 }
 
-// Open threshold of a node for opening ratio beta: with t = beta*R rounded,
-// sqrt_rn(d2) > t  <=>  d2 > B, B = (t + ulp(t)/2)^2 (exact in FP64), except
-// d2 == B, which rounds half to even and is decided by the exact test.  The
-// float stored is B rounded down, negated when B is itself a float.
+// Open threshold of a node for opening ratio beta.  With t = beta*R rounded,
+// the far test of the reference, sqrt_rn(d2) > t, holds for an up-set of
+// floats d2 (sqrt_rn is monotone), so one float T decides it exactly:
+// far <=> d2 > T, T the largest float d2 that is not far.  Estimate: the
+// boundary is B = (t + ulp(t)/2)^2 (exact in FP64); d2 == B (when B is a
+// float) rounds half to even, i.e. is far exactly when t's last mantissa bit
+// is 1.  The estimate is then confirmed with the test itself.
+__device__ __forceinline__ bool open_far(float d2, float t) { return __fsqrt_rn(d2) > t; }
+
 __global__ void k_node_thr(const float* __restrict__ node_r, const int* __restrict__ meta, int M, float beta,
-                           float4* __restrict__ node_a) {
+                           float4* __restrict__ node_a, unsigned int* __restrict__ err) {
     int v = blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= M) return;
     if ((unsigned)meta[v] & kMetaLeafBit) return;
     const float t = __fmul_rn(beta, node_r[v]);
     float thr;
     if (t == 0.f) {
-        thr = -0.0f;  // every d2 > 0 is far; d2 == 0 takes the exact test
+        thr = 0.0f;  // every d2 > 0 is far
     } else {
         const double hulp = ((double)nextafterf(t, INFINITY) - (double)t) * 0.5;
         const double b = ((double)t + hulp) * ((double)t + hulp);
-        const float bf = __double2float_rd(b);
-        thr = ((double)bf == b) ? -bf : bf;
+        thr = __double2float_rd(b);
+        if ((double)thr == b && (__float_as_uint(t) & 1u)) thr = nextafterf(thr, 0.f);
+        // confirm: thr is not far and the next float is (a few steps at most)
+        for (int it = 0; it < 4 && open_far(thr, t); ++it) thr = nextafterf(thr, 0.f);
+        for (int it = 0; it < 4 && !open_far(nextafterf(thr, INFINITY), t); ++it) thr = nextafterf(thr, INFINITY);
+        if (open_far(thr, t) || !open_far(nextafterf(thr, INFINITY), t)) atomicOr(err, 8u);
     }
     float4 a = node_a[v];
     a.w = thr;
@@ -552,7 +561,8 @@ int octree_update_centres(Octree& t, cudaStream_t s) {
 
 int octree_set_beta(Octree& t, float beta, cudaStream_t s) {
     if (t.thr_beta == beta) return DWG_OK;
-    k_node_thr<<<div_up(t.M, 256), 256, 0, s>>>(t.node_r.ptr, t.node_meta.ptr, t.M, beta, t.node_a.ptr);
+    k_node_thr<<<div_up(t.M, 256), 256, 0, s>>>(t.node_r.ptr, t.node_meta.ptr, t.M, beta, t.node_a.ptr,
+                                                 t.work.ptr + 1);
     DWG_CHECK_LAUNCH();
     t.thr_beta = beta;
     return DWG_OK;

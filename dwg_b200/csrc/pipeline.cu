@@ -288,8 +288,10 @@ int Pipeline::setup(const float* points_dev, const float* normals_dev, int n_poi
     DWG_REQUIRE(p.knn_tri >= 1 && p.knn_tri <= 64 && p.knn_zero >= 1 && p.knn_zero <= 64 && p.kw >= 1 &&
                     p.kw <= 64 && p.final_kw >= 1 && p.final_kw <= 64 && p.normal_kw >= 1 && p.normal_kw <= 64,
                 "pipeline: k values must be in [1, 64]");
-    DWG_REQUIRE(p.in_normal == 0 || p.in_normal == 1 || p.in_normal == 3, "pipeline: in_normal must be 0, 1 or 3");
-    DWG_REQUIRE(p.in_normal == 3 || normals_dev, "pipeline: in_normal %d needs input normals", p.in_normal);
+    DWG_REQUIRE(p.in_normal == 0 || p.in_normal == 1 || p.in_normal == 3 || p.in_normal == 4,
+                "pipeline: in_normal must be 0, 1, 3 or 4");
+    DWG_REQUIRE(p.in_normal >= 3 || normals_dev, "pipeline: in_normal %d needs input normals", p.in_normal);
+    DWG_REQUIRE(p.in_normal != 4 || init_mlp, "pipeline: in_normal 4 needs a learned initialiser");
     prm = p;
     caller = stream;
     DWG_CHECK_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
@@ -326,7 +328,7 @@ int Pipeline::setup(const float* points_dev, const float* normals_dev, int n_poi
     k_gather_xyz<<<div_up(L, 256), 256, 0, s>>>(raw_pos.ptr, t2.perm.ptr, L, leaf_pos.ptr);
     k_fill<<<div_up(L, 256), 256, 0, s>>>(leaf_rad.ptr, L, p.screen);
     DWG_CHECK_LAUNCH();
-    if (p.in_normal != 3) {
+    if (p.in_normal < 3) {
         DWG_TRY(octree_set_point_data(t1, Nin.ptr, nullptr, nullptr, s));
         DevBuf<double> sm, part;
         DWG_TRY(sm.reserve((size_t)L * 3));
@@ -354,6 +356,9 @@ int Pipeline::setup(const float* points_dev, const float* normals_dev, int n_poi
     // iteration grid around the points (include/DWGProcess.h:672)
     DWG_TRY(voxel_grid_host(P.ptr, n, p.offset_1, p.grid_reso, s, gres, gorg, &gh));
     if (p.in_normal == 3) DWG_TRY(gauss_map(leaf_pos.ptr, L, leaf_nrm.ptr, s));
+    // learned initialiser in place of the Gauss map (falls back to it per leaf
+    // where the network output is degenerate)
+    if (p.in_normal == 4) DWG_TRY(mlp_init_normals(*init_mlp, kidx, leaf_pos.ptr, L, leaf_nrm.ptr, s));
     k_set_nr<<<div_up(L, 256), 256, 0, s>>>(t2.nr.ptr, leaf_nrm.ptr, leaf_rad.ptr, L);
     DWG_CHECK_LAUNCH();
     // buffers of one iteration
@@ -381,35 +386,51 @@ int Pipeline::setup(const float* points_dev, const float* normals_dev, int n_poi
     return join_out();
 }
 
-// one DWG iteration, src/TurboDWG.cu:516-657
-int Pipeline::iterate_once() {
-    k_iter_begin<<<1, 1, 0, s>>>(iter_dev.ptr, sigma_tab.ptr, half_tab.ptr, cur_sigma.ptr, cur_half.ptr,
-                                 terms_cur.ptr);
-    DWG_CHECK_LAUNCH();
-    // UpdateMassNormals (:535)
-    k_set_nr<<<div_up(L, 256), 256, 0, s>>>(t2.nr.ptr, leaf_nrm.ptr, nullptr, L);
-    DWG_TRY(octree_update_normals(t2, s));
-    // screened GWN at the leaves and at the grid (:536-537)
-    dwg_gwn_params gp;
+// one DWG iteration, src/TurboDWG.cu:516-657, in three phases so that a
+// batch of clouds can share one launch for the grid sums
+dwg_gwn_params Pipeline::gwn_params() const {
+    dwg_gwn_params gp{};
+    gp.tile = prm.tile;
     gp.beta = prm.beta;
     gp.sigma = prm.lambda;
     gp.screen = prm.screen;
     gp.screened = 1;
     gp.use_radii = prm.use_radii;
     gp.precision = prm.precision;
+    return gp;
+}
+
+// moments, GWN at the leaves, mean iso
+int Pipeline::iterate_pre() {
+    k_iter_begin<<<1, 1, 0, s>>>(iter_dev.ptr, sigma_tab.ptr, half_tab.ptr, cur_sigma.ptr, cur_half.ptr,
+                                 terms_cur.ptr);
+    DWG_CHECK_LAUNCH();
+    // UpdateMassNormals (:535)
+    k_set_nr<<<div_up(L, 256), 256, 0, s>>>(t2.nr.ptr, leaf_nrm.ptr, nullptr, L);
+    DWG_TRY(octree_update_normals(t2, s));
+    // screened GWN at the leaves (:536)
+    const dwg_gwn_params gp = gwn_params();
     GwnQuery ql;
     ql.q = leaf_pos.ptr;
     ql.nq = L;
     DWG_TRY(gwn_eval(t2, ql, gp, wleaf.ptr, terms_cur.ptr, nullptr, s, cur_sigma.ptr));
+    // mean iso value, halved every 5th iteration (:541-550)
+    return mean_to_iso(wleaf.ptr, L, iso_dev.ptr, cur_half.ptr, iso_hist.ptr, iter_dev.ptr, partial, s);
+}
+
+// screened GWN at the grid (:537)
+int Pipeline::iterate_grid() {
     GwnQuery qg;
     for (int d = 0; d < 3; ++d) {
         qg.res[d] = gres[d];
         qg.origin[d] = gorg[d];
     }
     qg.spacing = gh;
-    DWG_TRY(gwn_eval(t2, qg, gp, field.ptr, terms_cur.ptr, nullptr, s, cur_sigma.ptr));
-    // mean iso value, halved every 5th iteration (:541-550)
-    DWG_TRY(mean_to_iso(wleaf.ptr, L, iso_dev.ptr, cur_half.ptr, iso_hist.ptr, iter_dev.ptr, partial, s));
+    return gwn_eval(t2, qg, gwn_params(), field.ptr, terms_cur.ptr, nullptr, s, cur_sigma.ptr);
+}
+
+// marching cubes, kNN, normal update, zero repair
+int Pipeline::iterate_post() {
     // marching cubes at the iso value (:554)
     McGrid g;
     for (int d = 0; d < 3; ++d) {
@@ -433,6 +454,12 @@ int Pipeline::iterate_once() {
                                zero_hist.ptr, terms_hist.ptr);
     DWG_CHECK_LAUNCH();
     return DWG_OK;
+}
+
+int Pipeline::iterate_once() {
+    DWG_TRY(iterate_pre());
+    DWG_TRY(iterate_grid());
+    return iterate_post();
 }
 
 int Pipeline::iterate(int n_iters) {
@@ -468,7 +495,8 @@ int Pipeline::iterate(int n_iters) {
 int Pipeline::finalize() {
     DWG_REQUIRE(!finalized, "pipeline: already finalized");
     DWG_TRY(join_in());
-    dwg_gwn_params gp;
+    dwg_gwn_params gp{};
+    gp.tile = prm.tile;
     gp.beta = prm.beta;
     gp.sigma = prm.lambda;
     gp.screen = prm.screen;

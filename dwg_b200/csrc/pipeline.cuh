@@ -4,6 +4,7 @@
 #include "gwn.cuh"
 #include "knn.cuh"
 #include "mc.cuh"
+#include "mlp.cuh"
 #include "normals.cuh"
 #include "octree.cuh"
 
@@ -11,6 +12,7 @@ namespace dwg {
 
 struct Pipeline {
     dwg_params prm;
+    Mlp* init_mlp = nullptr;        // learned initialiser of in_normal 4 (used during setup only)
     cudaStream_t s = nullptr;       // the pipeline's own non-blocking stream
     cudaStream_t caller = nullptr;  // the stream the caller passed
     cudaEvent_t ev = nullptr;
@@ -64,6 +66,11 @@ struct Pipeline {
               cudaStream_t stream);
     int iterate(int n_iters);
     int iterate_once();
+    // the phases of one iteration on stream s (graph-capturable)
+    int iterate_pre();
+    int iterate_grid();
+    int iterate_post();
+    dwg_gwn_params gwn_params() const;
     int finalize();
     int ensure_hist(int total);
     // order the pipeline stream after the caller's work, and back

@@ -131,7 +131,9 @@ def superquadric_union(n, k=12, outlier_frac=0.01, noise=0.0, seed=0):
     areas = []
     for p in sq:
         a = p["a"]
-        areas.append(4 * np.pi * ((a[0] * a[1]) ** 1.6 + (a[0] * a[2]) ** 1.6 + (a[1] * a[2]) ** 1.6) / 3) ** (1 / 1.6)
+        # ellipsoid surface area, Knud Thomsen's approximation (p = 1.6)
+        areas.append(4 * np.pi * (((a[0] * a[1]) ** 1.6 + (a[0] * a[2]) ** 1.6 + (a[1] * a[2]) ** 1.6) / 3)
+                     ** (1 / 1.6))
     areas = np.array(areas)
     outP, outN, have = [], [], 0
     while have < n:
@@ -164,6 +166,27 @@ def superquadric_union(n, k=12, outlier_frac=0.01, noise=0.0, seed=0):
     return P.astype(np.float32), N.astype(np.float32)
 
 
+def random_cloud(rng, lo, hi, kinds=3):
+    """One cloud of log-uniform size in [lo, hi] from {sphere, torus,
+    3-superquadric union} (``kinds=4`` adds unions of 4-12 superquadrics with
+    1% outliers), noise sigma uniform in [0.001, 0.01]."""
+    n = int(np.exp(rng.uniform(np.log(lo), np.log(hi))))
+    kind = int(rng.integers(0, kinds))
+    sig = float(rng.uniform(0.001, 0.01))
+    s = int(rng.integers(0, 2**31))
+    if kind == 0:
+        P, N = sphere(n, noise=sig, seed=s)
+    elif kind == 1:
+        P, N = torus(n, noise=sig, seed=s)
+    elif kind == 2:
+        P, N = superquadric_union(n, k=3, outlier_frac=0.0, noise=sig, seed=s)
+    else:
+        k = int(rng.integers(4, 13))
+        m = int(round(n / 1.01))
+        P, N = superquadric_union(m, k=k, outlier_frac=0.01, noise=sig, seed=s)
+    return dict(points=P, normals=N, kind=kind, noise=sig)
+
+
 def batch(count=64, lo=2000, hi=200000, seed=0):
     """Clouds of log-uniform size from {sphere, torus, 3-superquadric union},
     noise sigma uniform in [0.001, 0.01]; per-cloud grid resolution
@@ -171,18 +194,10 @@ def batch(count=64, lo=2000, hi=200000, seed=0):
     rng = np.random.default_rng(seed)
     out = []
     for i in range(count):
-        n = int(np.exp(rng.uniform(np.log(lo), np.log(hi))))
-        kind = int(rng.integers(0, 3))
-        sig = float(rng.uniform(0.001, 0.01))
-        s = int(rng.integers(0, 2**31))
-        if kind == 0:
-            P, N = sphere(n, noise=sig, seed=s)
-        elif kind == 1:
-            P, N = torus(n, noise=sig, seed=s)
-        else:
-            P, N = superquadric_union(n, k=3, outlier_frac=0.0, noise=sig, seed=s)
-        res = int(np.clip(round(128 * (n / 2000.0) ** (1 / 3)), 128, 256))
-        out.append(dict(points=P, normals=N, grid_reso=res, kind=kind, noise=sig))
+        c = random_cloud(rng, lo, hi)
+        n = len(c["points"])
+        c["grid_reso"] = int(np.clip(round(128 * (n / 2000.0) ** (1 / 3)), 128, 256))
+        out.append(c)
     return out
 
 

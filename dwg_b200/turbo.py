@@ -50,6 +50,7 @@ class TurboNormalInitialization:
             pass
         capi.check(capi.load().dwg_gauss_map_init(capi.ptr(point_pos), n, capi.ptr(point_normal),
                                                   capi.stream_ptr()))
+        return point_normal
 
 
 class TurboLibiGWN:
@@ -111,14 +112,16 @@ class TurboLibiGWN:
         return self._launch(query_points, i_Normals, i_As, i_radii if use_radii else None, p, out_gwn)
 
     def grid(self, res, origin, spacing, i_Normals=None, i_As=None, beta=2.3, sigma=10.0, screened=True,
-             precision=1, out=None, terms=None, screen=0.0015):
-        """GWN at the closed-form grid origin + index * spacing (x fastest)."""
+             precision=1, out=None, terms=None, screen=0.0015, tile=0):
+        """GWN at the closed-form grid origin + index * spacing (x fastest);
+        ``tile`` picks the brick of samples a warp evaluates together."""
         res = np.ascontiguousarray(res, np.int32)
         org = np.ascontiguousarray(origin, np.float32)
         n = int(np.prod(res.astype(np.int64)))
         if out is None:
             out = torch.empty(n, dtype=torch.float32, device="cuda")
-        p = capi.gwn_params(beta=beta, sigma=sigma, screen=screen, screened=screened, precision=precision)
+        p = capi.gwn_params(beta=beta, sigma=sigma, screen=screen, screened=screened, precision=precision,
+                            tile=tile)
         capi.check(capi.load().dwg_gwn_grid(self._h, capi.ptr(i_Normals), capi.ptr(i_As), None, res.ctypes.data,
                                             org.ctypes.data, float(spacing), C.byref(p), capi.ptr(out),
                                             capi.ptr(terms), capi.stream_ptr()))
@@ -242,13 +245,21 @@ class TurboDWG:
     GPU pipeline: ``TurboDWG(points, normals=None, **flags)``, then
     ``TurboScreenedDWGLaunch(total_iters)`` and ``GenerateMesh()``."""
 
-    def __init__(self, points, normals=None, **flags):
+    def __init__(self, points, normals=None, init_model=None, **flags):
         _req_cuda_f32(points, "points", 3)
+        if init_model is not None:
+            flags["in_normal"] = 4
         self.params = capi.default_params(**flags)
         self.points = points
         self._h = C.c_void_p()
-        capi.check(capi.load().dwg_pipeline_create(capi.ptr(points), capi.ptr(normals), points.shape[0],
-                                                   C.byref(self.params), capi.stream_ptr(), C.byref(self._h)))
+        if init_model is not None:
+            capi.check(capi.load().dwg_pipeline_create_learned(capi.ptr(points), points.shape[0],
+                                                               C.byref(self.params), init_model.handle,
+                                                               capi.stream_ptr(), C.byref(self._h)))
+        else:
+            capi.check(capi.load().dwg_pipeline_create(capi.ptr(points), capi.ptr(normals), points.shape[0],
+                                                       C.byref(self.params), capi.stream_ptr(),
+                                                       C.byref(self._h)))
 
     def TurboScreenedDWGLaunch(self, total_iters=None):
         n = self.params.total_iter if total_iters is None else int(total_iters)
@@ -293,9 +304,100 @@ class TurboDWG:
             pass
 
 
-def reconstruct(points, normals=None, **flags):
+class LearnedNormalInit:
+    """The learned initialiser (replaces ``TurboNormalInitialization::
+    GaussMapInit``, src/TurboNormalInit.cu:3-44, as the source of initial
+    normals): ``LearnedNormalInit(path=None, seed=0)``; ``init_normals(points)``
+    returns unit normals, ``features(points)`` the 12 network inputs,
+    ``train_step(features, targets, lr)`` one Adam step."""
+
+    FEATURES = 12
+
+    def __init__(self, path=None, seed=0):
+        self.handle = C.c_void_p()
+        capi.check(capi.load().dwg_mlp_create(int(seed), capi.stream_ptr(), C.byref(self.handle)))
+        if path is not None:
+            self.load(path)
+
+    @staticmethod
+    def param_count():
+        return int(capi.load().dwg_mlp_param_count())
+
+    def load(self, path):
+        capi.check(capi.load().dwg_mlp_load(self.handle, str(path).encode()))
+
+    def save(self, path):
+        capi.check(capi.load().dwg_mlp_save(self.handle, str(path).encode()))
+
+    def get_params(self):
+        out = np.empty(self.param_count(), np.float32)
+        capi.check(capi.load().dwg_mlp_get_params(self.handle, out.ctypes.data, out.size))
+        return out
+
+    def set_params(self, flat):
+        flat = np.ascontiguousarray(flat, np.float32)
+        capi.check(capi.load().dwg_mlp_set_params(self.handle, flat.ctypes.data, flat.size))
+
+    @staticmethod
+    def features(points, out=None):
+        import torch
+        _req_cuda_f32(points, "points", 3)
+        if out is None:
+            out = torch.empty((points.shape[0], LearnedNormalInit.FEATURES), dtype=torch.float32,
+                              device=points.device)
+        capi.check(capi.load().dwg_mlp_features(capi.ptr(points), points.shape[0], capi.ptr(out),
+                                                capi.stream_ptr()))
+        return out
+
+    def forward(self, features, out=None):
+        import torch
+        _req_cuda_f32(features, "features", self.FEATURES)
+        if out is None:
+            out = torch.empty((features.shape[0], 3), dtype=torch.float32, device=features.device)
+        capi.check(capi.load().dwg_mlp_forward(self.handle, capi.ptr(features), features.shape[0], capi.ptr(out),
+                                               capi.stream_ptr()))
+        return out
+
+    def init_normals(self, points, out=None):
+        import torch
+        _req_cuda_f32(points, "points", 3)
+        if out is None:
+            out = torch.empty_like(points)
+        capi.check(capi.load().dwg_mlp_init_normals(self.handle, capi.ptr(points), points.shape[0], capi.ptr(out),
+                                                    capi.stream_ptr()))
+        return out
+
+    def train_step(self, features, targets, lr):
+        _req_cuda_f32(features, "features", self.FEATURES)
+        _req_cuda_f32(targets, "targets", 3)
+        loss = C.c_float()
+        capi.check(capi.load().dwg_mlp_train_step(self.handle, capi.ptr(features), capi.ptr(targets),
+                                                  features.shape[0], float(lr), C.byref(loss), capi.stream_ptr()))
+        return loss.value
+
+    def gradients(self, features, targets):
+        loss = C.c_float()
+        g = np.empty(self.param_count(), np.float32)
+        capi.check(capi.load().dwg_mlp_gradients(self.handle, capi.ptr(features), capi.ptr(targets),
+                                                 features.shape[0], C.byref(loss), g.ctypes.data, g.size,
+                                                 capi.stream_ptr()))
+        return loss.value, g
+
+    def close(self):
+        if getattr(self, "handle", None) and self.handle.value:
+            capi.load().dwg_mlp_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def reconstruct(points, normals=None, init_model=None, **flags):
     """Full reconstruction on the GPU; returns a dict of host arrays."""
-    d = TurboDWG(points, normals, **flags)
+    d = TurboDWG(points, normals, init_model=init_model, **flags)
     d.TurboScreenedDWGLaunch()
     d.GenerateMesh()
     out = {k: d.get(k) for k in ("leaf_pos", "leaf_nrm", "iso", "tri_count", "zero_count", "terms", "tris",

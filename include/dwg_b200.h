@@ -69,8 +69,8 @@ int dwg_octree_update_info(dwg_octree* tree, const float* normals_dev, const flo
                            void* stream);
 /* Sticky error word of the traversal kernels of this tree (synchronises):
  * 0 = none; bit 0 stack overflow, bit 1 malformed node links, bit 2 leaf
- * range outside the point array.  Any set bit makes the call return
- * DWG_ERR_DEVICE. */
+ * range outside the point array, bit 3 an opening threshold that failed its
+ * self-check.  Any set bit makes the call return DWG_ERR_DEVICE. */
 int dwg_octree_status(const dwg_octree* tree, unsigned int* flags);
 /* Copy the node table to host memory (for checking).  Arrays may be NULL.
  * Nodes are in depth-first pre-order; points are in the octree's sorted
@@ -97,7 +97,10 @@ typedef struct {
     float screen;    /* screen radius s when use_radii == 0, reference 0.0015 */
     int screened;    /* 1 screened kernel, 0 plain kernel */
     int use_radii;   /* 1: s = radii[i] for point terms (far field keeps `screen`) */
-    int precision;   /* 0 plain FP32 accumulation, 1 FP32 compensated (default) */
+    int precision;   /* 0 plain FP32 accumulation, 1 FP32 compensated (default),
+                        2 compensated with correctly rounded sqrt / exp / division */
+    int tile;        /* grid samples per warp: 0 4x4x2 (default), 1 8x4x1,
+                        2 2x4x4, 3 8x2x2 (point queries ignore it) */
 } dwg_gwn_params;
 
 int dwg_gwn_points(dwg_octree* tree, const float* normals_dev, const float* areas_dev,
@@ -217,7 +220,8 @@ int dwg_radii(const float* points_dev, int n, const int* knn_dev, int k, float* 
  * (src/main.cpp:19-39).
  * ------------------------------------------------------------------------ */
 typedef struct {
-    int in_normal;          /* 0 random, 1 input, 3 Gauss map (default) */
+    int in_normal;          /* 0 random, 1 input, 3 Gauss map (default),
+                               4 learned (dwg_pipeline_create_learned) */
     int grid_reso;          /* --grid_reso (400) */
     int final_reso;         /* --final_reso (500) */
     int kw, final_kw, normal_kw; /* 10, 10, 10 */
@@ -235,6 +239,7 @@ typedef struct {
     int knn_zero;           /* 10 */
     int precision;          /* dwg_gwn_params.precision */
     int use_graph;          /* capture one iteration in a CUDA graph and replay it */
+    int tile;               /* dwg_gwn_params.tile of the grid sums */
 } dwg_params;
 
 void dwg_params_default(dwg_params* p);
@@ -260,6 +265,88 @@ int dwg_pipeline_get(dwg_pipeline* p, const char* what, void* dst_host);
 /* device pointer of a pipeline array (no copy): "leaf_pos", "leaf_nrm",
  * "point_nrm", "tris", "field", "final_field" */
 int dwg_pipeline_device_ptr(dwg_pipeline* p, const char* what, void** ptr);
+
+/* ------------------------------------------------------------------------
+ * Batched reconstruction of many clouds (no counterpart in the reference,
+ * which reconstructs one cloud per DWG_CUDA run).  Each cloud is a pipeline
+ * with its own flags (params[i]; in_normal 3, one tile and one precision for
+ * all); one iteration of all clouds is one CUDA graph whose grid sums run as
+ * a single persistent launch over the bricks of every cloud.
+ * ------------------------------------------------------------------------ */
+typedef struct dwg_batch dwg_batch;
+int dwg_batch_create(const float* const* points_dev, const int* counts, int num_clouds, const dwg_params* params,
+                     void* stream, dwg_batch** out);
+int dwg_batch_destroy(dwg_batch* b);
+int dwg_batch_iterate(dwg_batch* b, int n_iters);
+int dwg_batch_finalize(dwg_batch* b);
+/* borrowed handle of cloud `index` for the dwg_pipeline_size / _get /
+ * _device_ptr getters; valid until dwg_batch_destroy, never destroyed by the
+ * caller */
+int dwg_batch_cloud(dwg_batch* b, int index, dwg_pipeline** cloud);
+
+/* ------------------------------------------------------------------------
+ * Autotuner of the grid sums (no counterpart in the reference, which fixes
+ * beta = 2.3 in src/TurboLibiGWN.cu and one thread per query).  For one
+ * cloud it runs `warm_iters` DWG iterations, measures the RMS error of the
+ * Barnes-Hut sums against exact sums at `samples` seeded grid samples for
+ * candidate opening ratios beta in [1.5, 4.5], times a full grid evaluation
+ * for those within `tol`, and then the four brick shapes at the fastest.
+ * ------------------------------------------------------------------------ */
+typedef struct {
+    float beta;     /* chosen opening ratio */
+    int tile;       /* chosen brick shape (dwg_gwn_params.tile) */
+    float rms_err;  /* RMS |w_beta - w_exact| at the samples */
+    float max_err;  /* max  |w_beta - w_exact| at the samples */
+    float grid_ms;  /* one grid evaluation at (beta, tile) */
+    float ref_ms;   /* one grid evaluation at beta 2.3, tile 0 */
+} dwg_tune_result;
+int dwg_autotune(const float* points_dev, int n, const dwg_params* params, float tol, int samples,
+                 int warm_iters, void* stream, dwg_tune_result* out);
+
+/* ------------------------------------------------------------------------
+ * Learned normal initialiser (no counterpart in the reference: it replaces
+ * TurboNormalInitialization::GaussMapInit, include/TurboNormalInit.h:13, as
+ * the source of the leaves' initial normals).  A point-wise MLP
+ * 12 -> 128 -> 128 -> 128 -> 3 (GELU) over covariance features of the 16
+ * nearest points, BF16 weights and activations, FP32 accumulation, trained
+ * with the library's own forward / backward / Adam kernels on DWG-converged
+ * normals.  A handle is used by one thread at a time.
+ * Parameters (host arrays, files): for each layer W [din x dout] row-major
+ * then b [dout], with din = 16, 128, 128, 128 and dout = 128, 128, 128, 8
+ * (inputs padded from 12 to 16, outputs from 3 to 8; padding entries zero).
+ * ------------------------------------------------------------------------ */
+typedef struct dwg_mlp dwg_mlp;
+#define DWG_MLP_FEATURES 12
+long long dwg_mlp_param_count(void);
+/* random initialisation (uniform, fan-in scaled) from `seed` */
+int dwg_mlp_create(unsigned long long seed, void* stream, dwg_mlp** out);
+int dwg_mlp_destroy(dwg_mlp* m);
+int dwg_mlp_set_params(dwg_mlp* m, const float* params_host, long long count);
+int dwg_mlp_get_params(dwg_mlp* m, float* params_host, long long count);
+/* file: 8 bytes "DWGMLP01", int64 count, count little-endian float32 */
+int dwg_mlp_load(dwg_mlp* m, const char* path);
+int dwg_mlp_save(dwg_mlp* m, const char* path);
+/* features_dev [n x 12]: eigenvalues of the covariance of the 16 nearest
+ * points (self included) over their sum, the smallest and the largest
+ * eigenvector turned away from the bounding-box centre, and the offset to the
+ * neighbourhood centroid over the RMS spread */
+int dwg_mlp_features(const float* points_dev, int n, float* features_dev, void* stream);
+/* raw outputs out_dev [n x 3] */
+int dwg_mlp_forward(dwg_mlp* m, const float* features_dev, long long n, float* out_dev, void* stream);
+/* loss = mean(1 - <y/|y|, t>) over the batch; gradients of the flat
+ * parameters into grads_host (count = dwg_mlp_param_count()); no update */
+int dwg_mlp_gradients(dwg_mlp* m, const float* features_dev, const float* targets_dev, long long n,
+                      float* loss_host, float* grads_host, long long count, void* stream);
+/* one Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on one batch */
+int dwg_mlp_train_step(dwg_mlp* m, const float* features_dev, const float* targets_dev, long long n,
+                       float lr, float* loss_host, void* stream);
+/* unit initial normals of n points (features, forward, normalise; the Gauss
+ * map where the output is degenerate) */
+int dwg_mlp_init_normals(dwg_mlp* m, const float* points_dev, int n, float* normals_dev, void* stream);
+/* dwg_pipeline_create with the leaves' initial normals from `init`
+ * (params->in_normal must be 4); `init` is used during the call only */
+int dwg_pipeline_create_learned(const float* points_dev, int n, const dwg_params* params, dwg_mlp* init,
+                                void* stream, dwg_pipeline** out);
 
 /* One call from host memory to host memory: create + iterate(total_iter) +
  * finalize + copy of the mesh and point normals.  tris_host holds up to

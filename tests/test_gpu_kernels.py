@@ -195,6 +195,22 @@ def test_knn_surface_cloud(oracle_lib):
     assert np.array_equal(got, ref)
 
 
+def test_knn_far_queries(oracle_lib):
+    # queries offset from the surface by up to ~25 grid cells, and outside the
+    # points' bounding box: the search continues over the occupancy pyramid
+    P, N = cloud(30000)
+    rng = np.random.default_rng(8)
+    sel = rng.choice(len(P), 3000, replace=False)
+    off = rng.uniform(-0.3, 0.3, (3000, 1)).astype(np.float32)
+    Q = np.concatenate([P[sel] + off * N[sel], rng.uniform(-0.8, 0.8, (500, 3)).astype(np.float32)])
+    Q = np.ascontiguousarray(Q, np.float32)
+    ix = turbo.KnnIndex(cu(P))
+    for k in (1, 10, 15, 40):
+        ref = oracle_lib.knn(P, Q, k)
+        got = ix.query(cu(Q), k).cpu().numpy()
+        assert np.array_equal(got, ref), k
+
+
 def test_diffusion_and_zero_repair_bit_exact(oracle_lib, dwg_lib):
     rng = np.random.default_rng(6)
     L, T, k = 4000, 9000, 15
