@@ -187,53 +187,36 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
         }
     };
 
-    // one child record (level order): a single-point leaf is one term, a
-    // larger leaf is summed point by point, an internal node is a dipole
-    // term when far for this lane and is opened (pushed with the lanes
-    // that need it) otherwise
+    // one child record (level order).  A single-point leaf is always a term;
+    // an internal node is a dipole term when far for this lane (sqrt_rn(d2) >
+    // beta R in round-to-nearest single precision, src/TurboLibiGWN.cu:636-644,
+    // as one comparison of d2 with the node's exact threshold) and is opened
+    // (pushed with the lanes that need it) otherwise; both use the same d2.
+    // Larger leaves (and every leaf when radii apply) are summed point by point.
     auto child = [&](int cidx, const float4& na, const float4& nb, bool act, int& sp) {
         const unsigned meta = (unsigned)__float_as_int(nb.w);
-        if (meta & kMetaLeafBit) {
-            if ((meta & kMetaSingle) && !a.use_radii) {
-                if (act) {
-                    const float dx = na.x - qx, dy = na.y - qy, dz = na.z - qz;
-                    const float d = fmaf(dx, nb.x, fmaf(dy, nb.y, dz * nb.z));
-                    float v;
-                    if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, a.screen, sigma, sigma_l2e, v)) {
-                        acc_add<PREC>(s, c, v);
-                        ++nterm;
-                    }
-                }
-            } else {
-                const int st = (int)(meta & kMetaIndex), cnt = __float_as_int(na.w);
-                if (cnt < 0 || st + cnt > a.num_points) {
-                    if (lane == 0) atomicOr(&a.work[1], 4u);
-                } else if (act) {
-                    leaf_points(st, cnt);
-                }
+        const bool leaf = (meta & kMetaLeafBit) != 0;
+        if (leaf && (!(meta & kMetaSingle) || a.use_radii)) {
+            const int st = (int)(meta & kMetaIndex), cnt = __float_as_int(na.w);
+            if (cnt < 0 || st + cnt > a.num_points) {
+                if (lane == 0) atomicOr(&a.work[1], 4u);
+            } else if (act) {
+                leaf_points(st, cnt);
             }
             return;
         }
-        bool near = false;
-        if (act) {
-            // opening test sqrt_rn(d2) > beta*R, d2 in round-to-nearest
-            // single precision (src/TurboLibiGWN.cu:636-644), as one
-            // comparison of d2 with the node's exact threshold
-            const float dx = __fsub_rn(na.x, qx), dy = __fsub_rn(na.y, qy), dz = __fsub_rn(na.z, qz);
-            const float d2 = sq3_rn(dx, dy, dz);
-            if (d2 > na.w) {
-                const float d = fmaf(dx, nb.x, fmaf(dy, nb.y, dz * nb.z));
-                float v;
-                // the far-field distance is the one of the opening test
-                if (gwn_term_r2<SCREENED, PREC>(d2, d, a.screen, sigma, sigma_l2e, v)) {
-                    acc_add<PREC>(s, c, v);
-                    ++nterm;
-                }
-            } else {
-                near = true;
+        const float dx = __fsub_rn(na.x, qx), dy = __fsub_rn(na.y, qy), dz = __fsub_rn(na.z, qz);
+        const float d2 = sq3_rn(dx, dy, dz);
+        const bool far = leaf || d2 > na.w;
+        if (act && far) {
+            const float d = fmaf(dx, nb.x, fmaf(dy, nb.y, dz * nb.z));
+            float v;
+            if (gwn_term_r2<SCREENED, PREC>(d2, d, a.screen, sigma, sigma_l2e, v)) {
+                acc_add<PREC>(s, c, v);
+                ++nterm;
             }
         }
-        const unsigned nm = __ballot_sync(FULL, near);
+        const unsigned nm = __ballot_sync(FULL, act && !far);
         if (nm) {
             if (sp < kGwnStack) {
                 if (lane == 0) stk[sp] = make_int2(cidx, (int)nm);

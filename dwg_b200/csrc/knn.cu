@@ -81,7 +81,8 @@ __global__ void k_pyr_next(const unsigned char* __restrict__ prev, int P0, int P
     occ[c] = o;
 }
 
-static int build_pyramid(KnnIndex& ix, cudaStream_t s) {
+// level dimensions and offsets of the occupancy pyramid of ix's grid
+static int pyramid_dims(KnnIndex& ix) {
     ix.levels = 0;
     int d[3] = {ix.G[0], ix.G[1], ix.G[2]};
     ix.ldim[0][0] = d[0];
@@ -99,9 +100,14 @@ static int build_pyramid(KnnIndex& ix, cudaStream_t s) {
         ix.loff[L] = total;
         total += (long long)d[0] * d[1] * d[2];
     }
-    if (L == 0) return DWG_OK;
-    DWG_TRY(ix.occ.reserve(total));
-    for (int l = 1; l <= L; ++l) {
+    ix.levels = L;
+    if (L > 0) DWG_TRY(ix.occ.reserve(total));
+    return DWG_OK;
+}
+
+// the occupancy flags of every level from ix.cell_start (stream-ordered)
+static int pyramid_fill(KnnIndex& ix, cudaStream_t s) {
+    for (int l = 1; l <= ix.levels; ++l) {
         const int* D = ix.ldim[l];
         const long long m = (long long)D[0] * D[1] * D[2];
         if (l == 1)
@@ -113,8 +119,12 @@ static int build_pyramid(KnnIndex& ix, cudaStream_t s) {
                                                       ix.occ.ptr + ix.loff[l]);
         DWG_CHECK_LAUNCH();
     }
-    ix.levels = L;
     return DWG_OK;
+}
+
+static int build_pyramid(KnnIndex& ix, cudaStream_t s) {
+    DWG_TRY(pyramid_dims(ix));
+    return pyramid_fill(ix, s);
 }
 
 int knn_build(KnnIndex& ix, const float* P, int n, cudaStream_t s) {
@@ -510,7 +520,6 @@ __global__ void __launch_bounds__(128) k_knn_thread(KnnArgs a) {
 // (or has no finite bound) sends its queries to the per-thread search.
 constexpr int kCqWarps = 2;
 constexpr int kCqNodes = 2048;  // frontier capacity per warp (ping-pong pair, shared memory)
-constexpr int kCqCands = 4096;  // candidate capacity per warp (global scratch, one slot per warp)
 constexpr int kCqChunk = 256;   // candidates staged in shared memory at a time
 
 __device__ __forceinline__ float cell_mid(float lo, int i, float h) { return lo + ((float)i + 0.5f) * h; }
@@ -687,8 +696,7 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
                                                              const unsigned int* __restrict__ mbits,
                                                              const float* __restrict__ kb,
                                                              const int* __restrict__ order,
-                                                             int* __restrict__ work, int* __restrict__ fb,
-                                                             float4* __restrict__ cand_scratch) {
+                                                             int* __restrict__ work, int* __restrict__ fb) {
     __shared__ int nodes[kCqWarps][2][kCqNodes];
     __shared__ float4 stage[kCqWarps][kCqChunk];
     if (a.gate_count && *a.gate_count <= a.gate_min) return;
@@ -700,7 +708,6 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
     const float h = a.g.h;
     const float eps = 1e-4f * h + 1e-6f;
     const int k = a.k;
-    float4* cand = cand_scratch + (size_t)(blockIdx.x * kCqWarps + w) * kCqCands;
     for (;;) {
         int wi = 0;
         if (lane == 0) wi = atomicAdd(&work[0], 1);
@@ -712,7 +719,8 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
         const int qs = cstart[c], qn = ccount[c];
         float R = (kb[c] + 2.0f * __uint_as_float(mbits[c])) * 1.00002f + 1e-6f * h;
         bool ok = isfinite(R);
-        int ncand = 0;
+        int* cur = nodes[w][0];
+        int nf = 0;
         if (ok) {
             const float R2 = R * R;
             // the ball's box in cells
@@ -729,9 +737,7 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
             }
             const int bx = (x1 >> l) - (x0 >> l) + 1, by = (y1 >> l) - (y0 >> l) + 1, bz = (z1 >> l) - (z0 >> l) + 1;
             const int tot = bx * by * bz;
-            int* cur = nodes[w][0];
             int* nxt = nodes[w][1];
-            int nf = 0;
             // stage A: the nodes of level l covering the box
             for (int b = 0; b < tot; b += 32) {
                 const int t = b + lane;
@@ -776,42 +782,17 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
                 nf = nn;
             }
             __syncwarp();
-            // stage C: the points of those cells within R of the centre
-            for (int b = 0; b < nf && ok; b += 32) {
-                const int t = b + lane;
-                int s0 = 0, cnt = 0;
-                if (t < nf) {
-                    const int cell = cur[t];
-                    s0 = a.cell_start[cell];
-                    cnt = a.cell_start[cell + 1] - s0;
-                }
-                const int mx = __reduce_max_sync(FULL, cnt);
-                for (int j = 0; j < mx; ++j) {
-                    bool keep = false;
-                    float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (j < cnt) {
-                        p = a.pts[s0 + j];
-                        const float ex = p.x - x, ey = p.y - y, ez = p.z - z;
-                        keep = ex * ex + ey * ey + ez * ez <= R2;
-                    }
-                    const unsigned bal = __ballot_sync(FULL, keep);
-                    const int pos = ncand + __popc(bal & below);
-                    if (keep && pos < kCqCands) cand[pos] = p;
-                    ncand += __popc(bal);
-                }
-                ok = ncand <= kCqCands;
-            }
-            __syncwarp();
         }
         if (!ok) {  // the per-thread search takes this cell's queries
             for (int t = lane; t < qn; t += 32) fb[atomicAdd(&work[1], 1)] = order[qs + t];
             continue;
         }
-        __threadfence_block();  // the candidates written above, visible to the whole warp
-        __syncwarp();
-        // stage D: every lane ranks the same candidates for its own query,
-        // starting from the bound kb[c] + |q - x_c| on its 16th distance
+        // stages C + D, per chunk of 32 queries: the points of the frontier
+        // cells within R of the centre are streamed through shared memory and
+        // every lane ranks them for its own query, starting from the bound
+        // kb[c] + |q - x_c| on its 16th distance
         const float kbc = kb[c];
+        const float R2 = R * R;
         for (int base = 0; base < qn; base += 32) {
             const bool has = base + lane < qn;
             long long qi = 0;
@@ -825,20 +806,43 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
             const unsigned long long T = ((unsigned long long)__float_as_uint(rq * rq * 1.00002f) << 32) | 0xffffffffull;
             TopK<KMAX> top;
             top.init_bound(k, T);
-            for (int c0 = 0; c0 < ncand; c0 += kCqChunk) {
-                // stage the next chunk of candidates in shared memory (coalesced)
-                const int cn = ncand - c0 < kCqChunk ? ncand - c0 : kCqChunk;
+            int staged = 0;
+            auto rank = [&]() {
                 __syncwarp();
-                for (int t = lane; t < cn; t += 32) stage[w][t] = cand[c0 + t];
-                __syncwarp();
-                for (int t = 0; t < cn; ++t) {
+                for (int t = 0; t < staged; ++t) {
                     const float4 pp = stage[w][t];
                     const float d2 = sq3_rn(__fsub_rn(pp.x, qx), __fsub_rn(pp.y, qy), __fsub_rn(pp.z, qz));
                     const unsigned long long v = ((unsigned long long)__float_as_uint(d2) << 32) |
                                                  (unsigned)__float_as_int(pp.w);
                     if (v < top.mx) top.replace_max(v);
                 }
+                __syncwarp();
+                staged = 0;
+            };
+            for (int b = 0; b < nf; b += 32) {
+                const int t = b + lane;
+                int s0 = 0, cnt = 0;
+                if (t < nf) {
+                    const int cell = cur[t];
+                    s0 = a.cell_start[cell];
+                    cnt = a.cell_start[cell + 1] - s0;
+                }
+                const int mx = __reduce_max_sync(FULL, cnt);
+                for (int j = 0; j < mx; ++j) {
+                    bool keep = false;
+                    float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (j < cnt) {
+                        p = a.pts[s0 + j];
+                        const float px = p.x - x, py = p.y - y, pz = p.z - z;
+                        keep = px * px + py * py + pz * pz <= R2;
+                    }
+                    const unsigned bal = __ballot_sync(FULL, keep);
+                    if (keep) stage[w][staged + __popc(bal & below)] = p;
+                    staged += __popc(bal);
+                    if (staged > kCqChunk - 32) rank();
+                }
             }
+            if (staged > 0) rank();
             top.sort();
             if (has) {
 #pragma unroll
@@ -908,16 +912,78 @@ static int knn_query_cells(const KnnIndex& ix, const KnnArgs& a0, long long nq, 
         if (bps <= 0) bps = 1;
     }
     const long long grid = (long long)num_sms() * bps;
-    DWG_TRY(ix.c_cand.reserve((size_t)grid * kCqWarps * kCqCands));
     k_knn_cells<16><<<(unsigned)grid, kCqWarps * 32, 0, s>>>(
         a, ix.c_active.ptr, ix.c_misc.ptr, ix.c_start.ptr, ix.c_count.ptr, ix.c_m.ptr, ix.kb.ptr, ix.q_order.ptr,
-        ix.c_misc.ptr + 1, ix.c_fb.ptr, ix.c_cand.ptr);
+        ix.c_misc.ptr + 1, ix.c_fb.ptr);
     DWG_CHECK_LAUNCH();
     // the queries of cells whose candidate sets did not fit
     KnnArgs f = a;
     f.order = ix.c_fb.ptr;
     f.nq_dev_i32 = ix.c_misc.ptr + 2;
     return knn_launch<16>(f, nq, s);
+}
+
+// ------------------------------------------------------------- subsets --
+__global__ void k_sub_count(long long ncell, const int* __restrict__ cs, const float4* __restrict__ pts,
+                            const unsigned char* __restrict__ exclude, int* __restrict__ count) {
+    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c > ncell) return;
+    int m = 0;
+    if (c < ncell) {
+        const int e = cs[c + 1];
+        for (int t = cs[c]; t < e; ++t) m += exclude[__float_as_int(pts[t].w)] ? 0 : 1;
+    }
+    count[c] = m;  // count[ncell] = 0 closes the scan
+}
+
+__global__ void k_sub_fill(long long ncell, const int* __restrict__ cs, const float4* __restrict__ pts,
+                           const unsigned char* __restrict__ exclude, const int* __restrict__ sub_start,
+                           float4* __restrict__ sub_pts) {
+    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (c >= ncell) return;
+    int o = sub_start[c];
+    const int e = cs[c + 1];
+    for (int t = cs[c]; t < e; ++t) {
+        const float4 p = pts[t];
+        if (!exclude[__float_as_int(p.w)]) sub_pts[o++] = p;
+    }
+}
+
+int knn_build_subset(const KnnIndex& full, const unsigned char* exclude, KnnIndex& sub, cudaStream_t s) {
+    DWG_REQUIRE(exclude && full.n >= 1, "knn subset: bad arguments");
+    const long long ncell = (long long)full.G[0] * full.G[1] * full.G[2];
+    if (sub.n != full.n || sub.G[0] != full.G[0] || sub.G[1] != full.G[1] || sub.G[2] != full.G[2]) {
+        sub.n = full.n;  // an upper bound; the kept count stays on the device
+        for (int d = 0; d < 3; ++d) {
+            sub.G[d] = full.G[d];
+            sub.lo[d] = full.lo[d];
+        }
+        sub.h = full.h;
+        sub.inv_h = full.inv_h;
+        sub.morton_shift = full.morton_shift;
+        DWG_TRY(sub.cell_start.reserve(ncell + 1));
+        DWG_TRY(sub.cell_fill.reserve(ncell + 1));
+        DWG_TRY(sub.pts.reserve(full.n));
+        DWG_TRY(sub.bbox.reserve(6));
+        DWG_CHECK_CUDA(cudaMemcpyAsync(sub.bbox.ptr, full.bbox.ptr, sizeof(float) * 6, cudaMemcpyDeviceToDevice, s));
+        DWG_TRY(pyramid_dims(sub));
+        size_t bytes = 0;
+        DWG_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, sub.cell_fill.ptr, sub.cell_start.ptr,
+                                                     (int)(ncell + 1), s));
+        DWG_TRY(sub.scratch.reserve(bytes + 256));
+    }
+    k_sub_count<<<div_up(ncell + 1, 256), 256, 0, s>>>(ncell, full.cell_start.ptr, full.pts.ptr, exclude,
+                                                       sub.cell_fill.ptr);
+    DWG_CHECK_LAUNCH();
+    size_t bytes = sub.scratch.n;
+    DWG_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(sub.scratch.ptr, bytes, sub.cell_fill.ptr, sub.cell_start.ptr,
+                                                 (int)(ncell + 1), s));
+    k_sub_fill<<<div_up(ncell, 256), 256, 0, s>>>(ncell, full.cell_start.ptr, full.pts.ptr, exclude,
+                                                  sub.cell_start.ptr, sub.pts.ptr);
+    DWG_CHECK_LAUNCH();
+    DWG_TRY(pyramid_fill(sub, s));
+    sub.kb_ready = false;
+    return build_kbound(sub, s);
 }
 
 constexpr int kKnnBuckets = 1 << 15;

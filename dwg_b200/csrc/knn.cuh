@@ -30,7 +30,6 @@ struct KnnIndex {
     mutable DevBuf<int> c_count, c_start, c_fill, c_active, c_misc, c_fb;
     mutable DevBuf<unsigned int> c_m;
     mutable DevBuf<unsigned char> c_scratch;
-    mutable DevBuf<float4> c_cand;  // per-warp candidate slots of the cell-grouped kernel
     // query bucketing workspace (grown on demand; not thread safe)
     int morton_shift = 0;
     mutable DevBuf<int> q_key, q_order, q_hist, q_fill;
@@ -56,5 +55,10 @@ struct KnnQuery {
 
 // out[j*k + i] = index of the i-th nearest; -1 when fewer than k candidates
 int knn_query(const KnnIndex& ix, const KnnQuery& q, int k, int* out, cudaStream_t s);
+
+// sub = the points of `full` with exclude[id] == 0, on the same grid (no
+// host synchronisation: capturable once sub's buffers exist); indices stay
+// those of full
+int knn_build_subset(const KnnIndex& full, const unsigned char* exclude, KnnIndex& sub, cudaStream_t s);
 
 }  // namespace dwg

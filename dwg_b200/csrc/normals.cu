@@ -133,17 +133,17 @@ int zero_repair(const KnnIndex& ix, const float* pos, int L, float* N, const uns
     DWG_TRY(ws.scratch.reserve(bytes + 256));
     bytes = ws.scratch.n;
     DWG_CHECK_CUDA(cub::DeviceSelect::Flagged(ws.scratch.ptr, bytes, it, is_zero, lp, cp, L, s));
-    // The zero points are sorted out of the candidate set by the filter, so the
-    // neighbours are the k nearest among the unflagged points, in key order.
+    // the neighbours are the k nearest among the unflagged points, in key
+    // order: the query runs on the index of those points alone
+    DWG_TRY(knn_build_subset(ix, is_zero, ws.sub, s));
     KnnQuery q;
     q.q_index = ws.list.ptr;
     q.q_source = pos;
     q.nq = L;
     q.nq_dev_i32 = ws.count.ptr;
-    q.exclude = is_zero;
     q.gate_count = ws.count.ptr;
     q.gate_min = min_zero;
-    DWG_TRY(knn_query(ix, q, k, ws.nb.ptr, s));
+    DWG_TRY(knn_query(ws.sub, q, k, ws.nb.ptr, s));
     long long blocks = (long long)num_sms() * 4;
     k_zero_apply<<<(unsigned)blocks, 256, 0, s>>>(ws.list.ptr, ws.count.ptr, min_zero, ws.nb.ptr, k, N);
     DWG_CHECK_LAUNCH();

@@ -17,6 +17,7 @@ int diffuse_normals(const int* knn, const float* tri_normals, long long num_tris
                     long long* acc, unsigned char* is_zero, int* zero_count, cudaStream_t s);
 
 struct ZeroRepairWs {
+    KnnIndex sub;  // the unflagged points, rebuilt per call
     DevBuf<int> list;
     DevBuf<int> count;
     DevBuf<int> nb;
