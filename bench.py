@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--iters", type=int, default=WORKLOAD["total_iter"])
     ap.add_argument("--precision", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the precision, learned-start and batched-clouds reports")
     return ap.parse_args()
 
 
@@ -216,6 +218,14 @@ def run_ours(a, rank, world, local_rank):
 
     # kernel-level roofline: the screened GWN grid kernel on the iteration-0 state
     roof = gwn_roofline(a, lib, capi, turbo, torch, dev, P)
+    extras = {}
+    if rank == 0 and not a.no_extras:
+        for name, fn in (("precision", precision_report), ("learned", learned_report), ("batched", batched_report)):
+            try:
+                extras[name] = fn(a, lib, capi, turbo, torch, dev)
+            except Exception as e:  # a report must not take the headline line down
+                extras[name] = {"error": f"{type(e).__name__}: {e}"}
+            print(f"{name} report done", file=sys.stderr, flush=True)
 
     # max over ranks
     vals = torch.tensor([ms, float(np.mean(e2e_ms))], dtype=torch.float64, device=dev)
@@ -253,6 +263,7 @@ def run_ours(a, rank, world, local_rank):
         "roofline": roof,
         "clocks": clk,
     }
+    out.update(extras)
     return out
 
 
@@ -375,6 +386,183 @@ def gwn_roofline(a, lib, capi, turbo, torch, dev, P):
                 "frac": 3.0 * nterm / t / 1e12 / mufu_peak},
         "algorithmic": "20 FP32 flops + 3 MUFU per pair term (screened), terms counted in-kernel",
     }
+
+
+def _pipeline_state(lib, capi, torch, dev, P, flags, iters):
+    """leaf positions / normals (device tensors), grid res and origin after `iters` iterations"""
+    import ctypes as C
+    prm = capi.default_params(**flags)
+    h = C.c_void_p()
+    Pd = torch.from_numpy(np.ascontiguousarray(P, np.float32)).to(dev)
+    capi.check(lib.dwg_pipeline_create(capi.ptr(Pd), None, len(P), C.byref(prm), None, C.byref(h)))
+    try:
+        if iters:
+            capi.check(lib.dwg_pipeline_iterate(h, iters))
+        L = C.c_longlong()
+        capi.check(lib.dwg_pipeline_size(h, b"leaves", C.byref(L)))
+        lp = np.empty((L.value, 3), np.float32)
+        ln = np.empty((L.value, 3), np.float32)
+        res = np.zeros(3, np.int32)
+        org = np.zeros(4, np.float32)
+        capi.check(lib.dwg_pipeline_get(h, b"leaf_pos", lp.ctypes.data))
+        capi.check(lib.dwg_pipeline_get(h, b"leaf_nrm", ln.ctypes.data))
+        capi.check(lib.dwg_pipeline_get(h, b"grid_res", res.ctypes.data))
+        capi.check(lib.dwg_pipeline_get(h, b"grid_origin", org.ctypes.data))
+    finally:
+        lib.dwg_pipeline_destroy(h)
+    return lp, ln, res, org
+
+
+def precision_report(a, lib, capi, turbo, torch, dev):
+    """Error of the FP32 sums against the FP64 oracle with the same octree and
+    opening decisions, per output (leaf field, grid field) and per precision
+    variant, plus the FP64 moments against the oracle's; the state is the bench
+    cloud after 2 DWG iterations (sigma 20), the grid a seeded 20,000-sample
+    subset."""
+    import oracle
+    P = make_cloud(a.points, 0)
+    lp, ln, res, org = _pipeline_state(lib, capi, torch, dev, P, dict(grid_reso=a.grid, final_reso=a.grid,
+                                                                   total_iter=2), 2)
+    n = len(lp)
+    A = np.full(n, 2e-6, np.float32)
+    rng = np.random.default_rng(7)
+    ng = int(np.prod(res.astype(np.int64)))
+    sel = rng.choice(ng, min(20000, ng), replace=False)
+    idx = np.stack([sel % res[0], (sel // res[0]) % res[1], sel // (res[0] * res[1])], 1).astype(np.float32)
+    Q = (org[None, :3].astype(np.float32) + idx * np.float32(org[3])).astype(np.float32)
+    ot = oracle.Octree(lp, WORKLOAD["max_depth"])
+    mom = ot.moments(lp, ln, A)
+    ref_leaf, _ = ot.gwn(lp, ln, A, lp, beta=2.3, sigma=20.0, screened=True, moments=mom)
+    ref_grid, _ = ot.gwn(lp, ln, A, Q, beta=2.3, sigma=20.0, screened=True, moments=mom)
+    lpd, lnd = torch.from_numpy(lp).to(dev), torch.from_numpy(ln).to(dev)
+    Ad, Qd = torch.from_numpy(A).to(dev), torch.from_numpy(Q).to(dev)
+    tree = turbo.TurboLibiGWN(lpd, max_depth=WORKLOAD["max_depth"], areas=Ad)
+    tree.UpdateMassNormals(lnd, Ad)
+    out = {"state": "bench cloud after 2 DWG iterations, sigma 20, beta 2.3; grid: 20,000 seeded samples",
+           "scale_rms": {"leaf": float(np.sqrt(np.mean(ref_leaf ** 2))), "grid": float(np.sqrt(np.mean(ref_grid ** 2)))}}
+    names = {0: "fp32", 1: "fp32-compensated", 2: "fp32-compensated-accurate-terms"}
+    for prec in (0, 1, 2):
+        wl = tree.TurboLibiScreenedGWNLaunch(lpd, i_Normals=None, i_As=None, beta=2.3, sigma=20.0,
+                                             precision=prec).cpu().numpy().astype(np.float64)
+        wg = tree.TurboLibiScreenedGWNLaunch(Qd, i_Normals=None, i_As=None, beta=2.3, sigma=20.0,
+                                             precision=prec).cpu().numpy().astype(np.float64)
+        el, eg = wl - ref_leaf, wg - ref_grid
+        out[names[prec]] = {"leaf_field": {"max_abs": float(np.abs(el).max()), "rms": float(np.sqrt(np.mean(el ** 2)))},
+                            "grid_field": {"max_abs": float(np.abs(eg).max()), "rms": float(np.sqrt(np.mean(eg ** 2)))}}
+    # moments: the same octree on both sides; nodes matched by (depth, first sorted point)
+    g = tree.export()
+    ost = ot.dfs_starts()
+    key = {(int(d), int(s0)): i for i, (d, s0, c) in enumerate(zip(ot.depth, ost, ot.counts)) if c > 0}
+    idx = np.array([key[(int(d), int(s0))] for d, s0 in zip(g["depth"], g["pt_start"])])
+    CM, R, EC = mom
+
+    def rel(x, y):
+        return float(np.max(np.abs(x - y)) / max(float(np.max(np.abs(y))), 1e-300))
+
+    out["moments"] = {"nodes": int(len(idx)), "cm_max_rel": rel(g["cm"], CM[idx]), "radius_max_rel": rel(g["radius"], R[idx]),
+                      "sum_An_max_rel": rel(g["ec"], EC[idx]), "note": "FP64 on the GPU and in the oracle"}
+    return out
+
+
+def learned_report(a, lib, capi, turbo, torch, dev):
+    """Plain (Gauss map) vs learned start on the bench cloud: orientation
+    agreement of the initial leaf normals with the true normals, and the RMS
+    distance of each iteration's grid field to the plain method's field after
+    all iterations (sign-matched: the orientation flips every iteration)."""
+    from dwg_b200 import datasets as D
+    from dwg_b200.train_init import DEFAULT_WEIGHTS
+    Praw, Ntrue = D.torus(a.points, R=1.0, r=0.35, noise=0.003, seed=1000)
+    P, _, _ = D.normalize(Praw)
+    Pd = torch.from_numpy(np.ascontiguousarray(P, np.float32)).to(dev)
+    flags = dict(grid_reso=a.grid, final_reso=a.grid, total_iter=a.iters, use_graph=1, precision=a.precision)
+    model = turbo.LearnedNormalInit(DEFAULT_WEIGHTS)
+    ref = turbo.TurboDWG(Pd, None, **flags)
+    ref.TurboScreenedDWGLaunch(a.iters)
+    w_ref = torch.from_numpy(ref.get("field")).to(dev)
+    leaves = torch.from_numpy(ref.get("leaf_pos")).to(dev)
+    ref.close()
+    nb = turbo.KnnIndex(Pd).query(leaves, 1).cpu().numpy()[:, 0]
+    truth = Ntrue[nb]
+    out = {"weights": os.path.relpath(DEFAULT_WEIGHTS, ROOT), "reference_field": f"plain start after {a.iters} iterations"}
+    for name, m in (("plain", None), ("learned", model)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        d = turbo.TurboDWG(Pd, None, init_model=m, **flags)
+        torch.cuda.synchronize()
+        create_ms = (time.perf_counter() - t0) * 1e3
+        n0 = d.get("leaf_nrm")
+        rms = []
+        for _ in range(a.iters):
+            d.TurboScreenedDWGLaunch(1)
+            w = torch.from_numpy(d.get("field")).to(dev)
+            rms.append(float(min(torch.sqrt(torch.mean((w - w_ref) ** 2)), torch.sqrt(torch.mean((w + w_ref) ** 2)))))
+        d.close()
+        out[name] = {"init_orientation_agreement": float(((n0 * truth).sum(1) > 0).mean()),
+                     "create_ms": create_ms,
+                     "rms_to_reference_every_5th": [round(x, 6) for x in rms[::5]],
+                     "iters_to_2e-3": next((t + 1 for t, e in enumerate(rms) if e <= 2e-3), None)}
+    return out
+
+
+def batched_report(a, lib, capi, turbo, torch, dev):
+    """The batched-clouds configuration: 64 clouds of log-uniform size in
+    [2,000, 200,000] (spheres, tori, 3-superquadric unions, noise 0.001-0.01),
+    per-cloud grid clamp(round(128 (n/2000)^(1/3)), 128, 256), 30 iterations,
+    in one batch (one graph per iteration, one persistent launch for all grid
+    sums) against the same clouds one by one; device time with CUDA events."""
+    import ctypes as C
+    from dwg_b200 import datasets as D
+    cl = D.batch(64, 2000, 200000, seed=0)
+    dev_pts, prms = [], []
+    for c in cl:
+        Pn, _, _ = D.normalize(c["points"])
+        dev_pts.append(torch.from_numpy(np.ascontiguousarray(Pn, np.float32)).to(dev))
+        prms.append(capi.default_params(grid_reso=c["grid_reso"], final_reso=c["grid_reso"], total_iter=a.iters,
+                                        precision=a.precision))
+    npts = sum(int(d.shape[0]) for d in dev_pts)
+    ptrs = (C.c_void_p * len(dev_pts))(*[capi.ptr(d) for d in dev_pts])
+    counts = (C.c_int * len(dev_pts))(*[int(d.shape[0]) for d in dev_pts])
+    parr = (capi.Params * len(prms))(*prms)
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    def batch_run():
+        b = C.c_void_p()
+        capi.check(lib.dwg_batch_create(ptrs, counts, len(dev_pts), parr, None, C.byref(b)))
+        capi.check(lib.dwg_batch_iterate(b, a.iters))
+        capi.check(lib.dwg_batch_finalize(b))
+        lib.dwg_batch_destroy(b)
+
+    def one_by_one():
+        for d, prm in zip(dev_pts, prms):
+            h = C.c_void_p()
+            capi.check(lib.dwg_pipeline_create(capi.ptr(d), None, int(d.shape[0]), C.byref(prm), None, C.byref(h)))
+            capi.check(lib.dwg_pipeline_iterate(h, a.iters))
+            capi.check(lib.dwg_pipeline_finalize(h))
+            lib.dwg_pipeline_destroy(h)
+
+    batch_run()  # warm-up
+    ms_b = timed(batch_run)
+    ms_s = timed(one_by_one)
+    # the autotuner on the largest cloud (its brick shape would be the batch's)
+    big = int(np.argmax([int(d.shape[0]) for d in dev_pts]))
+    r = capi.TuneResult()
+    capi.check(lib.dwg_autotune(capi.ptr(dev_pts[big]), int(dev_pts[big].shape[0]), C.byref(prms[big]), 1e-4, 4096,
+                                2, None, C.byref(r)))
+    return {"clouds": len(dev_pts), "points": npts, "iterations": a.iters,
+            "batched": {"ms": ms_b, "Mpts_per_s": npts / ms_b / 1e3},
+            "one_by_one": {"ms": ms_s, "Mpts_per_s": npts / ms_s / 1e3},
+            "autotune_largest_cloud": {"points": int(dev_pts[big].shape[0]), "beta": r.beta, "tile": r.tile,
+                                       "rms_err": r.rms_err, "max_err": r.max_err, "grid_ms": r.grid_ms,
+                                       "reference_setting_grid_ms": r.ref_ms, "tol": 1e-4}}
 
 
 def cudart_copy(torch, dst, src_ptr, nbytes):
