@@ -39,13 +39,13 @@ class Params(C.Structure):
         ("offset_1", C.c_float), ("offset_2", C.c_float), ("use_leaves_generate", C.c_int),
         ("total_iter", C.c_int), ("beta", C.c_float), ("area", C.c_float), ("screen", C.c_float),
         ("knn_tri", C.c_int), ("knn_zero", C.c_int), ("precision", C.c_int), ("use_graph", C.c_int),
-        ("tile", C.c_int),
+        ("tile", C.c_int), ("as_thres", C.c_float),
     ]
 
 
 class TuneResult(C.Structure):
     _fields_ = [("beta", C.c_float), ("tile", C.c_int), ("rms_err", C.c_float), ("max_err", C.c_float),
-                ("grid_ms", C.c_float), ("ref_ms", C.c_float)]
+                ("grid_ms", C.c_float), ("ref_ms", C.c_float), ("ref_rms_err", C.c_float), ("field_rms", C.c_float)]
 
 
 # name -> (restype, argtypes)

@@ -55,7 +55,6 @@ int main(int argc, char** argv) {
     dwg_params_default(&prm);
     int output_mode = 1, com_As = 0, test_iter = 999999;
     unsigned long long seed = 0;
-    float As_threshold = 0.f;
     for (int i = 1; i + 1 < argc; i += 2) {
         const std::string k = argv[i];
         const char* v = argv[i + 1];
@@ -76,7 +75,7 @@ int main(int argc, char** argv) {
         else if (k == "--use_leaves_generate") prm.use_leaves_generate = std::atoi(v);
         else if (k == "--use_radii") prm.use_radii = std::atoi(v);
         else if (k == "--com_As") com_As = std::atoi(v);
-        else if (k == "--As_thres") As_threshold = (float)std::atof(v);
+        else if (k == "--As_thres") prm.as_thres = (float)std::atof(v);
         else if (k == "--offset_1") prm.offset_1 = (float)std::atof(v);
         else if (k == "--offset_2") prm.offset_2 = (float)std::atof(v);
         else if (k == "--test_iter") test_iter = std::atoi(v);
@@ -92,7 +91,6 @@ int main(int argc, char** argv) {
         fprintf(stderr, "--com_As 1 (CGAL point areas) is not supported by this build\n");
         return 2;
     }
-    if (As_threshold != 0.f) fprintf(stderr, "note: --As_thres is ignored (outlier filtering is not built)\n");
     if (test_iter != 999999) fprintf(stderr, "note: --test_iter intermediate meshes are not written\n");
     const std::string full = in_path + "/" + in_name;
     const std::string pure = in_name.size() > 4 ? in_name.substr(0, in_name.size() - 4) : in_name;

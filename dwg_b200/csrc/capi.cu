@@ -401,6 +401,7 @@ void dwg_params_default(dwg_params* p) {
     p->precision = 1;
     p->use_graph = 1;
     p->tile = 0;
+    p->as_thres = 0.f;
 }
 
 int dwg_pipeline_create(const float* points_dev, const float* normals_dev, int n, const dwg_params* params,

@@ -138,148 +138,6 @@ struct GwnArgs {
     int num_nodes, num_points;
 };
 
-// The sum for the 32 queries of group g (a brick of grid samples, or 32
-// consecutive points); returns this lane's term count.
-template <bool GRID, bool SCREENED, int PREC, int SHAPE>
-__device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g, int lane, int2* __restrict__ stk,
-                                         float sigma, float sigma_l2e) {
-    const unsigned FULL = 0xffffffffu;
-    bool valid;
-    float qx = 0.f, qy = 0.f, qz = 0.f;
-    long long qi;
-    if (GRID) {
-        using B = Brick<SHAPE>;
-        const long long bxi = (long long)(g % (unsigned long long)a.bx);
-        const unsigned long long t = g / (unsigned long long)a.bx;
-        const long long byi = (long long)(t % (unsigned long long)a.by);
-        const long long bzi = (long long)(t / (unsigned long long)a.by);
-        const long long x = bxi * B::X + (lane % B::X), y = byi * B::Y + ((lane / B::X) % B::Y),
-                        z = bzi * B::Z + lane / (B::X * B::Y);
-        valid = x < a.rx && y < a.ry && z < a.rz;
-        qi = x + (long long)a.rx * (y + (long long)a.ry * z);
-        qx = __fadd_rn(a.ox, __fmul_rn((float)x, a.h));
-        qy = __fadd_rn(a.oy, __fmul_rn((float)y, a.h));
-        qz = __fadd_rn(a.oz, __fmul_rn((float)z, a.h));
-    } else {
-        qi = (long long)g * 32 + lane;
-        valid = qi < a.nq;
-        if (valid) {
-            qx = a.q[qi * 3];
-            qy = a.q[qi * 3 + 1];
-            qz = a.q[qi * 3 + 2];
-        }
-    }
-    const unsigned vm = __ballot_sync(FULL, valid);
-    float s = 0.f, c = 0.f;
-    int nterm = 0;
-    auto leaf_points = [&](int start, int cnt) {
-        for (int j = start; j < start + cnt; ++j) {
-            float4 p = a.pa[j];
-            float4 nn = a.nr[j];
-            float dx = p.x - qx, dy = p.y - qy, dz = p.z - qz;
-            float d = p.w * fmaf(dx, nn.x, fmaf(dy, nn.y, dz * nn.z));
-            float sc = a.use_radii ? nn.w : a.screen;
-            float v;
-            if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, sc, sigma, sigma_l2e, v)) {
-                acc_add<PREC>(s, c, v);
-                ++nterm;
-            }
-        }
-    };
-
-    // one child record (level order).  A single-point leaf is always a term;
-    // an internal node is a dipole term when far for this lane (sqrt_rn(d2) >
-    // beta R in round-to-nearest single precision, src/TurboLibiGWN.cu:636-644,
-    // as one comparison of d2 with the node's exact threshold) and is opened
-    // (pushed with the lanes that need it) otherwise; both use the same d2.
-    // Larger leaves (and every leaf when radii apply) are summed point by point.
-    auto child = [&](int cidx, const float4& na, const float4& nb, bool act, int& sp) {
-        const unsigned meta = (unsigned)__float_as_int(nb.w);
-        const bool leaf = (meta & kMetaLeafBit) != 0;
-        if (leaf && (!(meta & kMetaSingle) || a.use_radii)) {
-            const int st = (int)(meta & kMetaIndex), cnt = __float_as_int(na.w);
-            if (cnt < 0 || st + cnt > a.num_points) {
-                if (lane == 0) atomicOr(&a.work[1], 4u);
-            } else if (act) {
-                leaf_points(st, cnt);
-            }
-            return;
-        }
-        const float dx = __fsub_rn(na.x, qx), dy = __fsub_rn(na.y, qy), dz = __fsub_rn(na.z, qz);
-        const float d2 = sq3_rn(dx, dy, dz);
-        const bool far = leaf || d2 > na.w;
-        if (act && far) {
-            const float d = fmaf(dx, nb.x, fmaf(dy, nb.y, dz * nb.z));
-            float v;
-            if (gwn_term_r2<SCREENED, PREC>(d2, d, a.screen, sigma, sigma_l2e, v)) {
-                acc_add<PREC>(s, c, v);
-                ++nterm;
-            }
-        }
-        const unsigned nm = __ballot_sync(FULL, act && !far);
-        if (nm) {
-            if (sp < kGwnStack) {
-                if (lane == 0) stk[sp] = make_int2(cidx, (int)nm);
-                ++sp;
-            } else if (lane == 0) {
-                atomicOr(&a.work[1], 1u);
-            }
-        }
-    };
-
-    int sp = 0;
-    {
-        const float4 ra = a.node_a[0], rb = a.node_b[0];
-        const unsigned rm = (unsigned)__float_as_int(rb.w);
-        if (rm & kMetaLeafBit) {
-            child(0, ra, rb, valid, sp);  // a leaf root is summed; nothing is pushed
-        } else {
-            if (lane == 0) stk[0] = make_int2(0, (int)vm);
-            sp = 1;
-        }
-    }
-    while (sp > 0) {
-        __syncwarp();
-        const int2 e = stk[--sp];
-        __syncwarp();
-        if (e.x < 0 || e.x >= a.num_nodes) {
-            if (lane == 0) atomicOr(&a.work[1], 2u);
-            continue;
-        }
-        const bool act = (((unsigned)e.y) >> lane) & 1u;
-        const unsigned pm = (unsigned)__float_as_int(a.node_b[e.x].w);
-        const int first = (int)(pm & kMetaIndex);
-        const int nch = (int)((pm >> 28) & 7u) + 1;
-        // structural guard: children come after the parent, inside the table
-        if ((pm & kMetaLeafBit) || first <= e.x || first + nch > a.num_nodes) {
-            if (lane == 0) atomicOr(&a.work[1], 2u);
-            continue;
-        }
-        float4 na = a.node_a[first], nb = a.node_b[first];
-        for (int j = 0; j < nch; ++j) {
-            float4 na2, nb2;
-            if (j + 1 < nch) {  // load the next sibling while this one is evaluated
-                na2 = a.node_a[first + j + 1];
-                nb2 = a.node_b[first + j + 1];
-            }
-            child(first + j, na, nb, act, sp);
-            na = na2;
-            nb = nb2;
-        }
-    }
-    if (valid) {
-        a.out[qi] = (PREC == 0) ? s : __fadd_rn(s, c);
-        if (a.per_query_terms) a.per_query_terms[qi] = nterm;
-    }
-    return nterm;
-}
-
-// Grid sums with two samples per lane: the brick of SHAPE (32 samples) and
-// the brick above it in z form the warp's 64 queries.  The traversal (stack
-// pops, record loads, the loop over children) is shared by both; each of the
-// two sums keeps the order of its own terms, so the values are bit for bit
-// those of one sample per lane.  The terms are evaluated branch-free and
-// masked, so that a lane's two samples never split the warp.
 template <bool SCREENED, int PREC>
 __device__ __forceinline__ float gwn_term_masked(bool take, float r2, float d, float s, float sigma,
                                                  float sigma_l2e, bool& counted) {
@@ -292,12 +150,15 @@ __device__ __forceinline__ float gwn_term_masked(bool take, float r2, float d, f
         const float rho = fmaxf(r, s);
         const float e = (PREC >= 2) ? expf(sigma * rho) : ex2_ftz(rho * sigma_l2e);
         const float den = fmaf(e, kFourPi * (rho * rho * rho), 1e-7f);
+        // the reference forces the sign of d onto the term
+        // (src/TurboLibiGWN.cu:550-584); den > 0, so |sigma rho + 1| d does
+        // that (an operand modifier, no extra instruction)
         const float num = fabsf(fmaf(sigma, rho, 1.0f)) * d;
         const float t = (PREC >= 2) ? __fdiv_rn(num, den) : num * rcp_ftz(den);
         v = ok ? t : 0.f;
         counted = ok;
     } else {
-        const bool zero = r2 == 0.0f;
+        const bool zero = r2 == 0.0f;  // a zero distance is a term of value 0
         const float r2s = (take && !zero) ? r2 : 1.0f;
         const float r = (PREC >= 2) ? sqrtf(r2s) : r2s * rsqrt_ftz(r2s);
         const float den = fmaf(kFourPi * r, r2s, 1e-8f);
@@ -308,43 +169,88 @@ __device__ __forceinline__ float gwn_term_masked(bool take, float r2, float d, f
     return v;
 }
 
-template <bool SCREENED, int PREC, int SHAPE>
-__device__ __forceinline__ int gwn_group2(const GwnArgs& a, unsigned long long g, int lane,
-                                          int4* __restrict__ stk, float sigma, float sigma_l2e) {
+// The sums of group g: 64 queries, two per lane -- for a grid, the brick of
+// SHAPE (32 samples) and the brick above it in z; for points, 64
+// consecutive (Morton-ordered) points.  The warp walks the octree once for
+// all 64: the stack entries carry the masks of the lanes whose first and
+// second query opened the node, so every query takes exactly the reference's
+// per-query decisions -- a child is a dipole term when |CM - q| > beta R,
+// otherwise it is opened, and leaves are summed point by point -- while the
+// traversal (stack pops, record loads, the loop over children) is shared.
+// Terms are evaluated branch-free and masked, so that a lane's two queries
+// never split the warp; each query's terms keep their depth-first order.
+// Returns the lane's term count.
+template <bool GRID, bool SCREENED, int PREC, int SHAPE>
+__device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g, int lane, int4* __restrict__ stk,
+                                         float sigma, float sigma_l2e) {
+    // grids take two samples per lane; point queries one (64 consecutive
+    // points span more of the tree than 32, which costs more than it shares)
+    constexpr bool TWO = GRID;
     const unsigned FULL = 0xffffffffu;
-    using B = Brick<SHAPE>;
-    const long long bxi = (long long)(g % (unsigned long long)a.bx);
-    const unsigned long long t = g / (unsigned long long)a.bx;
-    const long long byi = (long long)(t % (unsigned long long)a.by);
-    const long long bzi = (long long)(t / (unsigned long long)a.by);
-    const long long x = bxi * B::X + (lane % B::X), y = byi * B::Y + ((lane / B::X) % B::Y);
-    const long long z0 = bzi * (2 * B::Z) + lane / (B::X * B::Y), z1 = z0 + B::Z;
-    const bool xy_ok = x < a.rx && y < a.ry;
-    const bool valid0 = xy_ok && z0 < a.rz, valid1 = xy_ok && z1 < a.rz;
-    const long long qi0 = x + (long long)a.rx * (y + (long long)a.ry * z0);
-    const long long qi1 = x + (long long)a.rx * (y + (long long)a.ry * z1);
-    const float qx = __fadd_rn(a.ox, __fmul_rn((float)x, a.h));
-    const float qy = __fadd_rn(a.oy, __fmul_rn((float)y, a.h));
-    const float qz0 = __fadd_rn(a.oz, __fmul_rn((float)z0, a.h));
-    const float qz1 = __fadd_rn(a.oz, __fmul_rn((float)z1, a.h));
+    bool valid0, valid1;
+    long long qi0, qi1;
+    float qx0, qy0, qz0, qx1, qy1, qz1;
+    if (GRID) {
+        using B = Brick<SHAPE>;
+        const long long bxi = (long long)(g % (unsigned long long)a.bx);
+        const unsigned long long t = g / (unsigned long long)a.bx;
+        const long long byi = (long long)(t % (unsigned long long)a.by);
+        const long long bzi = (long long)(t / (unsigned long long)a.by);
+        const long long x = bxi * B::X + (lane % B::X), y = byi * B::Y + ((lane / B::X) % B::Y);
+        const long long z0 = bzi * (2 * B::Z) + lane / (B::X * B::Y), z1 = z0 + B::Z;
+        const bool xy_ok = x < a.rx && y < a.ry;
+        valid0 = xy_ok && z0 < a.rz;
+        valid1 = xy_ok && z1 < a.rz;
+        qi0 = x + (long long)a.rx * (y + (long long)a.ry * z0);
+        qi1 = x + (long long)a.rx * (y + (long long)a.ry * z1);
+        qx0 = __fadd_rn(a.ox, __fmul_rn((float)x, a.h));
+        qy0 = __fadd_rn(a.oy, __fmul_rn((float)y, a.h));
+        qx1 = qx0;
+        qy1 = qy0;
+        qz0 = __fadd_rn(a.oz, __fmul_rn((float)z0, a.h));
+        qz1 = __fadd_rn(a.oz, __fmul_rn((float)z1, a.h));
+    } else {
+        qi0 = (long long)g * (TWO ? 64 : 32) + lane;
+        qi1 = qi0 + 32;
+        valid0 = qi0 < a.nq;
+        valid1 = TWO && qi1 < a.nq;
+        qx0 = qy0 = qz0 = qx1 = qy1 = qz1 = 0.f;
+        if (valid0) {
+            qx0 = a.q[qi0 * 3];
+            qy0 = a.q[qi0 * 3 + 1];
+            qz0 = a.q[qi0 * 3 + 2];
+        }
+        if (valid1) {
+            qx1 = a.q[qi1 * 3];
+            qy1 = a.q[qi1 * 3 + 1];
+            qz1 = a.q[qi1 * 3 + 2];
+        }
+    }
     float s0 = 0.f, c0 = 0.f, s1 = 0.f, c1 = 0.f;
-    int nterm = 0;
+    int n0 = 0, n1 = 0;
 
-    auto leaf_points = [&](int start, int cnt, float qzz, float& s, float& c) {
+    auto leaf_points = [&](int start, int cnt, float qx, float qy, float qz, float& s, float& c, int& n) {
         for (int j = start; j < start + cnt; ++j) {
             const float4 p = a.pa[j];
             const float4 nn = a.nr[j];
-            const float dx = p.x - qx, dy = p.y - qy, dz = p.z - qzz;
+            const float dx = p.x - qx, dy = p.y - qy, dz = p.z - qz;
             const float d = p.w * fmaf(dx, nn.x, fmaf(dy, nn.y, dz * nn.z));
             const float sc = a.use_radii ? nn.w : a.screen;
             float v;
             if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, sc, sigma, sigma_l2e, v)) {
                 acc_add<PREC>(s, c, v);
-                ++nterm;
+                ++n;
             }
         }
     };
 
+    // one child record (level order).  A single-point leaf is always a term;
+    // an internal node is a dipole term when far for the query (sqrt_rn(d2)
+    // > beta R in round-to-nearest single precision, src/TurboLibiGWN.cu:
+    // 636-644, as one comparison of d2 with the node's exact threshold) and is
+    // opened (pushed with the queries that need it) otherwise; both use the
+    // same d2.  Larger leaves (every leaf when radii apply) are summed point
+    // by point.
     auto child = [&](int cidx, const float4& na, const float4& nb, bool act0, bool act1, int& sp) {
         const unsigned meta = (unsigned)__float_as_int(nb.w);
         const bool leaf = (meta & kMetaLeafBit) != 0;
@@ -353,28 +259,26 @@ __device__ __forceinline__ int gwn_group2(const GwnArgs& a, unsigned long long g
             if (cnt < 0 || st + cnt > a.num_points) {
                 if (lane == 0) atomicOr(&a.work[1], 4u);
             } else {
-                if (act0) leaf_points(st, cnt, qz0, s0, c0);
-                if (act1) leaf_points(st, cnt, qz1, s1, c1);
+                if (act0) leaf_points(st, cnt, qx0, qy0, qz0, s0, c0, n0);
+                if (act1) leaf_points(st, cnt, qx1, qy1, qz1, s1, c1, n1);
             }
             return;
         }
-        const float dx = __fsub_rn(na.x, qx), dy = __fsub_rn(na.y, qy);
-        const float dz0 = __fsub_rn(na.z, qz0), dz1 = __fsub_rn(na.z, qz1);
-        const float dxy = __fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy));
-        const float d20 = __fadd_rn(dxy, __fmul_rn(dz0, dz0));
-        const float d21 = __fadd_rn(dxy, __fmul_rn(dz1, dz1));
+        const float dx0 = __fsub_rn(na.x, qx0), dy0 = __fsub_rn(na.y, qy0), dz0 = __fsub_rn(na.z, qz0);
+        const float dx1 = __fsub_rn(na.x, qx1), dy1 = __fsub_rn(na.y, qy1), dz1 = __fsub_rn(na.z, qz1);
+        const float d20 = sq3_rn(dx0, dy0, dz0), d21 = sq3_rn(dx1, dy1, dz1);
         const bool far0 = leaf || d20 > na.w, far1 = leaf || d21 > na.w;
         const bool take0 = act0 && far0, take1 = act1 && far1;
         if (__any_sync(FULL, take0 || take1)) {
-            // d in the operation order of the one-sample path
-            const float dd0 = fmaf(dx, nb.x, fmaf(dy, nb.y, dz0 * nb.z));
-            const float dd1 = fmaf(dx, nb.x, fmaf(dy, nb.y, dz1 * nb.z));
+            const float dd0 = fmaf(dx0, nb.x, fmaf(dy0, nb.y, dz0 * nb.z));
+            const float dd1 = fmaf(dx1, nb.x, fmaf(dy1, nb.y, dz1 * nb.z));
             bool k0, k1;
             const float v0 = gwn_term_masked<SCREENED, PREC>(take0, d20, dd0, a.screen, sigma, sigma_l2e, k0);
             const float v1 = gwn_term_masked<SCREENED, PREC>(take1, d21, dd1, a.screen, sigma, sigma_l2e, k1);
             if (k0) acc_add<PREC>(s0, c0, v0);
             if (k1) acc_add<PREC>(s1, c1, v1);
-            nterm += (int)k0 + (int)k1;
+            n0 += (int)k0;
+            n1 += (int)k1;
         }
         const unsigned nm0 = __ballot_sync(FULL, act0 && !far0), nm1 = __ballot_sync(FULL, act1 && !far1);
         if (nm0 | nm1) {
@@ -392,7 +296,7 @@ __device__ __forceinline__ int gwn_group2(const GwnArgs& a, unsigned long long g
         const float4 ra = a.node_a[0], rb = a.node_b[0];
         const unsigned rm = (unsigned)__float_as_int(rb.w);
         if (rm & kMetaLeafBit) {
-            child(0, ra, rb, valid0, valid1, sp);
+            child(0, ra, rb, valid0, valid1, sp);  // a leaf root is summed; nothing is pushed
         } else {
             const unsigned m0 = __ballot_sync(FULL, valid0), m1 = __ballot_sync(FULL, valid1);
             if (lane == 0) stk[0] = make_int4(0, (int)m0, (int)m1, 0);
@@ -411,6 +315,7 @@ __device__ __forceinline__ int gwn_group2(const GwnArgs& a, unsigned long long g
         const unsigned pm = (unsigned)__float_as_int(a.node_b[e.x].w);
         const int first = (int)(pm & kMetaIndex);
         const int nch = (int)((pm >> 28) & 7u) + 1;
+        // structural guard: children come after the parent, inside the table
         if ((pm & kMetaLeafBit) || first <= e.x || first + nch > a.num_nodes) {
             if (lane == 0) atomicOr(&a.work[1], 2u);
             continue;
@@ -418,7 +323,7 @@ __device__ __forceinline__ int gwn_group2(const GwnArgs& a, unsigned long long g
         float4 na = a.node_a[first], nb = a.node_b[first];
         for (int j = 0; j < nch; ++j) {
             float4 na2, nb2;
-            if (j + 1 < nch) {
+            if (j + 1 < nch) {  // load the next sibling while this one is evaluated
                 na2 = a.node_a[first + j + 1];
                 nb2 = a.node_b[first + j + 1];
             }
@@ -427,36 +332,20 @@ __device__ __forceinline__ int gwn_group2(const GwnArgs& a, unsigned long long g
             nb = nb2;
         }
     }
-    if (valid0) a.out[qi0] = (PREC == 0) ? s0 : __fadd_rn(s0, c0);
-    if (valid1) a.out[qi1] = (PREC == 0) ? s1 : __fadd_rn(s1, c1);
-    return nterm;
-}
-
-template <bool SCREENED, int PREC, int SHAPE>
-__global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn2(GwnArgs a) {
-    __shared__ int4 stack[kGwnWarps][kGwnStack];
-    const unsigned FULL = 0xffffffffu;
-    const int lane = threadIdx.x & 31;
-    const int w = threadIdx.x >> 5;
-    const float sigma = a.sigma_dev ? *a.sigma_dev : a.sigma;
-    const float sigma_l2e = sigma * 1.4426950408889634f;
-    unsigned long long my_terms = 0;
-    for (;;) {
-        unsigned g = 0;
-        if (lane == 0) g = atomicAdd(&a.work[0], 1u);
-        g = __shfl_sync(FULL, g, 0);
-        if ((long long)g >= a.ngroups) break;
-        my_terms += (unsigned long long)gwn_group2<SCREENED, PREC, SHAPE>(a, g, lane, stack[w], sigma, sigma_l2e);
+    if (valid0) {
+        a.out[qi0] = (PREC == 0) ? s0 : __fadd_rn(s0, c0);
+        if (a.per_query_terms) a.per_query_terms[qi0] = n0;
     }
-    if (a.terms_total) {
-        for (int o = 16; o > 0; o >>= 1) my_terms += __shfl_down_sync(FULL, my_terms, o);
-        if (lane == 0 && my_terms) atomicAdd(a.terms_total, my_terms);
+    if (valid1) {
+        a.out[qi1] = (PREC == 0) ? s1 : __fadd_rn(s1, c1);
+        if (a.per_query_terms) a.per_query_terms[qi1] = n1;
     }
+    return n0 + n1;
 }
 
 template <bool GRID, bool SCREENED, int PREC, int SHAPE>
-__global__ void __launch_bounds__(kGwnWarps * 32, 4) k_gwn(GwnArgs a) {
-    __shared__ int2 stack[kGwnWarps][kGwnStack];
+__global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn(GwnArgs a) {
+    __shared__ int4 stack[kGwnWarps][kGwnStack];
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
@@ -501,8 +390,8 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3)
         }
         const GwnArgs& a = table[lo];
         const float sigma = a.sigma_dev ? *a.sigma_dev : a.sigma;
-        int nt = gwn_group2<SCREENED, PREC, SHAPE>(a, g - prefix[lo], lane, stack[w], sigma,
-                                                   sigma * 1.4426950408889634f);
+        int nt = gwn_group<true, SCREENED, PREC, SHAPE>(a, g - prefix[lo], lane, stack[w], sigma,
+                                                       sigma * 1.4426950408889634f);
         if (a.terms_total) {
             for (int o = 16; o > 0; o >>= 1) nt += __shfl_down_sync(FULL, nt, o);
             if (lane == 0 && nt) atomicAdd(a.terms_total, (unsigned long long)nt);
@@ -517,19 +406,14 @@ static int blocks_for(K kernel) {
     return bps > 0 ? bps : 1;
 }
 
-// grids take two samples per lane (k_gwn2), point queries one (k_gwn)
 template <bool GRID, bool SCREENED, int PREC, int SHAPE>
 static int launch(const GwnArgs& a, cudaStream_t s) {
     static int blocks_per_sm = 0;
-    if (!blocks_per_sm)
-        blocks_per_sm = GRID ? blocks_for(k_gwn2<SCREENED, PREC, SHAPE>) : blocks_for(k_gwn<false, SCREENED, PREC, 0>);
+    if (!blocks_per_sm) blocks_per_sm = blocks_for(k_gwn<GRID, SCREENED, PREC, SHAPE>);
     long long want = (a.ngroups + kGwnWarps - 1) / kGwnWarps;
     long long grid = (long long)num_sms() * blocks_per_sm;
     if (want < grid) grid = want > 0 ? want : 1;
-    if (GRID)
-        k_gwn2<SCREENED, PREC, SHAPE><<<(unsigned)grid, kGwnWarps * 32, 0, s>>>(a);
-    else
-        k_gwn<false, SCREENED, PREC, 0><<<(unsigned)grid, kGwnWarps * 32, 0, s>>>(a);
+    k_gwn<GRID, SCREENED, PREC, SHAPE><<<(unsigned)grid, kGwnWarps * 32, 0, s>>>(a);
     DWG_CHECK_LAUNCH();
     return DWG_OK;
 }
@@ -591,7 +475,7 @@ int gwn_eval(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, float*
         a.rx = a.ry = a.rz = 0;
         a.ox = a.oy = a.oz = a.h = 0.f;
         a.bx = a.by = 1;
-        a.ngroups = (q.nq + 31) / 32;
+        a.ngroups = (q.nq + 31) / 32;  // one point per lane
         if (a.ngroups == 0) return DWG_OK;
         return dispatch<false>(a, p, s);
     }

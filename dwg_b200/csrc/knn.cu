@@ -518,8 +518,8 @@ __global__ void __launch_bounds__(128) k_knn_thread(KnnArgs a) {
 // then ranks the same candidates for its own query: no divergence, one search
 // per cell instead of one per query.  A cell whose candidate set does not fit
 // (or has no finite bound) sends its queries to the per-thread search.
-constexpr int kCqWarps = 2;
-constexpr int kCqNodes = 2048;  // frontier capacity per warp (ping-pong pair, shared memory)
+constexpr int kCqWarps = 4;
+constexpr int kCqNodes = 1024;  // frontier capacity per warp (ping-pong pair, shared memory), at level >= 1
 constexpr int kCqChunk = 256;   // candidates staged in shared memory at a time
 
 __device__ __forceinline__ float cell_mid(float lo, int i, float h) { return lo + ((float)i + 0.5f) * h; }
@@ -527,10 +527,26 @@ __device__ __forceinline__ float cell_mid(float lo, int i, float h) { return lo 
 // kb from the 3x3x3 block around each cell: the 16th smallest distance, or
 // +inf when the block holds fewer than 16 points
 __global__ void k_kb_local(KnnGrid g, const int* __restrict__ cell_start, const float4* __restrict__ pts,
-                           float* __restrict__ kb) {
+                           const unsigned char* __restrict__ occ1, int D0, int D1, float* __restrict__ kb) {
     const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (c >= (long long)g.G0 * g.G1 * g.G2) return;
     const int i = (int)(c % g.G0), j = (int)((c / g.G0) % g.G1), k = (int)(c / ((long long)g.G0 * g.G1));
+    if (occ1) {
+        // the 3x3x3 block lies in at most 2x2x2 nodes of pyramid level 1:
+        // when they are all empty the bound stays +inf (cheap for empty space)
+        bool any = false;
+        for (int z = max(k - 1, 0) >> 1; z <= min(k + 1, g.G2 - 1) >> 1 && !any; ++z)
+            for (int y = max(j - 1, 0) >> 1; y <= min(j + 1, g.G1 - 1) >> 1 && !any; ++y)
+                for (int x = max(i - 1, 0) >> 1; x <= min(i + 1, g.G0 - 1) >> 1; ++x)
+                    if (occ1[x + (long long)D0 * (y + (long long)D1 * z)]) {
+                        any = true;
+                        break;
+                    }
+        if (!any) {
+            kb[c] = INFINITY;
+            return;
+        }
+    }
     const float x = cell_mid(g.lo0, i, g.h), y = cell_mid(g.lo1, j, g.h), z = cell_mid(g.lo2, k, g.h);
     float d[kKnnBoundK];
 #pragma unroll
@@ -606,7 +622,9 @@ static int build_kbound(const KnnIndex& ix, cudaStream_t s) {
     KnnGrid g{ix.G[0], ix.G[1], ix.G[2], ix.lo[0], ix.lo[1], ix.lo[2], ix.h, ix.inv_h};
     DWG_TRY(ix.kb.reserve(ncell));
     DWG_TRY(ix.kb_tmp.reserve(ncell));
-    k_kb_local<<<div_up(ncell, 128), 128, 0, s>>>(g, ix.cell_start.ptr, ix.pts.ptr, ix.kb.ptr);
+    const unsigned char* occ1 = ix.levels >= 1 ? ix.occ.ptr + ix.loff[1] : nullptr;
+    k_kb_local<<<div_up(ncell, 128), 128, 0, s>>>(g, ix.cell_start.ptr, ix.pts.ptr, occ1, ix.ldim[1][0], ix.ldim[1][1],
+                                                   ix.kb.ptr);
     DWG_CHECK_LAUNCH();
     const int gmax = max(ix.G[0], max(ix.G[1], ix.G[2]));
     int step = 1;
@@ -721,6 +739,7 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
         bool ok = isfinite(R);
         int* cur = nodes[w][0];
         int nf = 0;
+        int l = 0;  // the level the frontier starts at
         if (ok) {
             const float R2 = R * R;
             // the ball's box in cells
@@ -728,7 +747,6 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
             const int y0 = cell_coord(y - R, a.g.lo1, a.g.inv_h, a.g.G1), y1 = cell_coord(y + R, a.g.lo1, a.g.inv_h, a.g.G1);
             const int z0 = cell_coord(z - R, a.g.lo2, a.g.inv_h, a.g.G2), z1 = cell_coord(z + R, a.g.lo2, a.g.inv_h, a.g.G2);
             // coarsest-enough level: at most 2048 nodes cover the box
-            int l = 0;
             for (;;) {
                 const long long nn = (long long)((x1 >> l) - (x0 >> l) + 1) * ((y1 >> l) - (y0 >> l) + 1) *
                                      ((z1 >> l) - (z0 >> l) + 1);
@@ -754,8 +772,8 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
                 nf += __popc(bal);
             }
             ok = nf <= kCqNodes;
-            // stage B: down to the cells
-            for (int lv = l; lv >= 1 && ok; --lv) {
+            // stage B: down to level 1 (the cells are expanded while streaming)
+            for (int lv = l; lv >= 2 && ok; --lv) {
                 __syncwarp();
                 const int* D = a.ldim[lv];
                 int nn = 0;
@@ -819,13 +837,28 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
                 __syncwarp();
                 staged = 0;
             };
-            for (int b = 0; b < nf; b += 32) {
+            // frontier entries are cells (level 0) or level-1 nodes of up to 8 cells
+            const int per = l >= 1 ? 8 : 1;
+            for (int b = 0; b < nf * per; b += 32) {
                 const int t = b + lane;
                 int s0 = 0, cnt = 0;
-                if (t < nf) {
-                    const int cell = cur[t];
-                    s0 = a.cell_start[cell];
-                    cnt = a.cell_start[cell + 1] - s0;
+                if (t < nf * per) {
+                    int cell;
+                    bool hit = true;
+                    if (per == 1) {
+                        cell = cur[t];
+                    } else {
+                        const int* D = a.ldim[1];
+                        const int node = cur[t >> 3], oc = t & 7;
+                        const int ni = node % D[0], nj = (node / D[0]) % D[1], nk = node / (D[0] * D[1]);
+                        const int ui = 2 * ni + (oc & 1), uj = 2 * nj + ((oc >> 1) & 1), uk = 2 * nk + (oc >> 2);
+                        hit = cq_node_hit(a, 0, ui, uj, uk, x, y, z, R2, eps);
+                        cell = ui + a.g.G0 * (uj + a.g.G1 * uk);
+                    }
+                    if (hit) {
+                        s0 = a.cell_start[cell];
+                        cnt = a.cell_start[cell + 1] - s0;
+                    }
                 }
                 const int mx = __reduce_max_sync(FULL, cnt);
                 for (int j = 0; j < mx; ++j) {

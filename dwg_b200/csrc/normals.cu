@@ -150,6 +150,43 @@ int zero_repair(const KnnIndex& ix, const float* pos, int L, float* N, const uns
     return DWG_OK;
 }
 
+__global__ void k_iota(int* __restrict__ v, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = i;
+}
+
+__global__ void k_area_div(float* __restrict__ areas, const int* __restrict__ idx, int k) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < k) areas[idx[i]] /= 1000.0f;
+}
+
+int outlier_filter(float* areas, int n, float thr, cudaStream_t s) {
+    DWG_REQUIRE(areas && n >= 1, "outlier_filter: bad arguments");
+    if (!(thr > 0.f)) return DWG_OK;
+    const int k = (int)ceilf((float)n * thr);
+    if (k <= 0) return DWG_OK;
+    DevBuf<float> keys_out;
+    DevBuf<int> ids, ids_out;
+    DevBuf<unsigned char> tmp;
+    DWG_TRY(keys_out.reserve(n));
+    DWG_TRY(ids.reserve(n));
+    DWG_TRY(ids_out.reserve(n));
+    k_iota<<<div_up(n, 256), 256, 0, s>>>(ids.ptr, n);
+    DWG_CHECK_LAUNCH();
+    size_t bytes = 0;
+    DWG_CHECK_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, bytes, areas, keys_out.ptr, ids.ptr, ids_out.ptr, n,
+                                                             0, 32, s));
+    DWG_TRY(tmp.reserve(bytes + 256));
+    bytes = tmp.n;
+    DWG_CHECK_CUDA(cub::DeviceRadixSort::SortPairsDescending(tmp.ptr, bytes, areas, keys_out.ptr, ids.ptr, ids_out.ptr,
+                                                             n, 0, 32, s));
+    const int kk = k < n ? k : n;
+    k_area_div<<<div_up(kk, 256), 256, 0, s>>>(areas, ids_out.ptr, kk);
+    DWG_CHECK_LAUNCH();
+    DWG_CHECK_CUDA(cudaStreamSynchronize(s));  // the sort buffers are released on return
+    return DWG_OK;
+}
+
 // LoadNormals (src/TurboDWG.cu:206-236)
 __global__ void k_load_normals(const int* __restrict__ knn, int k, long long nq, const float* __restrict__ LN,
                                float* __restrict__ out) {

@@ -26,6 +26,11 @@ struct ZeroRepairWs {
 int zero_repair(const KnnIndex& ix, const float* positions, int L, float* normals, const unsigned char* is_zero,
                 int k, int min_zero, ZeroRepairWs& ws, cudaStream_t s);
 
+// OutlierFilter + AsFiltertoZero (src/TurboDWG.cu:991-1009, :442-454): the
+// ceil(n * thr) largest areas are divided by 1000; equal areas are taken in
+// index order (a stable descending sort)
+int outlier_filter(float* areas, int n, float thr, cudaStream_t s);
+
 int load_normals(const int* knn, int k, long long nq, const float* leaf_normals, float* out, cudaStream_t s);
 int radii(const float* P, int n, const int* knn, int k, float* out, cudaStream_t s);
 

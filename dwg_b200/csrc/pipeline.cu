@@ -84,6 +84,12 @@ __global__ void k_gather_xyz(const float* __restrict__ src, const int* __restric
     dst[(size_t)j * 3 + 2] = src[(size_t)i * 3 + 2];
 }
 
+// area of canonical leaf i into the octree record of sorted point i (the two orders coincide for t2)
+__global__ void k_set_area(float4* __restrict__ pa, const float* __restrict__ area, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) pa[i].w = area[i];
+}
+
 __global__ void k_fill(float* __restrict__ x, long long n, float v) {
     long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i < n) x[i] = v;
@@ -328,6 +334,12 @@ int Pipeline::setup(const float* points_dev, const float* normals_dev, int n_poi
     k_gather_xyz<<<div_up(L, 256), 256, 0, s>>>(raw_pos.ptr, t2.perm.ptr, L, leaf_pos.ptr);
     k_fill<<<div_up(L, 256), 256, 0, s>>>(leaf_rad.ptr, L, p.screen);
     DWG_CHECK_LAUNCH();
+    if (p.as_thres > 0.f) {
+        // OutlierFilter on the leaves' areas (src/TurboDWG.cu:512), canonical order
+        DWG_TRY(outlier_filter(leaf_area.ptr, L, p.as_thres, s));
+        k_set_area<<<div_up(L, 256), 256, 0, s>>>(t2.pa.ptr, leaf_area.ptr, L);
+        DWG_CHECK_LAUNCH();
+    }
     if (p.in_normal < 3) {
         DWG_TRY(octree_set_point_data(t1, Nin.ptr, nullptr, nullptr, s));
         DevBuf<double> sm, part;
@@ -553,7 +565,9 @@ int Pipeline::finalize() {
             DWG_TRY(radii(P.ptr, n, nb.ptr, prm.final_kw, pt_rad.ptr, s));
             DWG_CHECK_CUDA(cudaStreamSynchronize(s));
         }
-        DWG_TRY(octree_set_point_data(t1, point_nrm.ptr, nullptr, pt_rad.ptr, s));
+        // OutlierFilter on the points' areas (src/TurboDWG.cu:876), input order
+        if (prm.as_thres > 0.f) DWG_TRY(outlier_filter(area_pts.ptr, n, prm.as_thres, s));
+        DWG_TRY(octree_set_point_data(t1, point_nrm.ptr, prm.as_thres > 0.f ? area_pts.ptr : nullptr, pt_rad.ptr, s));
         DWG_TRY(p_sorted.reserve((size_t)n * 3));
         k_sorted_xyz<<<div_up(n, 256), 256, 0, s>>>(t1.pa.ptr, n, p_sorted.ptr);
         DWG_CHECK_LAUNCH();

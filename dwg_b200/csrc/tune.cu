@@ -7,8 +7,9 @@
 //      opened; correctly rounded terms, compensated accumulation);
 //   2. for each candidate opening ratio, the RMS and max error of the
 //      Barnes-Hut sums at those samples against the exact ones;
-//   3. among the ratios within `tol`, time a full grid evaluation and keep
-//      the fastest; then time the four brick shapes at that ratio.
+//   3. among the ratios within `tol` (tol <= 0: within the error of the
+//      reference's beta = 2.3), time a full grid evaluation and keep the
+//      fastest; then time the four brick shapes at that ratio.
 // The reference setting (beta 2.3, 4x4x2 bricks) is timed beside it.
 #include <algorithm>
 #include <random>
@@ -63,7 +64,7 @@ static int time_grid(Pipeline& p, const dwg_gwn_params& gp, float* ms, cudaStrea
 
 int autotune(const float* points_dev, int n, const dwg_params& prm, float tol, int samples, int warm_iters,
              cudaStream_t stream, dwg_tune_result* out) {
-    DWG_REQUIRE(out && tol > 0.f && samples >= 32, "autotune: bad arguments");
+    DWG_REQUIRE(out && samples >= 32, "autotune: bad arguments");
     Pipeline p;
     DWG_TRY(p.setup(points_dev, nullptr, n, prm, stream));
     DWG_TRY(p.iterate(warm_iters > 0 ? warm_iters : 1));
@@ -98,11 +99,15 @@ int autotune(const float* points_dev, int n, const dwg_params& prm, float tol, i
     std::vector<float> we((size_t)m), wb((size_t)m);
     DWG_CHECK_CUDA(cudaMemcpyAsync(we.data(), w_exact.ptr, sizeof(float) * m, cudaMemcpyDeviceToHost, s));
     DWG_CHECK_CUDA(cudaStreamSynchronize(s));
-    // error of each opening ratio
-    float best_beta = -1.f, best_ms = 0.f, best_rms = 0.f, best_max = 0.f;
-    for (float beta : kBetas) {
+    // error of each opening ratio against the exact sums
+    double fsq = 0;
+    for (int i = 0; i < m; ++i) fsq += (double)we[i] * we[i];
+    constexpr int nb = sizeof(kBetas) / sizeof(kBetas[0]);
+    float rms_of[nb], max_of[nb];
+    float ref_rms = 0.f;
+    for (int bi = 0; bi < nb; ++bi) {
         dwg_gwn_params gb = gp;
-        gb.beta = beta;
+        gb.beta = kBetas[bi];
         DWG_TRY(gwn_eval(p.t2, qs, gb, w.ptr, nullptr, nullptr, s, p.cur_sigma.ptr));
         DWG_CHECK_CUDA(cudaMemcpyAsync(wb.data(), w.ptr, sizeof(float) * m, cudaMemcpyDeviceToHost, s));
         DWG_CHECK_CUDA(cudaStreamSynchronize(s));
@@ -112,18 +117,29 @@ int autotune(const float* points_dev, int n, const dwg_params& prm, float tol, i
             se += e * e;
             mx = std::max(mx, std::fabs(e));
         }
-        const float rms = (float)std::sqrt(se / m);
-        if (rms > tol) continue;
+        rms_of[bi] = (float)std::sqrt(se / m);
+        max_of[bi] = (float)mx;
+        if (kBetas[bi] == 2.3f) ref_rms = rms_of[bi];
+    }
+    // tol <= 0: no less accurate than the reference's beta = 2.3
+    const float limit = tol > 0.f ? tol : ref_rms * 1.000001f;
+    float best_beta = -1.f, best_ms = 0.f, best_rms = 0.f, best_max = 0.f;
+    for (int bi = 0; bi < nb; ++bi) {
+        if (rms_of[bi] > limit) continue;
+        dwg_gwn_params gb = gp;
+        gb.beta = kBetas[bi];
         float ms = 0.f;
         DWG_TRY(time_grid(p, gb, &ms, s));
         if (best_beta < 0.f || ms < best_ms) {
-            best_beta = beta;
+            best_beta = kBetas[bi];
             best_ms = ms;
-            best_rms = rms;
-            best_max = (float)mx;
+            best_rms = rms_of[bi];
+            best_max = max_of[bi];
         }
     }
-    DWG_REQUIRE(best_beta > 0.f, "autotune: no opening ratio reaches RMS error %g", tol);
+    out->ref_rms_err = ref_rms;
+    out->field_rms = (float)std::sqrt(fsq / m);
+    DWG_REQUIRE(best_beta > 0.f, "autotune: no opening ratio reaches RMS error %g", limit);
     // brick shape at that ratio
     int best_tile = 0;
     float tile_ms = 0.f;

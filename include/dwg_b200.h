@@ -240,6 +240,7 @@ typedef struct {
     int precision;          /* dwg_gwn_params.precision */
     int use_graph;          /* capture one iteration in a CUDA graph and replay it */
     int tile;               /* dwg_gwn_params.tile of the grid sums */
+    float as_thres;         /* --As_thres (0): the ceil(n * as_thres) largest areas are divided by 1000 */
 } dwg_params;
 
 void dwg_params_default(dwg_params* p);
@@ -290,7 +291,9 @@ int dwg_batch_cloud(dwg_batch* b, int index, dwg_pipeline** cloud);
  * cloud it runs `warm_iters` DWG iterations, measures the RMS error of the
  * Barnes-Hut sums against exact sums at `samples` seeded grid samples for
  * candidate opening ratios beta in [1.5, 4.5], times a full grid evaluation
- * for those within `tol`, and then the four brick shapes at the fastest.
+ * for those within `tol` (absolute RMS; tol <= 0: no larger than the error
+ * of the reference's beta = 2.3), and then the four brick shapes at the
+ * fastest.
  * ------------------------------------------------------------------------ */
 typedef struct {
     float beta;     /* chosen opening ratio */
@@ -299,6 +302,8 @@ typedef struct {
     float max_err;  /* max  |w_beta - w_exact| at the samples */
     float grid_ms;  /* one grid evaluation at (beta, tile) */
     float ref_ms;   /* one grid evaluation at beta 2.3, tile 0 */
+    float ref_rms_err; /* RMS error at beta 2.3 */
+    float field_rms;   /* RMS of the exact sums at the samples */
 } dwg_tune_result;
 int dwg_autotune(const float* points_dev, int n, const dwg_params* params, float tol, int samples,
                  int warm_iters, void* stream, dwg_tune_result* out);

@@ -1042,6 +1042,27 @@ static void field_pass(const dwgo_octree* tr, const float* pos, int n, const flo
     free(wg);
 }
 
+static const float* g_filter_keys;
+static int cmp_desc_stable(const void* x, const void* y) {
+    const int a = *(const int*)x, b = *(const int*)y;
+    if (g_filter_keys[a] > g_filter_keys[b]) return -1;
+    if (g_filter_keys[a] < g_filter_keys[b]) return 1;
+    return a < b ? -1 : (a > b);
+}
+
+void dwgo_outlier_filter(float* A, int n, float thr) {
+    if (!(thr > 0.f) || n <= 0) return;
+    int k = (int)ceilf((float)n * thr);
+    if (k > n) k = n;
+    if (k <= 0) return;
+    int* idx = xmalloc((size_t)n * sizeof(int));
+    for (int i = 0; i < n; i++) idx[i] = i;
+    g_filter_keys = A;
+    qsort(idx, (size_t)n, sizeof(int), cmp_desc_stable);
+    for (int i = 0; i < k; i++) A[idx[i]] /= 1000.0f;
+    free(idx);
+}
+
 dwgo_run* dwgo_reconstruct(const float* P, int n, const float* N_in,
                            const dwgo_params* prm, int nthreads) {
     dwgo_run* run = xcalloc(1, sizeof(dwgo_run));
@@ -1112,6 +1133,7 @@ dwgo_run* dwgo_reconstruct(const float* P, int n, const float* N_in,
     free(Ld);
     float* lA = xmalloc((size_t)L * sizeof(float));
     for (int i = 0; i < L; i++) lA[i] = prm->area;
+    dwgo_outlier_filter(lA, L, prm->as_thres); /* src/TurboDWG.cu:512 */
     float* lrad = xmalloc((size_t)L * sizeof(float));
     if (prm->use_radii) {
         int* nb = xmalloc((size_t)L * prm->kw * sizeof(int));
@@ -1191,6 +1213,7 @@ dwgo_run* dwgo_reconstruct(const float* P, int n, const float* N_in,
         free(nb);
         float* pA = xmalloc((size_t)n * sizeof(float));
         for (int i = 0; i < n; i++) pA[i] = prm->area;
+        dwgo_outlier_filter(pA, n, prm->as_thres); /* src/TurboDWG.cu:876 */
         float* prad = xmalloc((size_t)n * sizeof(float));
         if (prm->use_radii) {
             int* nb2 = xmalloc((size_t)n * prm->final_kw * sizeof(int));

@@ -97,7 +97,12 @@ typedef struct {
     float beta, area, screen;
     int knn_tri;         /* 15 */
     int knn_zero;        /* 10 */
+    float as_thres;      /* --As_thres (0) */
 } dwgo_params;
+
+/* OutlierFilter + AsFiltertoZero (src/TurboDWG.cu:991-1009, :442-454): the
+ * ceil(n * thr) largest areas divided by 1000, equal areas in index order */
+void dwgo_outlier_filter(float* A, int n, float thr);
 
 typedef struct dwgo_run dwgo_run;
 dwgo_run* dwgo_reconstruct(const float* P, int n, const float* N_in,

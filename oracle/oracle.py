@@ -40,7 +40,7 @@ class Params(C.Structure):
         ("offset_1", C.c_float), ("offset_2", C.c_float),
         ("use_leaves_generate", C.c_int), ("total_iter", C.c_int),
         ("beta", C.c_float), ("area", C.c_float), ("screen", C.c_float),
-        ("knn_tri", C.c_int), ("knn_zero", C.c_int),
+        ("knn_tri", C.c_int), ("knn_zero", C.c_int), ("as_thres", C.c_float),
     ]
 
 
@@ -80,6 +80,7 @@ def lib():
     L.dwgo_gauss_map.argtypes = [_f32p, C.c_int, _f32p]
     L.dwgo_load_normals.argtypes = [_i32p, C.c_int, C.c_longlong, _f32p, _f32p]
     L.dwgo_radii.argtypes = [_f32p, C.c_int, _i32p, C.c_int, _f32p]
+    L.dwgo_outlier_filter.argtypes = [_f32p, C.c_int, C.c_float]
     L.dwgo_reconstruct.restype = vp
     L.dwgo_reconstruct.argtypes = [_f32p, C.c_int, vp, C.POINTER(Params), C.c_int]
     L.dwgo_run_free.argtypes = [vp]
@@ -233,6 +234,13 @@ def marching_cubes(field, res, origin, spacing, iso, want=("tris", "centroids", 
     return out
 
 
+def outlier_filter(A, thr):
+    """OutlierFilter + AsFiltertoZero (src/TurboDWG.cu:991-1009, :442-454)."""
+    A = np.ascontiguousarray(A, np.float32).copy()
+    lib().dwgo_outlier_filter(A, len(A), C.c_float(thr))
+    return A
+
+
 def knn(P, Q, k, nthreads=None):
     """Brute-force k nearest, ordered by the cukd key (dist2 bits, id)."""
     P = _f32(P).reshape(-1)
@@ -289,7 +297,7 @@ def radii(P, knn_idx):
 DEFAULT_PARAMS = dict(in_normal=3, grid_reso=400, final_reso=500, kw=10, final_kw=10,
                       normal_kw=10, max_depth=10, lambda_=10.0, min_num=0, use_radii=0,
                       offset_1=0.05, offset_2=0.01, use_leaves_generate=0, total_iter=40,
-                      beta=2.3, area=2e-6, screen=0.0015, knn_tri=15, knn_zero=10)
+                      beta=2.3, area=2e-6, screen=0.0015, knn_tri=15, knn_zero=10, as_thres=0.0)
 
 
 def reconstruct(P, normals=None, nthreads=None, **kw):

@@ -181,3 +181,13 @@ def test_oracle_reconstruct_small_sphere():
     assert s.mean() > 0.7
     sp = np.sign((r["point_nrm"] * Pn).sum(1))
     assert sp.mean() > 0.98
+
+
+def test_oracle_outlier_filter_known_answer(oracle_lib):
+    A = np.array([1, 3, 3, 2, 5, 5, 0.5], np.float32)
+    # ceil(7 * 0.4) = 3 largest: the two 5s, then the first 3 (index order on ties)
+    got = oracle_lib.outlier_filter(A, 0.4)
+    want = A.copy()
+    want[[4, 5, 1]] /= 1000.0
+    assert np.array_equal(got, want)
+    assert np.array_equal(oracle_lib.outlier_filter(A, 0.0), A)
