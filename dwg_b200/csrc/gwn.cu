@@ -169,27 +169,32 @@ __device__ __forceinline__ float gwn_term_masked(bool take, float r2, float d, f
     return v;
 }
 
-// The sums of group g: 64 queries, two per lane -- for a grid, the brick of
-// SHAPE (32 samples) and the brick above it in z; for points, 64
-// consecutive (Morton-ordered) points.  The warp walks the octree once for
-// all 64: the stack entries carry the masks of the lanes whose first and
-// second query opened the node, so every query takes exactly the reference's
-// per-query decisions -- a child is a dipole term when |CM - q| > beta R,
-// otherwise it is opened, and leaves are summed point by point -- while the
-// traversal (stack pops, record loads, the loop over children) is shared.
-// Terms are evaluated branch-free and masked, so that a lane's two queries
-// never split the warp; each query's terms keep their depth-first order.
+// Queries per lane: grids take NQ_GRID samples per lane (the brick of SHAPE
+// stacked NQ_GRID times in z), point queries one (consecutive points spread
+// over more of the tree than grid bricks, which costs more than it shares).
+#ifndef DWG_NQ_GRID
+#define DWG_NQ_GRID 2
+#endif
+constexpr int kNqGrid = DWG_NQ_GRID;
+
+// The sums of group g: 32 x NQ queries, NQ per lane.  The warp walks the
+// octree once for all of them: each stack entry carries, per query slot, the
+// mask of the lanes whose query opened the node, so every query takes exactly
+// the reference's per-query decisions -- a child is a dipole term when
+// |CM - q| > beta R, otherwise it is opened, and leaves are summed point by
+// point -- while the traversal (stack pops, record loads, the loop over
+// children) is shared.  Terms are evaluated branch-free and masked, so that a
+// lane's queries never split the warp; each query's terms keep their
+// depth-first order (its value does not depend on NQ or the brick shape).
 // Returns the lane's term count.
-template <bool GRID, bool SCREENED, int PREC, int SHAPE>
-__device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g, int lane, int4* __restrict__ stk,
-                                         float sigma, float sigma_l2e) {
-    // grids take two samples per lane; point queries one (64 consecutive
-    // points span more of the tree than 32, which costs more than it shares)
-    constexpr bool TWO = GRID;
+template <bool GRID, bool SCREENED, int PREC, int SHAPE, int NQ>
+__device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g, int lane,
+                                         int* __restrict__ stk_node, unsigned* __restrict__ stk_mask, float sigma,
+                                         float sigma_l2e) {
     const unsigned FULL = 0xffffffffu;
-    bool valid0, valid1;
-    long long qi0, qi1;
-    float qx0, qy0, qz0, qx1, qy1, qz1;
+    bool valid[NQ];
+    long long qi[NQ];
+    float qx[NQ], qy[NQ], qz[NQ];
     if (GRID) {
         using B = Brick<SHAPE>;
         const long long bxi = (long long)(g % (unsigned long long)a.bx);
@@ -197,49 +202,52 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
         const long long byi = (long long)(t % (unsigned long long)a.by);
         const long long bzi = (long long)(t / (unsigned long long)a.by);
         const long long x = bxi * B::X + (lane % B::X), y = byi * B::Y + ((lane / B::X) % B::Y);
-        const long long z0 = bzi * (2 * B::Z) + lane / (B::X * B::Y), z1 = z0 + B::Z;
+        const long long z0 = bzi * (NQ * B::Z) + lane / (B::X * B::Y);
         const bool xy_ok = x < a.rx && y < a.ry;
-        valid0 = xy_ok && z0 < a.rz;
-        valid1 = xy_ok && z1 < a.rz;
-        qi0 = x + (long long)a.rx * (y + (long long)a.ry * z0);
-        qi1 = x + (long long)a.rx * (y + (long long)a.ry * z1);
-        qx0 = __fadd_rn(a.ox, __fmul_rn((float)x, a.h));
-        qy0 = __fadd_rn(a.oy, __fmul_rn((float)y, a.h));
-        qx1 = qx0;
-        qy1 = qy0;
-        qz0 = __fadd_rn(a.oz, __fmul_rn((float)z0, a.h));
-        qz1 = __fadd_rn(a.oz, __fmul_rn((float)z1, a.h));
-    } else {
-        qi0 = (long long)g * (TWO ? 64 : 32) + lane;
-        qi1 = qi0 + 32;
-        valid0 = qi0 < a.nq;
-        valid1 = TWO && qi1 < a.nq;
-        qx0 = qy0 = qz0 = qx1 = qy1 = qz1 = 0.f;
-        if (valid0) {
-            qx0 = a.q[qi0 * 3];
-            qy0 = a.q[qi0 * 3 + 1];
-            qz0 = a.q[qi0 * 3 + 2];
+        const float fx = __fadd_rn(a.ox, __fmul_rn((float)x, a.h));
+        const float fy = __fadd_rn(a.oy, __fmul_rn((float)y, a.h));
+#pragma unroll
+        for (int u = 0; u < NQ; ++u) {
+            const long long z = z0 + u * B::Z;
+            valid[u] = xy_ok && z < a.rz;
+            qi[u] = x + (long long)a.rx * (y + (long long)a.ry * z);
+            qx[u] = fx;
+            qy[u] = fy;
+            qz[u] = __fadd_rn(a.oz, __fmul_rn((float)z, a.h));
         }
-        if (valid1) {
-            qx1 = a.q[qi1 * 3];
-            qy1 = a.q[qi1 * 3 + 1];
-            qz1 = a.q[qi1 * 3 + 2];
+    } else {
+#pragma unroll
+        for (int u = 0; u < NQ; ++u) {
+            qi[u] = (long long)g * (32 * NQ) + u * 32 + lane;
+            valid[u] = qi[u] < a.nq;
+            qx[u] = qy[u] = qz[u] = 0.f;
+            if (valid[u]) {
+                qx[u] = a.q[qi[u] * 3];
+                qy[u] = a.q[qi[u] * 3 + 1];
+                qz[u] = a.q[qi[u] * 3 + 2];
+            }
         }
     }
-    float s0 = 0.f, c0 = 0.f, s1 = 0.f, c1 = 0.f;
-    int n0 = 0, n1 = 0;
+    float sum[NQ], cmp[NQ];
+    int nt[NQ];
+#pragma unroll
+    for (int u = 0; u < NQ; ++u) {
+        sum[u] = 0.f;
+        cmp[u] = 0.f;
+        nt[u] = 0;
+    }
 
-    auto leaf_points = [&](int start, int cnt, float qx, float qy, float qz, float& s, float& c, int& n) {
+    auto leaf_points = [&](int start, int cnt, int u) {
         for (int j = start; j < start + cnt; ++j) {
             const float4 p = a.pa[j];
             const float4 nn = a.nr[j];
-            const float dx = p.x - qx, dy = p.y - qy, dz = p.z - qz;
+            const float dx = p.x - qx[u], dy = p.y - qy[u], dz = p.z - qz[u];
             const float d = p.w * fmaf(dx, nn.x, fmaf(dy, nn.y, dz * nn.z));
             const float sc = a.use_radii ? nn.w : a.screen;
             float v;
             if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, sc, sigma, sigma_l2e, v)) {
-                acc_add<PREC>(s, c, v);
-                ++n;
+                acc_add<PREC>(sum[u], cmp[u], v);
+                ++nt[u];
             }
         }
     };
@@ -251,7 +259,7 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
     // opened (pushed with the queries that need it) otherwise; both use the
     // same d2.  Larger leaves (every leaf when radii apply) are summed point
     // by point.
-    auto child = [&](int cidx, const float4& na, const float4& nb, bool act0, bool act1, int& sp) {
+    auto child = [&](int cidx, const float4& na, const float4& nb, const bool* act, int& sp) {
         const unsigned meta = (unsigned)__float_as_int(nb.w);
         const bool leaf = (meta & kMetaLeafBit) != 0;
         if (leaf && (!(meta & kMetaSingle) || a.use_radii)) {
@@ -259,31 +267,49 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
             if (cnt < 0 || st + cnt > a.num_points) {
                 if (lane == 0) atomicOr(&a.work[1], 4u);
             } else {
-                if (act0) leaf_points(st, cnt, qx0, qy0, qz0, s0, c0, n0);
-                if (act1) leaf_points(st, cnt, qx1, qy1, qz1, s1, c1, n1);
+#pragma unroll
+                for (int u = 0; u < NQ; ++u)
+                    if (act[u]) leaf_points(st, cnt, u);
             }
             return;
         }
-        const float dx0 = __fsub_rn(na.x, qx0), dy0 = __fsub_rn(na.y, qy0), dz0 = __fsub_rn(na.z, qz0);
-        const float dx1 = __fsub_rn(na.x, qx1), dy1 = __fsub_rn(na.y, qy1), dz1 = __fsub_rn(na.z, qz1);
-        const float d20 = sq3_rn(dx0, dy0, dz0), d21 = sq3_rn(dx1, dy1, dz1);
-        const bool far0 = leaf || d20 > na.w, far1 = leaf || d21 > na.w;
-        const bool take0 = act0 && far0, take1 = act1 && far1;
-        if (__any_sync(FULL, take0 || take1)) {
-            const float dd0 = fmaf(dx0, nb.x, fmaf(dy0, nb.y, dz0 * nb.z));
-            const float dd1 = fmaf(dx1, nb.x, fmaf(dy1, nb.y, dz1 * nb.z));
-            bool k0, k1;
-            const float v0 = gwn_term_masked<SCREENED, PREC>(take0, d20, dd0, a.screen, sigma, sigma_l2e, k0);
-            const float v1 = gwn_term_masked<SCREENED, PREC>(take1, d21, dd1, a.screen, sigma, sigma_l2e, k1);
-            if (k0) acc_add<PREC>(s0, c0, v0);
-            if (k1) acc_add<PREC>(s1, c1, v1);
-            n0 += (int)k0;
-            n1 += (int)k1;
+        float dx[NQ], dy[NQ], dz[NQ], d2[NQ];
+        bool far[NQ], take[NQ];
+        bool any = false;
+#pragma unroll
+        for (int u = 0; u < NQ; ++u) {
+            dx[u] = __fsub_rn(na.x, qx[u]);
+            dy[u] = __fsub_rn(na.y, qy[u]);
+            dz[u] = __fsub_rn(na.z, qz[u]);
+            d2[u] = sq3_rn(dx[u], dy[u], dz[u]);
+            far[u] = leaf || d2[u] > na.w;
+            take[u] = act[u] && far[u];
+            any = any || take[u];
         }
-        const unsigned nm0 = __ballot_sync(FULL, act0 && !far0), nm1 = __ballot_sync(FULL, act1 && !far1);
-        if (nm0 | nm1) {
+        if (__any_sync(FULL, any)) {
+#pragma unroll
+            for (int u = 0; u < NQ; ++u) {
+                const float dd = fmaf(dx[u], nb.x, fmaf(dy[u], nb.y, dz[u] * nb.z));
+                bool k;
+                const float v = gwn_term_masked<SCREENED, PREC>(take[u], d2[u], dd, a.screen, sigma, sigma_l2e, k);
+                if (k) acc_add<PREC>(sum[u], cmp[u], v);
+                nt[u] += (int)k;
+            }
+        }
+        unsigned nm[NQ];
+        unsigned anym = 0;
+#pragma unroll
+        for (int u = 0; u < NQ; ++u) {
+            nm[u] = __ballot_sync(FULL, act[u] && !far[u]);
+            anym |= nm[u];
+        }
+        if (anym) {
             if (sp < kGwnStack) {
-                if (lane == 0) stk[sp] = make_int4(cidx, (int)nm0, (int)nm1, 0);
+                if (lane == 0) {
+                    stk_node[sp] = cidx;
+#pragma unroll
+                    for (int u = 0; u < NQ; ++u) stk_mask[sp * NQ + u] = nm[u];
+                }
                 ++sp;
             } else if (lane == 0) {
                 atomicOr(&a.work[1], 1u);
@@ -296,27 +322,36 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
         const float4 ra = a.node_a[0], rb = a.node_b[0];
         const unsigned rm = (unsigned)__float_as_int(rb.w);
         if (rm & kMetaLeafBit) {
-            child(0, ra, rb, valid0, valid1, sp);  // a leaf root is summed; nothing is pushed
+            child(0, ra, rb, valid, sp);  // a leaf root is summed; nothing is pushed
         } else {
-            const unsigned m0 = __ballot_sync(FULL, valid0), m1 = __ballot_sync(FULL, valid1);
-            if (lane == 0) stk[0] = make_int4(0, (int)m0, (int)m1, 0);
+            unsigned m[NQ];
+#pragma unroll
+            for (int u = 0; u < NQ; ++u) m[u] = __ballot_sync(FULL, valid[u]);
+            if (lane == 0) {
+                stk_node[0] = 0;
+#pragma unroll
+                for (int u = 0; u < NQ; ++u) stk_mask[u] = m[u];
+            }
             sp = 1;
         }
     }
     while (sp > 0) {
         __syncwarp();
-        const int4 e = stk[--sp];
+        --sp;
+        const int node = stk_node[sp];
+        bool act[NQ];
+#pragma unroll
+        for (int u = 0; u < NQ; ++u) act[u] = (stk_mask[sp * NQ + u] >> lane) & 1u;
         __syncwarp();
-        if (e.x < 0 || e.x >= a.num_nodes) {
+        if (node < 0 || node >= a.num_nodes) {
             if (lane == 0) atomicOr(&a.work[1], 2u);
             continue;
         }
-        const bool act0 = (((unsigned)e.y) >> lane) & 1u, act1 = (((unsigned)e.z) >> lane) & 1u;
-        const unsigned pm = (unsigned)__float_as_int(a.node_b[e.x].w);
+        const unsigned pm = (unsigned)__float_as_int(a.node_b[node].w);
         const int first = (int)(pm & kMetaIndex);
         const int nch = (int)((pm >> 28) & 7u) + 1;
         // structural guard: children come after the parent, inside the table
-        if ((pm & kMetaLeafBit) || first <= e.x || first + nch > a.num_nodes) {
+        if ((pm & kMetaLeafBit) || first <= node || first + nch > a.num_nodes) {
             if (lane == 0) atomicOr(&a.work[1], 2u);
             continue;
         }
@@ -327,25 +362,33 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
                 na2 = a.node_a[first + j + 1];
                 nb2 = a.node_b[first + j + 1];
             }
-            child(first + j, na, nb, act0, act1, sp);
+            child(first + j, na, nb, act, sp);
             na = na2;
             nb = nb2;
         }
     }
-    if (valid0) {
-        a.out[qi0] = (PREC == 0) ? s0 : __fadd_rn(s0, c0);
-        if (a.per_query_terms) a.per_query_terms[qi0] = n0;
+    int total = 0;
+#pragma unroll
+    for (int u = 0; u < NQ; ++u) {
+        if (valid[u]) {
+            a.out[qi[u]] = (PREC == 0) ? sum[u] : __fadd_rn(sum[u], cmp[u]);
+            if (a.per_query_terms) a.per_query_terms[qi[u]] = nt[u];
+        }
+        total += nt[u];
     }
-    if (valid1) {
-        a.out[qi1] = (PREC == 0) ? s1 : __fadd_rn(s1, c1);
-        if (a.per_query_terms) a.per_query_terms[qi1] = n1;
-    }
-    return n0 + n1;
+    return total;
+}
+
+template <bool GRID>
+__host__ __device__ constexpr int nq_of() {
+    return GRID ? kNqGrid : 1;
 }
 
 template <bool GRID, bool SCREENED, int PREC, int SHAPE>
-__global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn(GwnArgs a) {
-    __shared__ int4 stack[kGwnWarps][kGwnStack];
+__global__ void __launch_bounds__(kGwnWarps * 32, (GRID && kNqGrid >= 4) ? 2 : 3) k_gwn(GwnArgs a) {
+    constexpr int NQ = nq_of<GRID>();
+    __shared__ int stk_node[kGwnWarps][kGwnStack];
+    __shared__ unsigned stk_mask[kGwnWarps][kGwnStack * NQ];
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
@@ -357,7 +400,8 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn(GwnArgs a) {
         if (lane == 0) g = atomicAdd(&a.work[0], 1u);
         g = __shfl_sync(FULL, g, 0);
         if ((long long)g >= a.ngroups) break;
-        my_terms += (unsigned long long)gwn_group<GRID, SCREENED, PREC, SHAPE>(a, g, lane, stack[w], sigma, sigma_l2e);
+        my_terms += (unsigned long long)gwn_group<GRID, SCREENED, PREC, SHAPE, NQ>(a, g, lane, stk_node[w], stk_mask[w],
+                                                                                  sigma, sigma_l2e);
     }
     if (a.terms_total) {
         for (int o = 16; o > 0; o >>= 1) my_terms += __shfl_down_sync(FULL, my_terms, o);
@@ -369,10 +413,11 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn(GwnArgs a) {
 // clouds form one work list (prefix[c] = first group of cloud c), taken in
 // order by the warps of the grid, so that small clouds do not idle the GPU.
 template <bool SCREENED, int PREC, int SHAPE>
-__global__ void __launch_bounds__(kGwnWarps * 32, 3)
+__global__ void __launch_bounds__(kGwnWarps * 32, kNqGrid >= 4 ? 2 : 3)
     k_gwn_batch(const GwnArgs* __restrict__ table, const unsigned long long* __restrict__ prefix, int nclouds,
                 unsigned long long* __restrict__ work) {
-    __shared__ int4 stack[kGwnWarps][kGwnStack];
+    __shared__ int stk_node[kGwnWarps][kGwnStack];
+    __shared__ unsigned stk_mask[kGwnWarps][kGwnStack * kNqGrid];
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
@@ -390,8 +435,8 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3)
         }
         const GwnArgs& a = table[lo];
         const float sigma = a.sigma_dev ? *a.sigma_dev : a.sigma;
-        int nt = gwn_group<true, SCREENED, PREC, SHAPE>(a, g - prefix[lo], lane, stack[w], sigma,
-                                                       sigma * 1.4426950408889634f);
+        int nt = gwn_group<true, SCREENED, PREC, SHAPE, kNqGrid>(a, g - prefix[lo], lane, stk_node[w], stk_mask[w],
+                                                                sigma, sigma * 1.4426950408889634f);
         if (a.terms_total) {
             for (int o = 16; o > 0; o >>= 1) nt += __shfl_down_sync(FULL, nt, o);
             if (lane == 0 && nt) atomicAdd(a.terms_total, (unsigned long long)nt);
@@ -494,7 +539,7 @@ int gwn_eval(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, float*
     brick_extent(p.tile, ex, ey, ez);
     a.bx = (q.res[0] + ex - 1) / ex;
     a.by = (q.res[1] + ey - 1) / ey;
-    a.ngroups = (long long)a.bx * a.by * ((q.res[2] + 2 * ez - 1) / (2 * ez));  // two bricks in z per warp
+    a.ngroups = (long long)a.bx * a.by * ((q.res[2] + kNqGrid * ez - 1) / (kNqGrid * ez));  // bricks stacked in z
     DWG_REQUIRE(a.ngroups < (1ll << 32), "gwn: grid too large");
     return dispatch<true>(a, p, s);
 }
@@ -525,7 +570,7 @@ static void fill_args(GwnArgs& a, const Octree& t, const GwnBatchItem& it, const
     brick_extent(p.tile, ex, ey, ez);
     a.bx = (a.rx + ex - 1) / ex;
     a.by = (a.ry + ey - 1) / ey;
-    a.ngroups = (long long)a.bx * a.by * ((a.rz + 2 * ez - 1) / (2 * ez));
+    a.ngroups = (long long)a.bx * a.by * ((a.rz + kNqGrid * ez - 1) / (kNqGrid * ez));
     a.out = it.out;
     a.terms_total = it.terms_total;
     a.per_query_terms = nullptr;
