@@ -212,6 +212,9 @@ struct KnnArgs {
     int* __restrict__ q_key;
     int* __restrict__ q_hist;
     int morton_shift;
+    // per-cell bound of the 16th-neighbour distance (null: none), seeds the
+    // per-thread search of queries with k <= 16
+    const float* __restrict__ kb;
     // occupancy pyramid
     const unsigned char* __restrict__ occ;
     int levels;
@@ -441,7 +444,17 @@ __global__ void __launch_bounds__(128) k_knn_thread(KnnArgs a) {
         const int cy = cell_coord(qy, a.g.lo1, a.g.inv_h, a.g.G1);
         const int cz = cell_coord(qz, a.g.lo2, a.g.inv_h, a.g.G2);
         TopK<KMAX> top;
-        top.init(k);
+        if (a.kb && k <= kKnnBoundK) {
+            // start from k copies of the key of the bound kb[c] + |q - x_c|
+            // on the 16th distance: everything beyond it is pruned at once
+            const float ex = qx - (a.g.lo0 + ((float)cx + 0.5f) * h), ey = qy - (a.g.lo1 + ((float)cy + 0.5f) * h),
+                        ez = qz - (a.g.lo2 + ((float)cz + 0.5f) * h);
+            const float rq = (a.kb[cx + a.g.G0 * (cy + a.g.G1 * cz)] + sqrtf(ex * ex + ey * ey + ez * ez) * 1.00002f) *
+                                 1.00002f + 1e-7f;
+            top.init_bound(k, ((unsigned long long)__float_as_uint(rq * rq * 1.00002f) << 32) | 0xffffffffull);
+        } else {
+            top.init(k);
+        }
         for (int r = 0;; ++r) {
             const float kd2 = top.mx == NONE ? INFINITY : __uint_as_float((unsigned)(top.mx >> 32)) * 1.00001f;
             for (int dz = -r; dz <= r; ++dz) {
@@ -739,18 +752,19 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
         bool ok = isfinite(R);
         int* cur = nodes[w][0];
         int nf = 0;
-        int l = 0;  // the level the frontier starts at
+        int l = 0;   // the level the frontier starts at
+        int fl = 0;  // the level it ends at (cells are streamed from there)
         if (ok) {
             const float R2 = R * R;
             // the ball's box in cells
             const int x0 = cell_coord(x - R, a.g.lo0, a.g.inv_h, a.g.G0), x1 = cell_coord(x + R, a.g.lo0, a.g.inv_h, a.g.G0);
             const int y0 = cell_coord(y - R, a.g.lo1, a.g.inv_h, a.g.G1), y1 = cell_coord(y + R, a.g.lo1, a.g.inv_h, a.g.G1);
             const int z0 = cell_coord(z - R, a.g.lo2, a.g.inv_h, a.g.G2), z1 = cell_coord(z + R, a.g.lo2, a.g.inv_h, a.g.G2);
-            // coarsest-enough level: at most 2048 nodes cover the box
+            // coarsest-enough level: the nodes covering the box fit the frontier
             for (;;) {
                 const long long nn = (long long)((x1 >> l) - (x0 >> l) + 1) * ((y1 >> l) - (y0 >> l) + 1) *
                                      ((z1 >> l) - (z0 >> l) + 1);
-                if (nn <= 2048 || l >= a.levels) break;
+                if (nn <= kCqNodes || l >= a.levels) break;
                 ++l;
             }
             const int bx = (x1 >> l) - (x0 >> l) + 1, by = (y1 >> l) - (y0 >> l) + 1, bz = (z1 >> l) - (z0 >> l) + 1;
@@ -772,7 +786,10 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
                 nf += __popc(bal);
             }
             ok = nf <= kCqNodes;
-            // stage B: down to level 1 (the cells are expanded while streaming)
+            // stage B: down to level 1 (the cells are expanded while
+            // streaming); when the next level would not fit, the frontier
+            // stays at the coarser level and its nodes' cells are streamed
+            fl = l;
             for (int lv = l; lv >= 2 && ok; --lv) {
                 __syncwarp();
                 const int* D = a.ldim[lv];
@@ -793,14 +810,19 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
                     if (keep && pos < kCqNodes) nxt[pos] = id;
                     nn += __popc(bal);
                 }
-                ok = nn <= kCqNodes;
+                if (nn > kCqNodes) break;  // keep the level-lv frontier
                 int* tmp = cur;
                 cur = nxt;
                 nxt = tmp;
                 nf = nn;
+                fl = lv - 1;
             }
             __syncwarp();
         }
+        // a ball so large that the frontier stayed coarse, for a handful of
+        // queries: the per-thread search, seeded with each query's own bound,
+        // prunes it faster than the warp streams it
+        if (ok && fl >= 2 && qn < 8) ok = false;
         if (!ok) {  // the per-thread search takes this cell's queries
             for (int t = lane; t < qn; t += 32) fb[atomicAdd(&work[1], 1)] = order[qs + t];
             continue;
@@ -837,21 +859,26 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
                 __syncwarp();
                 staged = 0;
             };
-            // frontier entries are cells (level 0) or level-1 nodes of up to 8 cells
-            const int per = l >= 1 ? 8 : 1;
-            for (int b = 0; b < nf * per; b += 32) {
-                const int t = b + lane;
+            // frontier entries are cells (level 0) or nodes of level fl,
+            // cubes of side 2^fl cells
+            const int side = 1 << fl;
+            const long long per = (long long)side * side * side;
+            const long long total = (long long)nf * per;
+            for (long long b = 0; b < total; b += 32) {
+                const long long t = b + lane;
                 int s0 = 0, cnt = 0;
-                if (t < nf * per) {
+                if (t < total) {
                     int cell;
                     bool hit = true;
-                    if (per == 1) {
+                    if (fl == 0) {
                         cell = cur[t];
                     } else {
-                        const int* D = a.ldim[1];
-                        const int node = cur[t >> 3], oc = t & 7;
+                        const int* D = a.ldim[fl];
+                        const int node = cur[t / per];
+                        const int o = (int)(t % per);
                         const int ni = node % D[0], nj = (node / D[0]) % D[1], nk = node / (D[0] * D[1]);
-                        const int ui = 2 * ni + (oc & 1), uj = 2 * nj + ((oc >> 1) & 1), uk = 2 * nk + (oc >> 2);
+                        const int ui = ni * side + o % side, uj = nj * side + (o / side) % side,
+                                  uk = nk * side + o / (side * side);
                         hit = cq_node_hit(a, 0, ui, uj, uk, x, y, z, R2, eps);
                         cell = ui + a.g.G0 * (uj + a.g.G1 * uk);
                     }
@@ -953,6 +980,7 @@ static int knn_query_cells(const KnnIndex& ix, const KnnArgs& a0, long long nq, 
     KnnArgs f = a;
     f.order = ix.c_fb.ptr;
     f.nq_dev_i32 = ix.c_misc.ptr + 2;
+    f.kb = ix.kb.ptr;
     return knn_launch<16>(f, nq, s);
 }
 
@@ -1049,6 +1077,7 @@ int knn_query(const KnnIndex& ix, const KnnQuery& q, int k, int* out, cudaStream
         for (int t = 0; t < 3; ++t) a.ldim[l][t] = ix.ldim[l][t];
     }
     a.order = nullptr;
+    a.kb = nullptr;
     if (k <= kKnnBoundK && !q.exclude && ix.n >= kKnnBoundK && q.use_cells) return knn_query_cells(ix, a, q.nq, s);
     // bucket the queries spatially (counting sort on device counts, no host sync)
     DWG_TRY(ix.q_key.reserve(q.nq));

@@ -7,6 +7,7 @@
 // in which the atomics land (the reference adds FP32 atomics,
 // src/TurboDWG.cu:199-201, whose sum depends on scheduling).
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include "normals.cuh"
 #include "octree.cuh"
@@ -125,7 +126,7 @@ int zero_repair(const KnnIndex& ix, const float* pos, int L, float* N, const uns
     DWG_TRY(ws.list.reserve(L));
     DWG_TRY(ws.count.reserve(1));
     DWG_TRY(ws.nb.reserve((size_t)L * k));
-    cub::CountingInputIterator<int> it(0);
+    thrust::counting_iterator<int> it(0);
     size_t bytes = 0;
     int* lp = ws.list.ptr;
     int* cp = ws.count.ptr;

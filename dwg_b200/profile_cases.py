@@ -1,7 +1,7 @@
 """Small, self-contained workloads for profiler captures of the hot kernels,
 and a summariser of a profiler launch list.
 
-    python -m dwg_b200.profile_cases step     [--points N --grid R --iters T --reps K]
+    python -m dwg_b200.profile_cases step     [--points N --grid R --iters T --reps K --shape torus|sq_union]
     python -m dwg_b200.profile_cases gwn_grid [--points N --grid R --launches K]
     python -m dwg_b200.profile_cases knn_tri  [--points N --grid R --launches K]
     python -m dwg_b200.profile_cases mc       [--points N --grid R --launches K]
@@ -29,9 +29,15 @@ import time
 import numpy as np
 
 
+_SHAPE = "torus"
+
+
 def _cloud(n, seed=1000):
     from . import datasets as D
-    P, _ = D.torus(n, seed=seed)
+    if _SHAPE == "sq_union":  # 12 superquadrics + 1 % outliers
+        P, _ = D.superquadric_union(int(round(n / 1.01)), seed=seed)
+    else:
+        P, _ = D.torus(n, seed=seed)
     Pn, _, _ = D.normalize(P)
     return Pn.astype(np.float32)
 
@@ -40,13 +46,15 @@ def case_step(a):
     import torch
     from . import capi
     lib = capi.load()
-    Pd = torch.from_numpy(_cloud(a.points)).cuda()
+    P = _cloud(a.points)
+    Pd = torch.from_numpy(P).cuda()
     prm = capi.default_params(grid_reso=a.grid, final_reso=a.grid, total_iter=a.iters)
+    n = len(P)
     for rep in range(a.reps):
         h = C.c_void_p()
         torch.cuda.synchronize()
         t = [time.perf_counter()]
-        capi.check(lib.dwg_pipeline_create(capi.ptr(Pd), None, a.points, C.byref(prm), None, C.byref(h)))
+        capi.check(lib.dwg_pipeline_create(capi.ptr(Pd), None, n, C.byref(prm), None, C.byref(h)))
         torch.cuda.synchronize()
         t.append(time.perf_counter())
         capi.check(lib.dwg_pipeline_iterate(h, a.iters))
@@ -172,7 +180,10 @@ def main(argv=None):
     ap.add_argument("--iters", type=int, default=30)
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--launches", type=int, default=2)
+    ap.add_argument("--shape", choices=["torus", "sq_union"], default="torus")
     a = ap.parse_args(argv)
+    global _SHAPE
+    _SHAPE = a.shape
     if a.case == "summarize":
         print(summarize(a.path))
         return
