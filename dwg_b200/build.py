@@ -29,6 +29,10 @@ NVCC_FLAGS = ARCH + [
     "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "-I" + os.path.join(ROOT, "include"),
 ]
 
+# per-file additions: the PCA normals and point areas evaluate the oracle's
+# FP64 sequence operation by operation, so nothing is fused into an FMA
+FILE_FLAGS = {"areas.cu": ["-fmad=false"]}
+
 
 def nvcc() -> str:
     for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
@@ -67,7 +71,7 @@ def build(force: bool = False, jobs: int = 0, verbose: bool = False) -> str:
 
     def compile_one(so):
         s, o = so
-        cmd = [nv] + NVCC_FLAGS + ["-c", s, "-o", o]
+        cmd = [nv] + NVCC_FLAGS + FILE_FLAGS.get(os.path.basename(s), []) + ["-c", s, "-o", o]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -39,7 +39,7 @@ class Params(C.Structure):
         ("offset_1", C.c_float), ("offset_2", C.c_float), ("use_leaves_generate", C.c_int),
         ("total_iter", C.c_int), ("beta", C.c_float), ("area", C.c_float), ("screen", C.c_float),
         ("knn_tri", C.c_int), ("knn_zero", C.c_int), ("precision", C.c_int), ("use_graph", C.c_int),
-        ("tile", C.c_int), ("as_thres", C.c_float),
+        ("tile", C.c_int), ("as_thres", C.c_float), ("com_as", C.c_int),
     ]
 
 
@@ -79,6 +79,8 @@ _SIGS = {
     "dwg_zero_repair": (_i, [_vp, _vp, _vp, _vp, _i, _i, _vp]),
     "dwg_load_normals": (_i, [_vp, _i, _ll, _vp, _vp, _vp]),
     "dwg_radii": (_i, [_vp, _i, _vp, _i, _vp, _vp]),
+    "dwg_pca_normals": (_i, [_vp, _i, _vp, _i, _vp, _vp, _vp]),
+    "dwg_point_areas": (_i, [_vp, _i, _vp, _i, _vp, _vp, _vp]),
     "dwg_params_default": (None, [C.POINTER(Params)]),
     "dwg_pipeline_create": (_i, [_vp, _vp, _i, C.POINTER(Params), _vp, C.POINTER(_vp)]),
     "dwg_pipeline_destroy": (_i, [_vp]),

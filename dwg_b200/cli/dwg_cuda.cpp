@@ -7,7 +7,8 @@
 // <grid_reso>_iter_<total_iter>.stl (--output_mode 1, default) and .xyz with
 // normals (2), or both (3).  Extra flags: --seed (random normals of
 // --in_normal 0), --precision (0 FP32, 1 FP32 compensated, 2 accurate terms),
-// --use_graph (0/1).  --com_As 1 (CGAL point areas) is not supported.
+// --use_graph (0/1).  --com_As 1 computes PCA normals and point areas on the
+// GPU (the reference's PCL NormalEstimation and CGAL point_areas).
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -27,7 +28,7 @@ static void help() {
         {"--in_name", "The file name of the input point cloud (only supports .xyz currently)"},
         {"--out_path", "The absolute path of the output mesh/point cloud with normals"},
         {"--output_mode", "Output mode: 1 Mesh(.stl) (default)   2 Point cloud with normals(.xyz)   3 Both 1 and 2"},
-        {"--in_normal", "Initialization mode: 0 Random   1 Input   3 Gauss map (default)"},
+        {"--in_normal", "Initialization mode: 0 Random   1 Input   2 Random leaves (--com_As 1)   3 Gauss map (default)"},
         {"--lambda", "Screening Coefficient"},
         {"--max_depth", "The max depth of octree"},
         {"--use_radii", "Turn on screening mode or not (0 turn off   1 turn on)"},
@@ -37,7 +38,7 @@ static void help() {
         {"--final_reso", "The resolution of Marching Cubes for the final output"},
         {"--total_iter", "The number of iteration"},
         {"--test_iter", "Output the result each [test_iter] iterations (off by default)"},
-        {"--com_As", "Computing area weight or not (only 0 is supported)"},
+        {"--com_As", "Computing area weight or not (0 or 1)"},
         {"--use_leaves_generate", "Mesh from the octree leaves (0 turn off   1 turn on)"},
         {"--seed", "Seed of the random initial normals (--in_normal 0)"},
         {"--precision", "0 FP32, 1 FP32 compensated (default), 2 accurate terms"},
@@ -74,7 +75,7 @@ int main(int argc, char** argv) {
         else if (k == "--output_mode") output_mode = std::atoi(v);
         else if (k == "--use_leaves_generate") prm.use_leaves_generate = std::atoi(v);
         else if (k == "--use_radii") prm.use_radii = std::atoi(v);
-        else if (k == "--com_As") com_As = std::atoi(v);
+        else if (k == "--com_As") com_As = prm.com_as = std::atoi(v);
         else if (k == "--As_thres") prm.as_thres = (float)std::atof(v);
         else if (k == "--offset_1") prm.offset_1 = (float)std::atof(v);
         else if (k == "--offset_2") prm.offset_2 = (float)std::atof(v);
@@ -87,8 +88,8 @@ int main(int argc, char** argv) {
             return 2;
         }
     }
-    if (com_As != 0) {
-        fprintf(stderr, "--com_As 1 (CGAL point areas) is not supported by this build\n");
+    if (com_As != 0 && com_As != 1) {
+        fprintf(stderr, "--com_As should be 0 or 1\n");  // include/DWGProcess.h:801-806
         return 2;
     }
     if (test_iter != 999999) fprintf(stderr, "note: --test_iter intermediate meshes are not written\n");
@@ -101,7 +102,7 @@ int main(int argc, char** argv) {
         int n = 0;
         dwg::check(dwg_read_xyz(full.c_str(), 1, &P, &N, &n));
         std::vector<float> normals(N, N + (size_t)n * 3);
-        if (prm.in_normal == 0) {
+        if (prm.in_normal == 0 || (prm.in_normal == 2 && !prm.com_as)) {
             // GetRandomNs (include/DWGProcess.h:264-281), seeded
             std::mt19937_64 gen(seed);
             std::uniform_real_distribution<double> dis(0.0, 2.0 * M_PI);

@@ -377,6 +377,24 @@ int dwg_radii(const float* points_dev, int n, const int* knn_dev, int k, float* 
     API_GUARD(return radii(points_dev, n, knn_dev, k, radii_dev, S(stream));)
 }
 
+int dwg_pca_normals(const float* points_dev, int n, const int* knn_dev, int k, const float* view_host,
+                    float* normals_dev, void* stream) {
+    API_GUARD({
+        DWG_REQUIRE(view_host, "pca_normals: null viewpoint");
+        DevBuf<float> view;
+        DWG_TRY(view.reserve(3));
+        DWG_CHECK_CUDA(cudaMemcpyAsync(view.ptr, view_host, sizeof(float) * 3, cudaMemcpyHostToDevice, S(stream)));
+        DWG_TRY(pca_normals(points_dev, n, knn_dev, k, view.ptr, normals_dev, S(stream)));
+        DWG_CHECK_CUDA(cudaStreamSynchronize(S(stream)));
+        return DWG_OK;
+    })
+}
+
+int dwg_point_areas(const float* points_dev, int n, const int* knn_dev, int k, const float* normals_dev,
+                    float* areas_dev, void* stream) {
+    API_GUARD(return point_areas(points_dev, n, knn_dev, k, normals_dev, areas_dev, S(stream));)
+}
+
 void dwg_params_default(dwg_params* p) {
     if (!p) return;
     p->in_normal = 3;
@@ -402,6 +420,7 @@ void dwg_params_default(dwg_params* p) {
     p->use_graph = 1;
     p->tile = 0;
     p->as_thres = 0.f;
+    p->com_as = 0;
 }
 
 int dwg_pipeline_create(const float* points_dev, const float* normals_dev, int n, const dwg_params* params,

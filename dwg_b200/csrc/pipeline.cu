@@ -20,6 +20,9 @@
 
 namespace dwg {
 
+constexpr int kPcaK = 10;   // ne.setKSearch(10), include/DWGProcess.h:178
+constexpr int kAreaK = 15;  // point_areas neighbourhoods, include/DWGProcess.h:232,357
+
 // Closed form of igl::voxel_grid(V, offset, s, 1) (deps/libigl/include/igl/voxel_grid.cpp:11-87)
 // in single precision; samples at origin + index * spacing.
 int voxel_grid_host(const float* P, int n, float offset, int s_res, cudaStream_t st, int res[3], float origin[3],
@@ -294,9 +297,12 @@ int Pipeline::setup(const float* points_dev, const float* normals_dev, int n_poi
     DWG_REQUIRE(p.knn_tri >= 1 && p.knn_tri <= 64 && p.knn_zero >= 1 && p.knn_zero <= 64 && p.kw >= 1 &&
                     p.kw <= 64 && p.final_kw >= 1 && p.final_kw <= 64 && p.normal_kw >= 1 && p.normal_kw <= 64,
                 "pipeline: k values must be in [1, 64]");
-    DWG_REQUIRE(p.in_normal == 0 || p.in_normal == 1 || p.in_normal == 3 || p.in_normal == 4,
-                "pipeline: in_normal must be 0, 1, 3 or 4");
-    DWG_REQUIRE(p.in_normal >= 3 || normals_dev, "pipeline: in_normal %d needs input normals", p.in_normal);
+    DWG_REQUIRE(p.in_normal >= 0 && p.in_normal <= 4, "pipeline: in_normal must be in [0, 4]");
+    DWG_REQUIRE(p.com_as == 0 || p.com_as == 1, "pipeline: com_as must be 0 or 1");
+    // --com_As 1 replaces the input normals by PCA normals unless in_normal is 1
+    // (include/DWGProcess.h:152-200, :494-495)
+    const bool pca = p.com_as && p.in_normal != 1;
+    DWG_REQUIRE(p.in_normal >= 3 || pca || normals_dev, "pipeline: in_normal %d needs input normals", p.in_normal);
     DWG_REQUIRE(p.in_normal != 4 || init_mlp, "pipeline: in_normal 4 needs a learned initialiser");
     prm = p;
     caller = stream;
@@ -310,9 +316,27 @@ int Pipeline::setup(const float* points_dev, const float* normals_dev, int n_poi
     DWG_TRY(area_pts.reserve(n));
     k_fill<<<div_up(n, 256), 256, 0, s>>>(area_pts.ptr, n, p.area);
     DWG_CHECK_LAUNCH();
-    if (normals_dev) {
+    if (normals_dev && !pca) {
         DWG_TRY(Nin.reserve((size_t)n * 3));
         DWG_CHECK_CUDA(cudaMemcpyAsync(Nin.ptr, normals_dev, sizeof(float) * 3 * n, cudaMemcpyDeviceToDevice, s));
+    }
+    if (pca) {
+        // NormalEstimation, 10 nearest points, viewpoint at the box centre
+        DWG_TRY(Nin.reserve((size_t)n * 3));
+        const int kp = n < kPcaK ? n : kPcaK;
+        KnnIndex pix;
+        DWG_TRY(knn_build(pix, P.ptr, n, s));
+        DevBuf<int> nb;
+        DWG_TRY(nb.reserve((size_t)n * kp));
+        KnnQuery q;
+        q.q = P.ptr;
+        q.nq = n;
+        DWG_TRY(knn_query(pix, q, kp, nb.ptr, s));
+        DevBuf<float> box;
+        DWG_TRY(box.reserve(9));
+        DWG_TRY(box_centre(P.ptr, n, box.ptr, box.ptr + 6, s));
+        DWG_TRY(pca_normals(P.ptr, n, nb.ptr, kp, box.ptr + 6, Nin.ptr, s));
+        DWG_CHECK_CUDA(cudaStreamSynchronize(s));
     }
     // octree on the points (include/DWGProcess.h:227)
     DWG_TRY(octree_build(t1, P.ptr, n, p.max_depth, area_pts.ptr, s));
@@ -334,13 +358,9 @@ int Pipeline::setup(const float* points_dev, const float* normals_dev, int n_poi
     k_gather_xyz<<<div_up(L, 256), 256, 0, s>>>(raw_pos.ptr, t2.perm.ptr, L, leaf_pos.ptr);
     k_fill<<<div_up(L, 256), 256, 0, s>>>(leaf_rad.ptr, L, p.screen);
     DWG_CHECK_LAUNCH();
-    if (p.as_thres > 0.f) {
-        // OutlierFilter on the leaves' areas (src/TurboDWG.cu:512), canonical order
-        DWG_TRY(outlier_filter(leaf_area.ptr, L, p.as_thres, s));
-        k_set_area<<<div_up(L, 256), 256, 0, s>>>(t2.pa.ptr, leaf_area.ptr, L);
-        DWG_CHECK_LAUNCH();
-    }
-    if (p.in_normal < 3) {
+    // leaf normals smoothed from the point normals: the start of in_normal
+    // 0-2, and the normals of the --com_As areas
+    if (p.in_normal < 3 || p.com_as) {
         DWG_TRY(octree_set_point_data(t1, Nin.ptr, nullptr, nullptr, s));
         DevBuf<double> sm, part;
         DWG_TRY(sm.reserve((size_t)L * 3));
@@ -365,6 +385,30 @@ int Pipeline::setup(const float* points_dev, const float* normals_dev, int n_poi
         DWG_TRY(radii(leaf_pos.ptr, L, nb.ptr, p.kw, leaf_rad.ptr, s));
         DWG_CHECK_CUDA(cudaStreamSynchronize(s));
     }
+    if (p.com_as) {
+        // leaf areas from the 15 nearest leaves (GetRadiiandAs,
+        // include/DWGProcess.h:345-378), before the moments (:680)
+        const int ka = L < kAreaK ? L : kAreaK;
+        DevBuf<int> nb;
+        DWG_TRY(nb.reserve((size_t)L * ka));
+        KnnQuery q;
+        q.q = leaf_pos.ptr;
+        q.nq = L;
+        DWG_TRY(knn_query(kidx, q, ka, nb.ptr, s));
+        DWG_TRY(point_areas(leaf_pos.ptr, L, nb.ptr, ka, leaf_nrm.ptr, leaf_area.ptr, s));
+        k_set_area<<<div_up(L, 256), 256, 0, s>>>(t2.pa.ptr, leaf_area.ptr, L);
+        DWG_CHECK_LAUNCH();
+        DWG_TRY(octree_update_centres(t2, s));
+        DWG_CHECK_CUDA(cudaStreamSynchronize(s));
+    }
+    if (p.as_thres > 0.f) {
+        // OutlierFilter on the leaves' areas (src/TurboDWG.cu:512), canonical
+        // order; the centres of mass keep the unfiltered areas
+        DWG_TRY(outlier_filter(leaf_area.ptr, L, p.as_thres, s));
+        k_set_area<<<div_up(L, 256), 256, 0, s>>>(t2.pa.ptr, leaf_area.ptr, L);
+        DWG_CHECK_LAUNCH();
+    }
+    if (p.in_normal == 2 && p.com_as) DWG_TRY(random_normals(leaf_nrm.ptr, L, s));
     // iteration grid around the points (include/DWGProcess.h:672)
     DWG_TRY(voxel_grid_host(P.ptr, n, p.offset_1, p.grid_reso, s, gres, gorg, &gh));
     if (p.in_normal == 3) DWG_TRY(gauss_map(leaf_pos.ptr, L, leaf_nrm.ptr, s));
@@ -553,9 +597,25 @@ int Pipeline::finalize() {
         DWG_TRY(pt_rad.reserve(n));
         k_fill<<<div_up(n, 256), 256, 0, s>>>(pt_rad.ptr, n, prm.screen);
         DWG_CHECK_LAUNCH();
+        KnnIndex pix;
+        if (prm.use_radii || prm.com_as) DWG_TRY(knn_build(pix, P.ptr, n, s));
+        if (prm.com_as) {
+            // point areas from the 15 nearest points and the loaded normals
+            // (include/DWGProcess.h:783-792), then the moments with these
+            // areas (UpdateGWNInfo, src/TurboDWG.cu:931)
+            const int ka = n < kAreaK ? n : kAreaK;
+            DevBuf<int> nb;
+            DWG_TRY(nb.reserve((size_t)n * ka));
+            KnnQuery q2;
+            q2.q = P.ptr;
+            q2.nq = n;
+            DWG_TRY(knn_query(pix, q2, ka, nb.ptr, s));
+            DWG_TRY(point_areas(P.ptr, n, nb.ptr, ka, point_nrm.ptr, area_pts.ptr, s));
+            DWG_TRY(octree_set_point_data(t1, nullptr, area_pts.ptr, nullptr, s));
+            DWG_TRY(octree_update_centres(t1, s));
+            DWG_CHECK_CUDA(cudaStreamSynchronize(s));
+        }
         if (prm.use_radii) {
-            KnnIndex pix;
-            DWG_TRY(knn_build(pix, P.ptr, n, s));
             DevBuf<int> nb;
             DWG_TRY(nb.reserve((size_t)n * prm.final_kw));
             KnnQuery q2;
@@ -565,9 +625,10 @@ int Pipeline::finalize() {
             DWG_TRY(radii(P.ptr, n, nb.ptr, prm.final_kw, pt_rad.ptr, s));
             DWG_CHECK_CUDA(cudaStreamSynchronize(s));
         }
-        // OutlierFilter on the points' areas (src/TurboDWG.cu:876), input order
+        // OutlierFilter on the points' areas (src/TurboDWG.cu:876, :935), input order
         if (prm.as_thres > 0.f) DWG_TRY(outlier_filter(area_pts.ptr, n, prm.as_thres, s));
-        DWG_TRY(octree_set_point_data(t1, point_nrm.ptr, prm.as_thres > 0.f ? area_pts.ptr : nullptr, pt_rad.ptr, s));
+        DWG_TRY(octree_set_point_data(t1, point_nrm.ptr, prm.as_thres > 0.f || prm.com_as ? area_pts.ptr : nullptr,
+                                      pt_rad.ptr, s));
         DWG_TRY(p_sorted.reserve((size_t)n * 3));
         k_sorted_xyz<<<div_up(n, 256), 256, 0, s>>>(t1.pa.ptr, n, p_sorted.ptr);
         DWG_CHECK_LAUNCH();

@@ -1,6 +1,7 @@
 // pipeline.cuh -- the DWG reconstruction driver on one GPU.
 #pragma once
 
+#include "areas.cuh"
 #include "gwn.cuh"
 #include "knn.cuh"
 #include "mc.cuh"

@@ -240,6 +240,31 @@ def voxel_grid(points, offset, s):
     return res, org, np.float32(h.value)
 
 
+def pca_normals(points, knn, view):
+    """PCA normals of the --com_As 1 mode (pcl::NormalEstimation with
+    setKSearch(10), include/DWGProcess.h:152-200): knn rows hold each point's
+    nearest points, self included; normals face ``view`` (3 floats)."""
+    _req_cuda_f32(points, "points", 3)
+    knn = knn.contiguous()
+    v = np.ascontiguousarray(np.asarray(view, np.float32).reshape(3))
+    out = torch.empty_like(points)
+    capi.check(capi.load().dwg_pca_normals(capi.ptr(points), points.shape[0], capi.ptr(knn), knn.shape[1],
+                                           v.ctypes.data, capi.ptr(out), capi.stream_ptr()))
+    return out
+
+
+def point_areas(points, knn, normals):
+    """igl::copyleft::cgal::point_areas (include/DWGProcess.h:345-378): the
+    area of every point from its knn row (self first, <= 32 columns)."""
+    _req_cuda_f32(points, "points", 3)
+    _req_cuda_f32(normals, "normals", 3)
+    knn = knn.contiguous()
+    out = torch.empty(points.shape[0], dtype=torch.float32, device=points.device)
+    capi.check(capi.load().dwg_point_areas(capi.ptr(points), points.shape[0], capi.ptr(knn), knn.shape[1],
+                                           capi.ptr(normals), capi.ptr(out), capi.stream_ptr()))
+    return out
+
+
 class TurboDWG:
     """The DWG iteration + meshing driver (src/TurboDWG.cu:456-989), as one
     GPU pipeline: ``TurboDWG(points, normals=None, **flags)``, then

@@ -214,14 +214,34 @@ int dwg_radii(const float* points_dev, int n, const int* knn_dev, int k, float* 
               void* stream);
 
 /* ------------------------------------------------------------------------
+ * --com_As 1 inputs: normals and areas from the points themselves.
+ * ------------------------------------------------------------------------ */
+/* PCA normals: the eigenvector of the smallest eigenvalue of the covariance
+ * of the k nearest points (knn_dev rows, self included), flipped so that
+ * (view - p) . n >= 0.  view_host: 3 floats in host memory.  Replaces
+ * pcl::NormalEstimation with setKSearch(10) and the bounding-box centre as
+ * viewpoint (include/DWGProcess.h:152-200). */
+int dwg_pca_normals(const float* points_dev, int n, const int* knn_dev, int k, const float* view_host,
+                    float* normals_dev, void* stream);
+/* Point areas: for point i, the neighbours of its knn_dev row (self first,
+ * k <= 32) whose normal has a positive dot product with n_i are projected
+ * on their PCA plane; the share of point i of every Delaunay triangle of
+ * that 2-D set around it (half, quarter or Voronoi share by the obtuse
+ * rules) is summed; 0 when fewer than 3 neighbours are kept.  Replaces
+ * igl::copyleft::cgal::point_areas (include/DWGProcess.h:345-378,789-790;
+ * deps/libigl/include/igl/copyleft/cgal/point_areas.cpp:39-210). */
+int dwg_point_areas(const float* points_dev, int n, const int* knn_dev, int k, const float* normals_dev,
+                    float* areas_dev, void* stream);
+
+/* ------------------------------------------------------------------------
  * Full reconstruction (TurboIterative + TurboDWG::TurboScreenedDWGLaunch +
  * TurboDWG::GenerateMesh, include/DWGProcess.h:474-797,
  * src/TurboDWG.cu:456-924).  Parameters mirror the DWG_CUDA flags
  * (src/main.cpp:19-39).
  * ------------------------------------------------------------------------ */
 typedef struct {
-    int in_normal;          /* 0 random, 1 input, 3 Gauss map (default),
-                               4 learned (dwg_pipeline_create_learned) */
+    int in_normal;          /* 0 random, 1 input, 2 random leaf normals (com_as 1), 3 Gauss map
+                               (default), 4 learned (dwg_pipeline_create_learned) */
     int grid_reso;          /* --grid_reso (400) */
     int final_reso;         /* --final_reso (500) */
     int kw, final_kw, normal_kw; /* 10, 10, 10 */
@@ -241,6 +261,9 @@ typedef struct {
     int use_graph;          /* capture one iteration in a CUDA graph and replay it */
     int tile;               /* dwg_gwn_params.tile of the grid sums */
     float as_thres;         /* --As_thres (0): the ceil(n * as_thres) largest areas are divided by 1000 */
+    int com_as;             /* --com_As (0): 1 = areas by dwg_point_areas (leaves, then points in the
+                               final pass) and, unless in_normal is 1, PCA normals (k = 10) as the
+                               input normals; in_normal 2 then starts from random leaf normals */
 } dwg_params;
 
 void dwg_params_default(dwg_params* p);

@@ -984,6 +984,241 @@ void dwgo_radii(const float* P, int n, const int* knn, int k, float* radii) {
     }
 }
 
+/* ---- --com_As 1: PCA normals, point areas, seeded random leaf normals ---- */
+
+/* eigen decomposition of a symmetric 3x3 matrix by cyclic Jacobi rotations
+ * (each rotation zeroes its pivot exactly); w ascending, V[:, i] the unit
+ * eigenvector of w[i].  Only +, -, *, / and sqrt, each rounded once, in a
+ * fixed order: the GPU evaluates the same sequence and gets the same bits. */
+static void jacobi3(const double A_in[3][3], double w[3], double V[3][3]) {
+    double a[3][3];
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            a[i][j] = A_in[i][j];
+            V[i][j] = i == j ? 1.0 : 0.0;
+        }
+    for (int sweep = 0; sweep < 32; sweep++) {
+        const double off = a[0][1] * a[0][1] + a[0][2] * a[0][2] + a[1][2] * a[1][2];
+        const double dg = a[0][0] * a[0][0] + a[1][1] * a[1][1] + a[2][2] * a[2][2];
+        if (off <= 1e-36 * dg) break;
+        for (int p = 0; p < 2; p++)
+            for (int q = p + 1; q < 3; q++) {
+                if (a[p][q] == 0.0) continue;
+                const double theta = (a[q][q] - a[p][p]) / (2.0 * a[p][q]);
+                const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                const double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+                for (int k = 0; k < 3; k++) { /* columns p, q */
+                    const double akp = a[k][p], akq = a[k][q];
+                    a[k][p] = c * akp - s * akq;
+                    a[k][q] = s * akp + c * akq;
+                }
+                for (int k = 0; k < 3; k++) { /* rows p, q */
+                    const double apk = a[p][k], aqk = a[q][k];
+                    a[p][k] = c * apk - s * aqk;
+                    a[q][k] = s * apk + c * aqk;
+                }
+                a[p][q] = 0.0;
+                a[q][p] = 0.0;
+                for (int k = 0; k < 3; k++) {
+                    const double vkp = V[k][p], vkq = V[k][q];
+                    V[k][p] = c * vkp - s * vkq;
+                    V[k][q] = s * vkp + c * vkq;
+                }
+            }
+    }
+    /* ascending eigenvalues, ties in index order */
+    int ord[3] = {0, 1, 2};
+    for (int i = 0; i < 3; i++)
+        for (int j = i + 1; j < 3; j++)
+            if (a[ord[j]][ord[j]] < a[ord[i]][ord[i]]) {
+                const int t = ord[i];
+                ord[i] = ord[j];
+                ord[j] = t;
+            }
+    double Vs[3][3];
+    for (int i = 0; i < 3; i++) {
+        w[i] = a[ord[i]][ord[i]];
+        for (int k = 0; k < 3; k++) Vs[k][i] = V[k][ord[i]];
+    }
+    memcpy(V, Vs, sizeof(Vs));
+}
+
+/* mean c and covariance C (divided by m) of the points ids[0..m) */
+static void covariance(const float* P, const int* ids, int m, double c[3], double C[3][3]) {
+    c[0] = c[1] = c[2] = 0;
+    for (int j = 0; j < m; j++)
+        for (int d = 0; d < 3; d++) c[d] += (double)P[(size_t)ids[j] * 3 + d];
+    for (int d = 0; d < 3; d++) c[d] /= m;
+    memset(C, 0, sizeof(double) * 9);
+    for (int j = 0; j < m; j++) {
+        double e[3];
+        for (int d = 0; d < 3; d++) e[d] = (double)P[(size_t)ids[j] * 3 + d] - c[d];
+        for (int r = 0; r < 3; r++)
+            for (int q = 0; q < 3; q++) C[r][q] += e[r] * e[q];
+    }
+    for (int r = 0; r < 3; r++)
+        for (int q = 0; q < 3; q++) C[r][q] /= m;
+}
+
+void dwgo_pca_normals(const float* P, int n, const int* knn, int k, const float view[3], float* normals) {
+    int* ids = xmalloc((size_t)k * sizeof(int));
+    for (int i = 0; i < n; i++) {
+        int m = 0;
+        for (int j = 0; j < k; j++)
+            if (knn[(size_t)i * k + j] >= 0) ids[m++] = knn[(size_t)i * k + j];
+        double nv[3] = {0, 0, 1};
+        if (m >= 3) {
+            double c[3], C[3][3], w[3], V[3][3];
+            covariance(P, ids, m, c, C);
+            jacobi3(C, w, V);
+            for (int d = 0; d < 3; d++) nv[d] = V[d][0];
+        }
+        /* flipNormalTowardsViewpoint: (view - p) . n >= 0 */
+        double dp = 0;
+        for (int d = 0; d < 3; d++) dp += ((double)view[d] - (double)P[(size_t)i * 3 + d]) * nv[d];
+        const double sg = dp < 0 ? -1.0 : 1.0;
+        for (int d = 0; d < 3; d++) normals[(size_t)i * 3 + d] = (float)(sg * nv[d]);
+    }
+    free(ids);
+}
+
+/* exact orientation of integer points (|coordinates| < 2^24): > 0 counter-clockwise */
+static long long orient_q(long long ax, long long ay, long long bx, long long by, long long cx, long long cy) {
+    return (bx - ax) * (cy - ay) - (by - ay) * (cx - ax);
+}
+
+/* exact in-circle determinant sign of d against the circle through a, b, c
+ * (> 0: d inside when a, b, c are counter-clockwise), 128-bit integers */
+static int incircle_q(long long ax, long long ay, long long bx, long long by, long long cx, long long cy,
+                      long long dx, long long dy) {
+    const __int128 adx = ax - dx, ady = ay - dy, bdx = bx - dx, bdy = by - dy, cdx = cx - dx, cdy = cy - dy;
+    const __int128 det = (adx * adx + ady * ady) * (bdx * cdy - cdx * bdy) -
+                         (bdx * bdx + bdy * bdy) * (adx * cdy - cdx * ady) +
+                         (cdx * cdx + cdy * cdy) * (adx * bdy - bdx * ady);
+    return det > 0 ? 1 : (det < 0 ? -1 : 0);
+}
+
+void dwgo_point_areas(const float* P, int n, const int* knn, int k, const float* normals, float* areas) {
+    int* ids = xmalloc((size_t)k * sizeof(int));
+    double* u = xmalloc((size_t)k * sizeof(double));
+    double* v = xmalloc((size_t)k * sizeof(double));
+    long long* qx = xmalloc((size_t)k * sizeof(long long));
+    long long* qy = xmalloc((size_t)k * sizeof(long long));
+    int* keep = xmalloc((size_t)k * sizeof(int));
+    for (int i = 0; i < n; i++) {
+        const int q0 = knn[(size_t)i * k];
+        areas[i] = 0.f;
+        if (q0 < 0) continue;
+        /* neighbours whose normal agrees with the first one's (point_areas.cpp:97-106) */
+        int m = 0;
+        for (int j = 0; j < k; j++) {
+            const int q = knn[(size_t)i * k + j];
+            if (q < 0) continue;
+            double d = 0;
+            for (int t = 0; t < 3; t++) d += (double)normals[(size_t)q0 * 3 + t] * (double)normals[(size_t)q * 3 + t];
+            if (d > 0) ids[m++] = q;
+        }
+        if (m <= 2) continue;
+        /* PCA plane (point_areas.cpp:114-133): scores on the two largest
+         * principal directions */
+        double c[3], C[3][3], w[3], V[3][3];
+        covariance(P, ids, m, c, C);
+        jacobi3(C, w, V);
+        double mx = 0;
+        for (int j = 0; j < m; j++) {
+            double e[3];
+            for (int d = 0; d < 3; d++) e[d] = (double)P[(size_t)ids[j] * 3 + d] - c[d];
+            u[j] = e[0] * V[0][2] + e[1] * V[1][2] + e[2] * V[2][2];
+            v[j] = e[0] * V[0][1] + e[1] * V[1][1] + e[2] * V[2][1];
+            if (fabs(u[j]) > mx) mx = fabs(u[j]);
+            if (fabs(v[j]) > mx) mx = fabs(v[j]);
+        }
+        if (!(mx > 0) || !isfinite(mx)) continue;
+        /* the 2-D Delaunay triangulation decided exactly on coordinates
+         * rounded to a grid of 2^-24 of the extent; coincident points after
+         * rounding are one vertex (the first) */
+        const double scale = ldexp(1.0, 23 - ilogb(mx));
+        int mk = 0;
+        for (int j = 0; j < m; j++) {
+            const long long x = llrint(u[j] * scale), y = llrint(v[j] * scale);
+            int dup = 0;
+            for (int t = 0; t < mk && !dup; t++) dup = qx[t] == x && qy[t] == y;
+            if (dup) continue;
+            qx[mk] = x;
+            qy[mk] = y;
+            keep[mk++] = j;
+        }
+        double acc = 0;
+        for (int b = 1; b < mk; b++)
+            for (int cc = b + 1; cc < mk; cc++) {
+                const long long orient = orient_q(qx[0], qy[0], qx[b], qy[b], qx[cc], qy[cc]);
+                if (orient == 0) continue; /* collinear: no face */
+                /* Delaunay: no point strictly inside the circumcircle; points
+                 * on it form a cocircular polygon, triangulated as the fan
+                 * from the point itself (its neighbours on the polygon are
+                 * adjacent: no cocircular point beyond the chord b-c) */
+                int ok = 1;
+                for (int t = 1; t < mk && ok; t++) {
+                    if (t == b || t == cc) continue;
+                    int sg = incircle_q(qx[0], qy[0], qx[b], qy[b], qx[cc], qy[cc], qx[t], qy[t]);
+                    if (orient < 0) sg = -sg;
+                    if (sg > 0) ok = 0;
+                    if (sg == 0) {
+                        const long long side = orient_q(qx[b], qy[b], qx[cc], qy[cc], qx[t], qy[t]);
+                        if ((side > 0) != (orient > 0) && side != 0) ok = 0;
+                    }
+                }
+                if (!ok) continue;
+                /* triangle XYZ with X the point itself (point_areas.cpp:160-193) */
+                const int jb = keep[b], jc = keep[cc];
+                const double ax = u[0], ay = v[0], bx = u[jb], by = v[jb], cx = u[jc], cy = v[jc];
+                const double x = sqrt((bx - cx) * (bx - cx) + (by - cy) * (by - cy));
+                const double y = sqrt((ax - cx) * (ax - cx) + (ay - cy) * (ay - cy));
+                const double z = sqrt((bx - ax) * (bx - ax) + (by - ay) * (by - ay));
+                const double cosX = (z * z + y * y - x * x) / (2 * y * z);
+                const double cosY = (z * z + x * x - y * y) / (2 * x * z);
+                const double cosZ = (x * x + y * y - z * z) / (2 * y * x);
+                double b0 = x * cosX, b1 = y * cosY, b2 = z * cosZ;
+                const double bs = b0 + b1 + b2;
+                b0 /= bs;
+                b1 /= bs;
+                b2 /= bs;
+                const double full = 0.25 * sqrt((x + (y + z)) * (z - (x - y)) * (z + (x - y)) * (x + (y - z)));
+                if (cosX < 0)
+                    acc += 0.5 * full;
+                else if (cosY < 0 || cosZ < 0)
+                    acc += 0.25 * full;
+                else
+                    acc += (b1 * full + b2 * full) / 2;
+            }
+        areas[i] = isfinite(acc) ? (float)acc : 0.f;
+    }
+    free(ids);
+    free(u);
+    free(v);
+    free(qx);
+    free(qy);
+    free(keep);
+}
+
+/* splitmix64 (S. Vigna) of an index: integer mixing, identical on the GPU */
+static uint64_t mix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+void dwgo_random_normals(int n, float* normals) {
+    for (int i = 0; i < n; i++) {
+        const double u = (double)(mix64((uint64_t)i * 2) >> 11) * (1.0 / 9007199254740992.0) * 6.283185307179586;
+        const double v = (double)(mix64((uint64_t)i * 2 + 1) >> 11) * (1.0 / 9007199254740992.0) * 6.283185307179586;
+        normals[(size_t)i * 3] = (float)(sin(u) * cos(v));
+        normals[(size_t)i * 3 + 1] = (float)(sin(u) * sin(v));
+        normals[(size_t)i * 3 + 2] = (float)cos(u);
+    }
+}
+
 /* ------------------------------------------------------------------------ */
 /* full reconstruction                                                        */
 /* ------------------------------------------------------------------------ */
@@ -1092,7 +1327,28 @@ dwgo_run* dwgo_reconstruct(const float* P, int n, const float* N_in,
     for (int i = 0; i < L; i++)
         for (int d = 0; d < 3; d++) lpos0[(size_t)i * 3 + d] = (float)t1->centers[(size_t)lnode[i] * 3 + d];
     float* lnrm0 = xcalloc((size_t)L * 3, sizeof(float));
-    if (prm->in_normal != 3 && N_in) {
+    /* --com_As 1: PCA normals (10 nearest, viewpoint at the box centre)
+     * replace the input unless in_normal is 1 (include/DWGProcess.h:152-200) */
+    float* Npca = NULL;
+    if (prm->com_as && prm->in_normal != 1) {
+        const int kp = n < 10 ? n : 10;
+        int* nb = xmalloc((size_t)n * kp * sizeof(int));
+        dwgo_knn(P, n, P, n, kp, nthreads, nb);
+        float lo[3], hi[3], view[3];
+        for (int d = 0; d < 3; d++) lo[d] = hi[d] = P[d];
+        for (int i = 1; i < n; i++)
+            for (int d = 0; d < 3; d++) {
+                const float x = P[(size_t)i * 3 + d];
+                if (x < lo[d]) lo[d] = x;
+                if (x > hi[d]) hi[d] = x;
+            }
+        for (int d = 0; d < 3; d++) view[d] = (hi[d] + lo[d]) / 2.0f;
+        Npca = xmalloc((size_t)n * 3 * sizeof(float));
+        dwgo_pca_normals(P, n, nb, kp, view, Npca);
+        free(nb);
+        N_in = Npca;
+    }
+    if ((prm->in_normal != 3 || prm->com_as) && N_in) {
         /* SmoothNormalstoOctreeLeaves (include/DWGProcess.h:430-472), then
          * the whole-matrix normalisation of :537 */
         double* acc = xcalloc((size_t)L * 3, sizeof(double));
@@ -1133,7 +1389,15 @@ dwgo_run* dwgo_reconstruct(const float* P, int n, const float* N_in,
     free(Ld);
     float* lA = xmalloc((size_t)L * sizeof(float));
     for (int i = 0; i < L; i++) lA[i] = prm->area;
-    dwgo_outlier_filter(lA, L, prm->as_thres); /* src/TurboDWG.cu:512 */
+    if (prm->com_as) {
+        /* leaf areas from the 15 nearest leaves and the smoothed normals
+         * (GetRadiiandAs, include/DWGProcess.h:345-378) */
+        const int ka = L < 15 ? L : 15;
+        int* nb = xmalloc((size_t)L * ka * sizeof(int));
+        dwgo_knn(lpos, L, lpos, L, ka, nthreads, nb);
+        dwgo_point_areas(lpos, L, nb, ka, lnrm, lA);
+        free(nb);
+    }
     float* lrad = xmalloc((size_t)L * sizeof(float));
     if (prm->use_radii) {
         int* nb = xmalloc((size_t)L * prm->kw * sizeof(int));
@@ -1150,6 +1414,11 @@ dwgo_run* dwgo_reconstruct(const float* P, int n, const float* N_in,
     double* CM2 = xmalloc((size_t)t2->n_nodes * 3 * sizeof(double));
     double* R2 = xmalloc((size_t)t2->n_nodes * sizeof(double));
     dwgo_moments(t2, lpos, lnrm, lA, CM2, R2, NULL);
+    /* OutlierFilter runs on the GPU copy of the areas (src/TurboDWG.cu:512):
+     * the centres of mass and radii keep the areas of the host precompute,
+     * the per-iteration sums of A n use the filtered ones */
+    dwgo_outlier_filter(lA, L, prm->as_thres);
+    if (prm->in_normal == 2 && prm->com_as) dwgo_random_normals(L, lnrm); /* include/DWGProcess.h:643-657 */
     if (prm->in_normal == 3) dwgo_gauss_map(lpos, L, lnrm);
 
     run->iters = prm->total_iter;
@@ -1213,7 +1482,16 @@ dwgo_run* dwgo_reconstruct(const float* P, int n, const float* N_in,
         free(nb);
         float* pA = xmalloc((size_t)n * sizeof(float));
         for (int i = 0; i < n; i++) pA[i] = prm->area;
-        dwgo_outlier_filter(pA, n, prm->as_thres); /* src/TurboDWG.cu:876 */
+        if (prm->com_as) {
+            /* point areas from the 15 nearest points and the loaded normals
+             * (include/DWGProcess.h:783-792); the moments below use them
+             * (UpdateGWNInfo, src/TurboDWG.cu:931) */
+            const int ka = n < 15 ? n : 15;
+            int* nb3 = xmalloc((size_t)n * ka * sizeof(int));
+            dwgo_knn(P, n, P, n, ka, nthreads, nb3);
+            dwgo_point_areas(P, n, nb3, ka, pn, pA);
+            free(nb3);
+        }
         float* prad = xmalloc((size_t)n * sizeof(float));
         if (prm->use_radii) {
             int* nb2 = xmalloc((size_t)n * prm->final_kw * sizeof(int));
@@ -1226,6 +1504,7 @@ dwgo_run* dwgo_reconstruct(const float* P, int n, const float* N_in,
         double* CM1 = xmalloc((size_t)t1->n_nodes * 3 * sizeof(double));
         double* R1 = xmalloc((size_t)t1->n_nodes * sizeof(double));
         dwgo_moments(t1, P, pn, pA, CM1, R1, NULL);
+        dwgo_outlier_filter(pA, n, prm->as_thres); /* src/TurboDWG.cu:876, :935, as above */
         run->final_field = xmalloc((size_t)ng2 * sizeof(float));
         double mean;
         field_pass(t1, P, n, pn, pA, prad, CM1, R1, prm, prm->lambda, run->fres, org2, h2, nthreads,
@@ -1257,6 +1536,7 @@ dwgo_run* dwgo_reconstruct(const float* P, int n, const float* N_in,
     free(perm);
     free(queue);
     free(lnode);
+    free(Npca);
     free(Pd);
     dwgo_octree_free(t1);
     dwgo_octree_free(t2);

@@ -86,9 +86,24 @@ void dwgo_load_normals(const int* knn, int k, long long nq,
                        const float* leaf_normals, float* out);
 void dwgo_radii(const float* P, int n, const int* knn, int k, float* radii);
 
+/* NormalEstimation (include/DWGProcess.h:152-200, PCL): the eigenvector of
+ * the smallest eigenvalue of the covariance of the k neighbours (knn, self
+ * included), flipped towards `view`; eigenvectors by cyclic Jacobi
+ * rotations in FP64 */
+void dwgo_pca_normals(const float* P, int n, const int* knn, int k, const float view[3], float* normals);
+/* igl::copyleft::cgal::point_areas (deps/libigl/include/igl/copyleft/cgal/
+ * point_areas.cpp:39-210) with the 2-D Delaunay triangulation restated by
+ * its definition (a triangle is Delaunay when no other point lies inside
+ * its circumcircle); knn rows start with the point itself */
+void dwgo_point_areas(const float* P, int n, const int* knn, int k, const float* normals, float* areas);
+/* seeded stand-in for the reference's unseeded random leaf normals of the
+ * --com_As 1 --in_normal 2 start (include/DWGProcess.h:643-657) */
+void dwgo_random_normals(int n, float* normals);
+
 /* ---- full reconstruction (include/DWGProcess.h:474-797 + src/TurboDWG.cu:456-924) ---- */
 typedef struct {
-    int in_normal;       /* 0 random(seeded, given as input), 1 input, 3 Gauss map */
+    int in_normal;       /* 0 random(seeded, given as input), 1 input, 2 random leaves
+                            (com_as 1), 3 Gauss map */
     int grid_reso, final_reso, kw, final_kw, normal_kw, max_depth;
     float lambda;        /* --lambda (sigma) */
     int min_num, use_radii;
@@ -98,6 +113,7 @@ typedef struct {
     int knn_tri;         /* 15 */
     int knn_zero;        /* 10 */
     float as_thres;      /* --As_thres (0) */
+    int com_as;          /* --com_As (0) */
 } dwgo_params;
 
 /* OutlierFilter + AsFiltertoZero (src/TurboDWG.cu:991-1009, :442-454): the

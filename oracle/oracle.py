@@ -40,7 +40,7 @@ class Params(C.Structure):
         ("offset_1", C.c_float), ("offset_2", C.c_float),
         ("use_leaves_generate", C.c_int), ("total_iter", C.c_int),
         ("beta", C.c_float), ("area", C.c_float), ("screen", C.c_float),
-        ("knn_tri", C.c_int), ("knn_zero", C.c_int), ("as_thres", C.c_float),
+        ("knn_tri", C.c_int), ("knn_zero", C.c_int), ("as_thres", C.c_float), ("com_as", C.c_int),
     ]
 
 
@@ -81,6 +81,9 @@ def lib():
     L.dwgo_load_normals.argtypes = [_i32p, C.c_int, C.c_longlong, _f32p, _f32p]
     L.dwgo_radii.argtypes = [_f32p, C.c_int, _i32p, C.c_int, _f32p]
     L.dwgo_outlier_filter.argtypes = [_f32p, C.c_int, C.c_float]
+    L.dwgo_pca_normals.argtypes = [_f32p, C.c_int, _i32p, C.c_int, _f32p, _f32p]
+    L.dwgo_point_areas.argtypes = [_f32p, C.c_int, _i32p, C.c_int, _f32p, _f32p]
+    L.dwgo_random_normals.argtypes = [C.c_int, _f32p]
     L.dwgo_reconstruct.restype = vp
     L.dwgo_reconstruct.argtypes = [_f32p, C.c_int, vp, C.POINTER(Params), C.c_int]
     L.dwgo_run_free.argtypes = [vp]
@@ -294,10 +297,39 @@ def radii(P, knn_idx):
     return out
 
 
+def pca_normals(P, knn_idx, view):
+    """NormalEstimation (include/DWGProcess.h:152-200): smallest principal
+    direction of each knn row, facing ``view``."""
+    P = _f32(P)
+    knn_idx = np.ascontiguousarray(knn_idx, np.int32)
+    out = np.empty((len(P), 3), np.float32)
+    lib().dwgo_pca_normals(P.reshape(-1), len(P), knn_idx.reshape(-1), knn_idx.shape[1],
+                           _f32(view).reshape(3), out.reshape(-1))
+    return out
+
+
+def point_areas(P, knn_idx, normals):
+    """igl::copyleft::cgal::point_areas (include/DWGProcess.h:345-378)."""
+    P = _f32(P)
+    knn_idx = np.ascontiguousarray(knn_idx, np.int32)
+    out = np.empty(len(P), np.float32)
+    lib().dwgo_point_areas(P.reshape(-1), len(P), knn_idx.reshape(-1), knn_idx.shape[1],
+                           _f32(normals).reshape(-1), out)
+    return out
+
+
+def random_normals(n):
+    """Seeded leaf normals of the --in_normal 2 --com_As 1 start."""
+    out = np.empty((n, 3), np.float32)
+    lib().dwgo_random_normals(int(n), out.reshape(-1))
+    return out
+
+
 DEFAULT_PARAMS = dict(in_normal=3, grid_reso=400, final_reso=500, kw=10, final_kw=10,
                       normal_kw=10, max_depth=10, lambda_=10.0, min_num=0, use_radii=0,
                       offset_1=0.05, offset_2=0.01, use_leaves_generate=0, total_iter=40,
-                      beta=2.3, area=2e-6, screen=0.0015, knn_tri=15, knn_zero=10, as_thres=0.0)
+                      beta=2.3, area=2e-6, screen=0.0015, knn_tri=15, knn_zero=10, as_thres=0.0,
+                      com_as=0)
 
 
 def reconstruct(P, normals=None, nthreads=None, **kw):

@@ -264,3 +264,36 @@ def test_voxel_grid_matches_oracle(oracle_lib):
         res, org, h = turbo.voxel_grid(cu(P), 0.05, s)
         r2, o2, h2 = oracle_lib.voxel_grid(P, 0.05, s)
         assert np.array_equal(res, r2) and np.array_equal(org, o2) and h == h2
+
+
+def _lattice_cloud(n=20000, cells=128, seed=6):
+    """octree-leaf-like input: a torus snapped to a lattice (many cocircular
+    neighbourhoods), duplicates removed"""
+    P, _ = cloud(n, kind="torus", seed=seed)
+    Q = np.unique(np.round(P * cells), axis=0) / cells
+    return Q.astype(np.float32)
+
+
+@pytest.mark.parametrize("kind", ["scattered", "lattice"])
+def test_pca_normals_and_point_areas_bit_exact(oracle_lib, kind):
+    # --com_As 1 inputs on the same neighbour rows: both sides run the same
+    # FP64 Jacobi sequence and exact Delaunay predicates
+    P = cloud(20000, kind="torus", seed=5)[0] if kind == "scattered" else _lattice_cloud()
+    P_d = cu(P)
+    nb10 = oracle_lib.knn(P, P, 10)
+    view = ((P.max(0) + P.min(0)) / np.float32(2)).astype(np.float32)
+    ref_n = oracle_lib.pca_normals(P, nb10, view)
+    got_n = turbo.pca_normals(P_d, cu(nb10), view)
+    torch.cuda.synchronize()
+    assert np.array_equal(got_n.cpu().numpy(), ref_n)
+    nb15 = oracle_lib.knn(P, P, 15)
+    ref_a = oracle_lib.point_areas(P, nb15, ref_n)
+    got_a = turbo.point_areas(P_d, cu(nb15), cu(ref_n))
+    torch.cuda.synchronize()
+    assert np.array_equal(got_a.cpu().numpy(), ref_a)
+    assert ref_a.min() >= 0 and np.mean(ref_a > 0) > 0.99
+    # the rows only need self first: a shorter k gives a finite answer too
+    got3 = turbo.point_areas(P_d, cu(nb15[:, :3].copy()), cu(ref_n))
+    assert torch.isfinite(got3).all()
+    with pytest.raises(capi.DwgError):
+        turbo.point_areas(cu(P[:2000]), cu(oracle_lib.knn(P[:2000], P[:2000], 33)), cu(ref_n[:2000]))

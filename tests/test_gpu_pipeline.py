@@ -99,3 +99,34 @@ def test_pipeline_outlier_filter_tracks_oracle(oracle_lib):
     # the filter changes the sums (30 % of the areas divided by 1000)
     assert not np.allclose(got["iso"], plain["iso"], rtol=1e-2)
     assert abs(got["final_iso"] - plain["final_iso"]) > 0.1 * abs(plain["final_iso"])
+
+
+@pytest.mark.parametrize("in_normal", [0, 2, 3])
+def test_pipeline_com_as_tracks_oracle(oracle_lib, in_normal):
+    # --com_As 1: PCA normals replace the input, leaf areas by point_areas
+    # before the moments, point areas again in the final pass; in_normal 2
+    # starts from the seeded random leaf normals
+    P, _ = D.torus(4000, seed=21)
+    Pn, _, _ = D.normalize(P)
+    cfg = dict(SMALL, total_iter=2, com_as=1, in_normal=in_normal)
+    ref = oracle_lib.reconstruct(Pn, **cfg)
+    got = turbo.reconstruct(cu(Pn), **cfg)
+    plain = turbo.reconstruct(cu(Pn), **dict(SMALL, total_iter=2, in_normal=3))
+    assert np.array_equal(got["leaf_pos"], ref["leaf_pos"])
+    # the areas are bit-identical; the sums differ by FP32-compensated vs FP64
+    # rounding (relative to the terms, so more where the mean cancels)
+    assert np.allclose(got["iso"], ref["iso"], rtol=2e-4, atol=1e-10)
+    assert np.all(np.abs(got["tri_count"] - ref["tri_count"]) <= 0.002 * ref["tri_count"] + 4)
+    assert np.allclose(got["final_iso"], ref["final_iso"], rtol=1e-3, atol=1e-10)
+    # the computed areas change the field (constant 2e-6 otherwise)
+    assert not np.allclose(got["iso"], plain["iso"], rtol=1e-2)
+
+
+def test_pipeline_com_as_random_start_matches_oracle(oracle_lib):
+    # with no iterations the leaf normals are the seeded random start itself
+    P, _ = D.sphere(3000, noise=0.002, seed=22)
+    Pn, _, _ = D.normalize(P)
+    cfg = dict(SMALL, total_iter=0, com_as=1, in_normal=2, use_leaves_generate=1)
+    got = turbo.reconstruct(cu(Pn), **cfg)
+    want = oracle_lib.random_normals(len(got["leaf_pos"]))
+    assert np.allclose(got["leaf_nrm"], want, atol=1e-7)

@@ -191,3 +191,51 @@ def test_oracle_outlier_filter_known_answer(oracle_lib):
     want[[4, 5, 1]] /= 1000.0
     assert np.array_equal(got, want)
     assert np.array_equal(oracle_lib.outlier_filter(A, 0.0), A)
+
+
+def _embed(xy, z=0.3, seed=0):
+    """planar 2-D points placed on a rotated plane in 3-D"""
+    rng = np.random.default_rng(seed)
+    q, _ = np.linalg.qr(rng.normal(size=(3, 3)))
+    P = np.c_[xy, np.full(len(xy), z)] @ q.T
+    return P.astype(np.float32), q[:, 2].astype(np.float32)
+
+
+def test_oracle_point_areas_known_answers(oracle_lib):
+    # centre of a regular hexagon of side 1: six equilateral Delaunay
+    # triangles, a third of each => sqrt(3)/2 (the hexagonal Voronoi cell)
+    ang = np.arange(6) * np.pi / 3
+    xy = np.r_[[[0.0, 0.0]], np.c_[np.cos(ang), np.sin(ang)]]
+    P, nrm = _embed(xy)
+    N = np.tile(nrm, (len(P), 1))
+    knn = np.arange(7, dtype=np.int32)[None, :]
+    a = oracle_lib.point_areas(P, np.repeat(knn, 7, 0), N)
+    assert abs(a[0] - np.sqrt(3) / 2) < 1e-5
+    # one triangle, obtuse at the point itself: half of its area (0.2 * 0.5)
+    P2, nrm2 = _embed(np.array([[0.0, 0.0], [-1.0, 0.2], [1.0, 0.2]]), seed=1)
+    N2 = np.tile(nrm2, (3, 1))
+    a2 = oracle_lib.point_areas(P2, np.array([[0, 1, 2]] * 3, np.int32), N2)
+    assert abs(a2[0] - 0.1) < 1e-6
+    # centre of a square lattice: every square around it is cocircular; one
+    # triangulation per square (not both diagonals) => the unit Voronoi cell
+    g = np.array([[x, y] for x in (-1.0, 0.0, 1.0) for y in (-1.0, 0.0, 1.0)])
+    g = np.r_[[[0.0, 0.0]], g[np.any(g != 0, axis=1)]]
+    P4, nrm4 = _embed(g, seed=4)
+    a4 = oracle_lib.point_areas(P4, np.arange(9, dtype=np.int32)[None, :].repeat(9, 0), np.tile(nrm4, (9, 1)))
+    assert abs(a4[0] - 1.0) < 1e-5
+    # a neighbour whose normal disagrees is dropped: 2 left -> area 0
+    N3 = N2.copy()
+    N3[2] *= -1
+    a3 = oracle_lib.point_areas(P2, np.array([[0, 1, 2]] * 3, np.int32), N3)
+    assert a3[0] == 0.0
+
+
+def test_oracle_pca_normals_face_the_viewpoint(oracle_lib):
+    rng = np.random.default_rng(3)
+    P, nrm = _embed(rng.uniform(-1, 1, (200, 2)), seed=2)
+    knn = oracle_lib.knn(P, P, 10)
+    centre = P.mean(0)
+    for s in (1.0, -1.0):
+        view = (centre + s * 5 * nrm).astype(np.float32)
+        N = oracle_lib.pca_normals(P, knn, view)
+        assert np.allclose(N, s * nrm[None, :], atol=1e-5)
