@@ -220,7 +220,8 @@ def run_ours(a, rank, world, local_rank):
     roof = gwn_roofline(a, lib, capi, turbo, torch, dev, P)
     extras = {}
     if rank == 0 and not a.no_extras:
-        for name, fn in (("precision", precision_report), ("learned", learned_report), ("batched", batched_report)):
+        for name, fn in (("precision", precision_report), ("farfield", farfield_report), ("learned", learned_report),
+                         ("batched", batched_report)):
             try:
                 extras[name] = fn(a, lib, capi, turbo, torch, dev)
             except Exception as e:  # a report must not take the headline line down
@@ -461,6 +462,60 @@ def precision_report(a, lib, capi, turbo, torch, dev):
 
     out["moments"] = {"nodes": int(len(idx)), "cm_max_rel": rel(g["cm"], CM[idx]), "radius_max_rel": rel(g["radius"], R[idx]),
                       "sum_An_max_rel": rel(g["ec"], EC[idx]), "note": "FP64 on the GPU and in the oracle"}
+    return out
+
+
+def farfield_report(a, lib, capi, turbo, torch, dev):
+    """Plain winding number with igl::fast_winding_number's far-field
+    expansions of orders 0, 1, 2 (beta 2, libigl's default) on the bench torus
+    with its true normals: device time of the whole iteration grid, pair terms,
+    and the error against the exact all-pairs sum (FP64 oracle) on a seeded
+    sample of grid points, beside the FP64 oracle's own Barnes-Hut error."""
+    import oracle
+    from dwg_b200 import datasets as D
+    P0, N0 = D.torus(a.points, R=1.0, r=0.35, noise=0.003, seed=1000)
+    P, _, sc = D.normalize(P0)
+    P = np.ascontiguousarray(P, np.float32)
+    N = np.ascontiguousarray(N0, np.float32)
+    A = np.full(len(P), 4 * np.pi ** 2 * 1.0 * 0.35 / sc ** 2 / len(P), np.float32)  # torus area / n
+    _, _, res, org = _pipeline_state(lib, capi, torch, dev, P, dict(grid_reso=a.grid, final_reso=a.grid,
+                                                                  total_iter=0), 0)
+    rng = np.random.default_rng(11)
+    ng = int(np.prod(res.astype(np.int64)))
+    sel = rng.choice(ng, min(4000, ng), replace=False)
+    idx = np.stack([sel % res[0], (sel // res[0]) % res[1], sel // (res[0] * res[1])], 1).astype(np.float32)
+    Q = (org[None, :3].astype(np.float32) + idx * np.float32(org[3])).astype(np.float32)
+    exact = oracle.gwn_exact(P, N, A, Q, screened=False)
+    ot = oracle.Octree(P, WORKLOAD["max_depth"])
+    Pd, Nd, Ad, Qd = (torch.from_numpy(x).to(dev) for x in (P, N, A, Q))
+    tree = turbo.TurboLibiGWN(Pd, max_depth=WORKLOAD["max_depth"], areas=Ad)
+    tree.UpdateMassNormals(Nd, Ad)
+    out = {"state": f"torus {a.points} points, true normals, uniform areas; grid {res.tolist()}; "
+                    f"error sample: {len(Q)} seeded grid points against the exact all-pairs sum",
+           "beta": 2.0, "field_rms": float(np.sqrt(np.mean(exact ** 2)))}
+    grid_out = torch.empty(ng, dtype=torch.float32, device=dev)
+    terms = torch.zeros(1, dtype=torch.int64, device=dev)
+    for order in (0, 1, 2):
+        w = tree.TurboLibiGWNLaunch(Qd, beta=2.0, order=order).cpu().numpy().astype(np.float64)
+        wo, _ = ot.fwn(P, N, A, Q, order, beta=2.0)
+        for _ in range(2):
+            tree.grid(res, org[:3], float(org[3]), beta=2.0, sigma=0.0, screened=False, order=order, out=grid_out)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        terms.zero_()
+        e0.record()
+        for _ in range(3):
+            tree.grid(res, org[:3], float(org[3]), beta=2.0, sigma=0.0, screened=False, order=order, out=grid_out,
+                      terms=terms)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        out[f"order{order}"] = {
+            "grid_ms": ms, "pair_terms": int(terms.item()) // 3,
+            "pair_terms_per_s": int(terms.item()) / 3 / (ms * 1e-3),
+            "gpu_err_vs_exact": {"rms": float(np.sqrt(np.mean((w - exact) ** 2))), "max": float(np.abs(w - exact).max())},
+            "oracle_fp64_err_vs_exact": {"rms": float(np.sqrt(np.mean((wo - exact) ** 2))),
+                                         "max": float(np.abs(wo - exact).max())}}
     return out
 
 

@@ -28,7 +28,8 @@ class DwgError(RuntimeError):
 
 class GwnParams(C.Structure):
     _fields_ = [("beta", C.c_float), ("sigma", C.c_float), ("screen", C.c_float),
-                ("screened", C.c_int), ("use_radii", C.c_int), ("precision", C.c_int), ("tile", C.c_int)]
+                ("screened", C.c_int), ("use_radii", C.c_int), ("precision", C.c_int), ("tile", C.c_int),
+                ("order", C.c_int)]
 
 
 class Params(C.Structure):
@@ -64,6 +65,7 @@ _SIGS = {
     "dwg_octree_update_info": (_i, [_vp, _vp, _vp, _vp]),
     "dwg_octree_status": (_i, [_vp, C.POINTER(C.c_uint)]),
     "dwg_octree_export": (_i, [_vp] * 9),
+    "dwg_octree_expansion": (_i, [_vp, _vp, _vp]),
     "dwg_gwn_points": (_i, [_vp, _vp, _vp, _vp, _vp, _ll, C.POINTER(GwnParams), _vp, _vp, _vp]),
     "dwg_gwn_points_counted": (_i, [_vp, _vp, _vp, _vp, _vp, _ll, C.POINTER(GwnParams), _vp, _vp, _vp]),
     "dwg_gwn_grid": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _f, C.POINTER(GwnParams), _vp, _vp, _vp]),
@@ -185,5 +187,5 @@ def default_params(**kw) -> Params:
 
 
 def gwn_params(beta=2.3, sigma=10.0, screen=0.0015, screened=True, use_radii=False, precision=1,
-               tile=0) -> GwnParams:
-    return GwnParams(beta, sigma, screen, int(screened), int(use_radii), int(precision), int(tile))
+               tile=0, order=0) -> GwnParams:
+    return GwnParams(beta, sigma, screen, int(screened), int(use_radii), int(precision), int(tile), int(order))

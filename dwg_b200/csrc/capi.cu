@@ -178,6 +178,18 @@ int dwg_octree_export(const dwg_octree* tree, int* depth, int* pt_start, int* pt
     })
 }
 
+int dwg_octree_expansion(dwg_octree* tree, double* out_host, void* stream) {
+    API_GUARD({
+        DWG_REQUIRE(tree && out_host, "octree_expansion: null argument");
+        Octree& t = tree->t;
+        DWG_TRY(octree_update_expansion(t, 2, S(stream)));
+        DWG_CHECK_CUDA(cudaMemcpyAsync(out_host, t.ho_d.ptr, sizeof(double) * 36 * t.M, cudaMemcpyDeviceToHost,
+                                       S(stream)));
+        DWG_CHECK_CUDA(cudaStreamSynchronize(S(stream)));
+        return DWG_OK;
+    })
+}
+
 static int gwn_common(dwg_octree* tree, const float* normals_dev, const float* areas_dev, const float* radii_dev,
                       const GwnQuery& q, const dwg_gwn_params* params, float* out_dev,
                       unsigned long long* terms_dev, int* per_query, void* stream) {

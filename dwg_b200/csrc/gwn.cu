@@ -136,6 +136,7 @@ struct GwnArgs {
     int* per_query_terms;
     unsigned int* work;  // [0] counter, [1] error flags (sticky)
     int num_nodes, num_points;
+    const float4* __restrict__ node_h;  // expansion records, 8 float4 each (plain sums, order >= 1)
 };
 
 template <bool SCREENED, int PREC>
@@ -169,6 +170,56 @@ __device__ __forceinline__ float gwn_term_masked(bool take, float r2, float d, f
     return v;
 }
 
+// Higher-order far field of the plain sum (igl::fast_winding_number
+// expansion_eval, deps/libigl/include/igl/fast_winding_number.cpp:187-241):
+// with loc = CM - q, r = |loc| and the node's coefficients m1 (9), m2 (27),
+//   order 1: sum_uv (delta_uv / (4 pi r^3) - 3 loc_u loc_v / (4 pi r^5)) m1[u + 3v]
+//          = tr(m1) / (4 pi r^3) - 3 loc^T m1 loc / (4 pi r^5)
+//   order 2: + sum_i sum_uv (15 loc_i loc_u loc_v / (4 pi r^7)
+//              - 3 (loc_i delta_uv + loc_v delta_ui + loc_u delta_vi) / (4 pi r^5)) m2[9i + u + 3v]
+//          = 15 sum_v loc_v sum_{i<=u} loc_i loc_u s(i,u,v) / (4 pi r^7) - 3 loc.g / (4 pi r^5)
+// on the node record's contraction (m1, tr m1, g, s; see octree.cuh); the
+// order-0 dipole is the usual term.
+template <int ORDER, int PREC>
+__device__ __forceinline__ float fwn_correction(float lx, float ly, float lz, float r2, const float4* __restrict__ H) {
+    const float r = (PREC >= 2) ? sqrtf(r2) : r2 * rsqrt_ftz(r2);
+    const float p3 = kFourPi * r * r * r;
+    const float p5 = p3 * r * r;
+    const float d = (PREC >= 2) ? __fdiv_rn(1.0f, p3) : rcp_ftz(p3);
+    const float c5 = (PREC >= 2) ? __fdiv_rn(-3.0f, p5) : -3.0f * rcp_ftz(p5);
+    float h[32];
+#pragma unroll
+    for (int t = 0; t < (ORDER >= 2 ? 8 : 3); ++t) {
+        const float4 c = H[t];
+        h[4 * t] = c.x;
+        h[4 * t + 1] = c.y;
+        h[4 * t + 2] = c.z;
+        h[4 * t + 3] = c.w;
+    }
+    // loc^T m1 loc
+    const float mx = fmaf(h[0], lx, fmaf(h[3], ly, h[6] * lz));
+    const float my = fmaf(h[1], lx, fmaf(h[4], ly, h[7] * lz));
+    const float mz = fmaf(h[2], lx, fmaf(h[5], ly, h[8] * lz));
+    const float q1 = fmaf(lx, mx, fmaf(ly, my, lz * mz));
+    float w = fmaf(d, h[9], c5 * q1);
+    if (ORDER >= 2) {
+        const float p7 = p5 * r * r;
+        const float i15 = (PREC >= 2) ? __fdiv_rn(15.0f, p7) : 15.0f * rcp_ftz(p7);
+        const float l00 = lx * lx, l01 = lx * ly, l02 = lx * lz, l11 = ly * ly, l12 = ly * lz, l22 = lz * lz;
+        float cub = 0.f;
+        const float lv[3] = {lx, ly, lz};
+#pragma unroll
+        for (int v = 0; v < 3; ++v) {
+            const float* sv = h + 13 + 6 * v;
+            const float t = fmaf(l00, sv[0], fmaf(l01, sv[1], fmaf(l02, sv[2], fmaf(l11, sv[3], fmaf(l12, sv[4], l22 * sv[5])))));
+            cub = fmaf(lv[v], t, cub);
+        }
+        const float lg = fmaf(lx, h[10], fmaf(ly, h[11], lz * h[12]));
+        w = fmaf(i15, cub, fmaf(c5, lg, w));
+    }
+    return w;
+}
+
 // Queries per lane: grids take NQ_GRID samples per lane (the brick of SHAPE
 // stacked NQ_GRID times in z), point queries one (consecutive points spread
 // over more of the tree than grid bricks, which costs more than it shares).
@@ -187,7 +238,7 @@ constexpr int kNqGrid = DWG_NQ_GRID;
 // lane's queries never split the warp; each query's terms keep their
 // depth-first order (its value does not depend on NQ or the brick shape).
 // Returns the lane's term count.
-template <bool GRID, bool SCREENED, int PREC, int SHAPE, int NQ>
+template <bool GRID, bool SCREENED, int PREC, int SHAPE, int NQ, int ORDER>
 __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g, int lane,
                                          int* __restrict__ stk_node, unsigned* __restrict__ stk_mask, float sigma,
                                          float sigma_l2e) {
@@ -291,7 +342,13 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
             for (int u = 0; u < NQ; ++u) {
                 const float dd = fmaf(dx[u], nb.x, fmaf(dy[u], nb.y, dz[u] * nb.z));
                 bool k;
-                const float v = gwn_term_masked<SCREENED, PREC>(take[u], d2[u], dd, a.screen, sigma, sigma_l2e, k);
+                float v = gwn_term_masked<SCREENED, PREC>(take[u], d2[u], dd, a.screen, sigma, sigma_l2e, k);
+                if (ORDER > 0 && !SCREENED && !leaf) {
+                    // far internal node: add the expansion terms (leaves are exact)
+                    const float c = fwn_correction<ORDER, PREC>(dx[u], dy[u], dz[u], take[u] ? d2[u] : 1.0f,
+                                                                a.node_h + (size_t)cidx * 8);
+                    v += take[u] ? c : 0.f;
+                }
                 if (k) acc_add<PREC>(sum[u], cmp[u], v);
                 nt[u] += (int)k;
             }
@@ -384,7 +441,7 @@ __host__ __device__ constexpr int nq_of() {
     return GRID ? kNqGrid : 1;
 }
 
-template <bool GRID, bool SCREENED, int PREC, int SHAPE>
+template <bool GRID, bool SCREENED, int PREC, int SHAPE, int ORDER>
 __global__ void __launch_bounds__(kGwnWarps * 32, (GRID && kNqGrid >= 4) ? 2 : 3) k_gwn(GwnArgs a) {
     constexpr int NQ = nq_of<GRID>();
     __shared__ int stk_node[kGwnWarps][kGwnStack];
@@ -400,7 +457,7 @@ __global__ void __launch_bounds__(kGwnWarps * 32, (GRID && kNqGrid >= 4) ? 2 : 3
         if (lane == 0) g = atomicAdd(&a.work[0], 1u);
         g = __shfl_sync(FULL, g, 0);
         if ((long long)g >= a.ngroups) break;
-        my_terms += (unsigned long long)gwn_group<GRID, SCREENED, PREC, SHAPE, NQ>(a, g, lane, stk_node[w], stk_mask[w],
+        my_terms += (unsigned long long)gwn_group<GRID, SCREENED, PREC, SHAPE, NQ, ORDER>(a, g, lane, stk_node[w], stk_mask[w],
                                                                                   sigma, sigma_l2e);
     }
     if (a.terms_total) {
@@ -435,7 +492,7 @@ __global__ void __launch_bounds__(kGwnWarps * 32, kNqGrid >= 4 ? 2 : 3)
         }
         const GwnArgs& a = table[lo];
         const float sigma = a.sigma_dev ? *a.sigma_dev : a.sigma;
-        int nt = gwn_group<true, SCREENED, PREC, SHAPE, kNqGrid>(a, g - prefix[lo], lane, stk_node[w], stk_mask[w],
+        int nt = gwn_group<true, SCREENED, PREC, SHAPE, kNqGrid, 0>(a, g - prefix[lo], lane, stk_node[w], stk_mask[w],
                                                                 sigma, sigma * 1.4426950408889634f);
         if (a.terms_total) {
             for (int o = 16; o > 0; o >>= 1) nt += __shfl_down_sync(FULL, nt, o);
@@ -451,40 +508,47 @@ static int blocks_for(K kernel) {
     return bps > 0 ? bps : 1;
 }
 
-template <bool GRID, bool SCREENED, int PREC, int SHAPE>
+template <bool GRID, bool SCREENED, int PREC, int SHAPE, int ORDER>
 static int launch(const GwnArgs& a, cudaStream_t s) {
     static int blocks_per_sm = 0;
-    if (!blocks_per_sm) blocks_per_sm = blocks_for(k_gwn<GRID, SCREENED, PREC, SHAPE>);
+    if (!blocks_per_sm) blocks_per_sm = blocks_for(k_gwn<GRID, SCREENED, PREC, SHAPE, ORDER>);
     long long want = (a.ngroups + kGwnWarps - 1) / kGwnWarps;
     long long grid = (long long)num_sms() * blocks_per_sm;
     if (want < grid) grid = want > 0 ? want : 1;
-    k_gwn<GRID, SCREENED, PREC, SHAPE><<<(unsigned)grid, kGwnWarps * 32, 0, s>>>(a);
+    k_gwn<GRID, SCREENED, PREC, SHAPE, ORDER><<<(unsigned)grid, kGwnWarps * 32, 0, s>>>(a);
     DWG_CHECK_LAUNCH();
     return DWG_OK;
 }
 
-template <bool GRID, bool SCREENED, int PREC>
+template <bool GRID, bool SCREENED, int PREC, int ORDER>
 static int launch_shape(const GwnArgs& a, int shape, cudaStream_t s) {
-    if (!GRID) return launch<GRID, SCREENED, PREC, 0>(a, s);
+    if (!GRID) return launch<GRID, SCREENED, PREC, 0, ORDER>(a, s);
     switch (shape) {
-        case 1: return launch<GRID, SCREENED, PREC, 1>(a, s);
-        case 2: return launch<GRID, SCREENED, PREC, 2>(a, s);
-        case 3: return launch<GRID, SCREENED, PREC, 3>(a, s);
-        default: return launch<GRID, SCREENED, PREC, 0>(a, s);
+        case 1: return launch<GRID, SCREENED, PREC, 1, ORDER>(a, s);
+        case 2: return launch<GRID, SCREENED, PREC, 2, ORDER>(a, s);
+        case 3: return launch<GRID, SCREENED, PREC, 3, ORDER>(a, s);
+        default: return launch<GRID, SCREENED, PREC, 0, ORDER>(a, s);
     }
+}
+
+template <bool GRID, int PREC>
+static int launch_plain(const GwnArgs& a, const dwg_gwn_params& p, cudaStream_t s) {
+    if (p.order == 1) return launch_shape<GRID, false, PREC, 1>(a, p.tile, s);
+    if (p.order == 2) return launch_shape<GRID, false, PREC, 2>(a, p.tile, s);
+    return launch_shape<GRID, false, PREC, 0>(a, p.tile, s);
 }
 
 template <bool GRID>
 static int dispatch(const GwnArgs& a, const dwg_gwn_params& p, cudaStream_t s) {
     const int prec = p.precision < 0 ? 0 : (p.precision > 2 ? 2 : p.precision);
     if (p.screened) {
-        if (prec == 0) return launch_shape<GRID, true, 0>(a, p.tile, s);
-        if (prec == 1) return launch_shape<GRID, true, 1>(a, p.tile, s);
-        return launch_shape<GRID, true, 2>(a, p.tile, s);
+        if (prec == 0) return launch_shape<GRID, true, 0, 0>(a, p.tile, s);
+        if (prec == 1) return launch_shape<GRID, true, 1, 0>(a, p.tile, s);
+        return launch_shape<GRID, true, 2, 0>(a, p.tile, s);
     }
-    if (prec == 0) return launch_shape<GRID, false, 0>(a, p.tile, s);
-    if (prec == 1) return launch_shape<GRID, false, 1>(a, p.tile, s);
-    return launch_shape<GRID, false, 2>(a, p.tile, s);
+    if (prec == 0) return launch_plain<GRID, 0>(a, p, s);
+    if (prec == 1) return launch_plain<GRID, 1>(a, p, s);
+    return launch_plain<GRID, 2>(a, p, s);
 }
 
 int gwn_eval(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, float* out,
@@ -492,9 +556,16 @@ int gwn_eval(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, float*
              const float* sigma_dev) {
     DWG_REQUIRE(t.M > 0, "gwn: octree is empty");
     DWG_REQUIRE(out != nullptr, "gwn: output is null");
+    DWG_REQUIRE(p.order >= 0 && p.order <= 2, "gwn: expansion order must be 0, 1 or 2 (got %d)", p.order);
+    DWG_REQUIRE(p.order == 0 || !p.screened, "gwn: expansion orders above 0 apply to the plain sum only");
     GwnArgs a;
     a.info = t.info.ptr;
     DWG_TRY(octree_set_beta(const_cast<Octree&>(t), p.beta, s));
+    a.node_h = nullptr;
+    if (p.order > 0) {
+        DWG_TRY(octree_update_expansion(const_cast<Octree&>(t), p.order, s));
+        a.node_h = t.node_h.ptr;
+    }
     a.node_a = t.node_a.ptr;
     a.node_b = t.node_b.ptr;
     a.node_r = t.node_r.ptr;
@@ -575,6 +646,7 @@ static void fill_args(GwnArgs& a, const Octree& t, const GwnBatchItem& it, const
     a.terms_total = it.terms_total;
     a.per_query_terms = nullptr;
     a.work = t.work.ptr;  // error word at [1]
+    a.node_h = nullptr;
     a.num_nodes = t.M;
     a.num_points = t.n;
 }

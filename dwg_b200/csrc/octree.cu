@@ -300,6 +300,106 @@ __global__ void k_ec_level(const int* __restrict__ nodes, int p0, int count, con
     node_b[p] = make_float4((float)ex, (float)ey, (float)ez, __int_as_float(meta[p]));
 }
 
+// expansion coefficients about the node's centre c, bottom-up one depth
+// level at a time.  A leaf sums its points (a = p - c):
+//   m1[u + 3v] = sum A a_u n_v,   m2[9i + u + 3v] = sum 0.5 a_i A a_u n_v;
+// an internal node shifts its children's sums to its own centre
+// (d = c_child - c):
+//   m1 += m1c[u + 3v] + d_u e_v,
+//   m2 += m2c[9i + u + 3v] + 0.5 (d_i m1c[u + 3v] + d_u m1c[i + 3v]) + 0.5 d_i d_u e_v
+// with e = sum A n of the child.  Every sum has a fixed order.
+__global__ void k_ho_level(const int* __restrict__ nodes, int p0, int count, const int4* __restrict__ info,
+                           const float4* __restrict__ pa, const float4* __restrict__ nr,
+                           const double* __restrict__ cm_d, const double* __restrict__ ec_d, int order,
+                           double* __restrict__ ho_d, float4* __restrict__ node_h) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    const int p = p0 + i;
+    const int v = nodes[p];
+    const int4 iv = info[v];
+    const double c0 = cm_d[(size_t)v * 3], c1 = cm_d[(size_t)v * 3 + 1], c2 = cm_d[(size_t)v * 3 + 2];
+    double m[36];
+#pragma unroll
+    for (int t = 0; t < 36; ++t) m[t] = 0.0;
+    if (iv.w & kLeafFlag) {
+        for (int j = iv.x; j < iv.x + iv.y; ++j) {
+            const float4 q = pa[j];
+            const float4 nn = nr[j];
+            const double A = q.w;
+            const double a[3] = {(double)q.x - c0, (double)q.y - c1, (double)q.z - c2};
+            const double an[3] = {A * (double)nn.x, A * (double)nn.y, A * (double)nn.z};
+#pragma unroll
+            for (int vv = 0; vv < 3; ++vv)
+#pragma unroll
+                for (int u = 0; u < 3; ++u) {
+                    const double t1 = a[u] * an[vv];
+                    m[u + 3 * vv] += t1;
+                    if (order >= 2) {
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) m[9 + 9 * k + u + 3 * vv] += 0.5 * a[k] * t1;
+                    }
+                }
+        }
+    } else {
+        for (int ch = v + 1; ch < iv.z; ch = info[ch].z) {
+            const double d[3] = {cm_d[(size_t)ch * 3] - c0, cm_d[(size_t)ch * 3 + 1] - c1,
+                                 cm_d[(size_t)ch * 3 + 2] - c2};
+            const double e[3] = {ec_d[(size_t)ch * 3], ec_d[(size_t)ch * 3 + 1], ec_d[(size_t)ch * 3 + 2]};
+            const double* hc = ho_d + (size_t)ch * 36;
+            double m1c[9];
+#pragma unroll
+            for (int t = 0; t < 9; ++t) m1c[t] = hc[t];
+#pragma unroll
+            for (int vv = 0; vv < 3; ++vv)
+#pragma unroll
+                for (int u = 0; u < 3; ++u) {
+                    m[u + 3 * vv] += m1c[u + 3 * vv] + d[u] * e[vv];
+                    if (order >= 2) {
+#pragma unroll
+                        for (int k = 0; k < 3; ++k)
+                            m[9 + 9 * k + u + 3 * vv] += hc[9 + 9 * k + u + 3 * vv] +
+                                                         0.5 * (d[k] * m1c[u + 3 * vv] + d[u] * m1c[k + 3 * vv]) +
+                                                         0.5 * d[k] * d[u] * e[vv];
+                    }
+                }
+        }
+    }
+    double* ho = ho_d + (size_t)v * 36;
+#pragma unroll
+    for (int t = 0; t < 36; ++t) ho[t] = m[t];
+    // traversal record, contracted for evaluation (32 floats, 8 float4):
+    //   [0..8] m1, [9] trace m1, [10..12] g_k = sum_u m2[k,u,u] + sum_i m2[i,i,k]
+    //   + sum_i m2[i,k,i], [13..30] s(i<=u, v) = m2[i,u,v] + m2[u,i,v] (i != u)
+    //   for v = 0..2 and (i,u) = 00 01 02 11 12 22
+    float r[32];
+#pragma unroll
+    for (int t = 0; t < 9; ++t) r[t] = (float)m[t];
+    r[9] = (float)(m[0] + m[4] + m[8]);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        double g = 0;
+#pragma unroll
+        for (int u = 0; u < 3; ++u)
+            g += m[9 + 9 * k + u + 3 * u] + m[9 + 9 * u + u + 3 * k] + m[9 + 9 * u + k + 3 * u];
+        r[10 + k] = (float)g;
+    }
+    {
+        int o = 13;
+#pragma unroll
+        for (int vv = 0; vv < 3; ++vv)
+#pragma unroll
+            for (int i2 = 0; i2 < 3; ++i2)
+#pragma unroll
+                for (int u = i2; u < 3; ++u)
+                    r[o++] = (float)(i2 == u ? m[9 + 9 * i2 + u + 3 * vv]
+                                             : m[9 + 9 * i2 + u + 3 * vv] + m[9 + 9 * u + i2 + 3 * vv]);
+    }
+    r[31] = 0.f;
+    float4* h = node_h + (size_t)p * 8;
+#pragma unroll
+    for (int t = 0; t < 8; ++t) h[t] = make_float4(r[4 * t], r[4 * t + 1], r[4 * t + 2], r[4 * t + 3]);
+}
+
 // level-order position of every node and the traversal meta word
 __global__ void k_lvl_of(const int* __restrict__ level_nodes, int M, int* __restrict__ lvl_of) {
     int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -574,6 +674,21 @@ int octree_update_normals(Octree& t, cudaStream_t s) {
         if (cnt <= 0) continue;
         k_ec_level<<<div_up(cnt, 128), 128, 0, s>>>(t.level_nodes.ptr, t.level_off[d], cnt, t.info.ptr, t.pa.ptr,
                                                      t.nr.ptr, t.node_meta.ptr, t.ec_d.ptr, t.node_b.ptr);
+    }
+    DWG_CHECK_LAUNCH();
+    return DWG_OK;
+}
+
+int octree_update_expansion(Octree& t, int order, cudaStream_t s) {
+    DWG_REQUIRE(order >= 1 && order <= 2, "octree: expansion order must be 1 or 2 (got %d)", order);
+    DWG_TRY(t.ho_d.reserve((size_t)t.M * 36));
+    DWG_TRY(t.node_h.reserve((size_t)t.M * 8));
+    for (int d = t.max_depth; d >= 0; --d) {
+        int cnt = t.level_off[d + 1] - t.level_off[d];
+        if (cnt <= 0) continue;
+        k_ho_level<<<div_up(cnt, 64), 64, 0, s>>>(t.level_nodes.ptr, t.level_off[d], cnt, t.info.ptr, t.pa.ptr,
+                                                   t.nr.ptr, t.cm_d.ptr, t.ec_d.ptr, order, t.ho_d.ptr,
+                                                   t.node_h.ptr);
     }
     DWG_CHECK_LAUNCH();
     return DWG_OK;

@@ -51,6 +51,14 @@ struct Octree {
     DevBuf<float> node_r;
     float thr_beta = -1.f;  // beta the open thresholds were computed for (-1: none)
     DevBuf<double> cm_d, r_d, ec_d;
+    // far-field expansion coefficients of orders 1 and 2 about each node's
+    // centre of mass (igl::fast_winding_number precompute,
+    // deps/libigl/include/igl/fast_winding_number.cpp:87-105): 9 + 27 per node,
+    // FP64 in pre-order (ho_d); their FP32 contraction for evaluation in level
+    // order (node_h, 8 float4: m1, trace m1, the linear part of order 2, the
+    // 18 distinct sums of the order-2 tensor symmetric in its first two indices)
+    DevBuf<double> ho_d;
+    DevBuf<float4> node_h;
     // level order: level d = positions level_off[d] .. level_off[d+1]
     DevBuf<int> level_nodes, lvl_of, node_meta;
     int level_off[kMaxDepth + 2] = {0};
@@ -69,6 +77,9 @@ int octree_set_sorted_normals(Octree& t, const float* normals_sorted_dev, cudaSt
 int octree_update_centres(Octree& t, cudaStream_t s);
 // FP64 sum A n from pa.w and nr.xyz
 int octree_update_normals(Octree& t, cudaStream_t s);
+// expansion coefficients of orders 1..order (1 or 2) from the current
+// centres, areas and normals (after octree_update_normals)
+int octree_update_expansion(Octree& t, int order, cudaStream_t s);
 // open thresholds for the opening ratio beta (no-op when already current)
 int octree_set_beta(Octree& t, float beta, cudaStream_t s);
 // node centre of every node at the octreeDWG recursion (FP64), for leaf extraction

@@ -98,9 +98,11 @@ class TurboLibiGWN:
         return out_gwn
 
     def TurboLibiGWNLaunch(self, query_points, point_cloud=None, query_size=None, i_Normals=None, i_As=None,
-                           beta=2.3, out_gwn=None, precision=1):
-        """Plain GWN, sum A (p-q).n / (4 pi r^3 + 1e-8) (src/TurboLibiGWN.cu:328-511,899-910)."""
-        p = capi.gwn_params(beta=beta, sigma=0.0, screened=False, precision=precision)
+                           beta=2.3, out_gwn=None, precision=1, order=0):
+        """Plain GWN, sum A (p-q).n / (4 pi r^3 + 1e-8) (src/TurboLibiGWN.cu:328-511,899-910);
+        ``order`` 1 or 2 adds igl::fast_winding_number's far-field expansion
+        terms (deps/libigl/include/igl/fast_winding_number.cpp:187-241)."""
+        p = capi.gwn_params(beta=beta, sigma=0.0, screened=False, precision=precision, order=order)
         return self._launch(query_points, i_Normals, i_As, None, p, out_gwn)
 
     def TurboLibiScreenedGWNLaunch(self, query_points, point_cloud=None, query_size=None, i_Normals=None,
@@ -112,7 +114,7 @@ class TurboLibiGWN:
         return self._launch(query_points, i_Normals, i_As, i_radii if use_radii else None, p, out_gwn)
 
     def grid(self, res, origin, spacing, i_Normals=None, i_As=None, beta=2.3, sigma=10.0, screened=True,
-             precision=1, out=None, terms=None, screen=0.0015, tile=0):
+             precision=1, out=None, terms=None, screen=0.0015, tile=0, order=0):
         """GWN at the closed-form grid origin + index * spacing (x fastest);
         ``tile`` picks the brick of samples a warp evaluates together."""
         res = np.ascontiguousarray(res, np.int32)
@@ -121,7 +123,7 @@ class TurboLibiGWN:
         if out is None:
             out = torch.empty(n, dtype=torch.float32, device="cuda")
         p = capi.gwn_params(beta=beta, sigma=sigma, screen=screen, screened=screened, precision=precision,
-                            tile=tile)
+                            tile=tile, order=order)
         capi.check(capi.load().dwg_gwn_grid(self._h, capi.ptr(i_Normals), capi.ptr(i_As), None, res.ctypes.data,
                                             org.ctypes.data, float(spacing), C.byref(p), capi.ptr(out),
                                             capi.ptr(terms), capi.stream_ptr()))
@@ -143,6 +145,12 @@ class TurboLibiGWN:
             self._h, *[out[k].ctypes.data for k in ("depth", "pt_start", "pt_count", "skip", "cm", "radius",
                                                     "ec", "perm")]))
         out["perm"] = out["perm"][: self.n]
+        return out
+
+    def expansion(self):
+        """FP64 far-field coefficients of orders 1 and 2, (M, 36): m1 (9), m2 (27)."""
+        out = np.empty((self.num_nodes(), 36), np.float64)
+        capi.check(capi.load().dwg_octree_expansion(self._h, out.ctypes.data, capi.stream_ptr()))
         return out
 
     def EarseMemory(self):

@@ -101,6 +101,11 @@ typedef struct {
                         2 compensated with correctly rounded sqrt / exp / division */
     int tile;        /* grid samples per warp: 0 4x4x2 (default), 1 8x4x1,
                         2 2x4x4, 3 8x2x2 (point queries ignore it) */
+    int order;       /* far-field expansion order of the plain sum: 0 (the DWG
+                        kernels), 1 or 2 (igl::fast_winding_number's
+                        expansion_order, deps/libigl/include/igl/
+                        fast_winding_number.cpp:9-120,187-241); screened sums
+                        take 0 only */
 } dwg_gwn_params;
 
 int dwg_gwn_points(dwg_octree* tree, const float* normals_dev, const float* areas_dev,
@@ -115,6 +120,14 @@ int dwg_gwn_points_counted(dwg_octree* tree, const float* normals_dev, const flo
                            const float* radii_dev, const float* queries_dev, long long num_queries,
                            const dwg_gwn_params* params, float* out_dev, int* per_query_terms_dev,
                            void* stream);
+
+/* Far-field expansion coefficients of orders 1 and 2 (FP64, node order of
+ * dwg_octree_export, 36 per node: m1[u + 3v] = sum A a_u n_v and
+ * m2[9i + u + 3v] = sum 0.5 a_i A a_u n_v with a = p - CM), computed from the
+ * tree's current normals and areas.  The coefficients of
+ * igl::fast_winding_number's precompute with expansion_order 2
+ * (deps/libigl/include/igl/fast_winding_number.cpp:87-105, EC columns 3..38). */
+int dwg_octree_expansion(dwg_octree* tree, double* out_host, void* stream);
 
 /* Same sum at the samples of a regular grid: q(x,y,z) = origin + (x,y,z) * spacing,
  * x fastest; out has res[0]*res[1]*res[2] values.  The reference materialises

@@ -65,10 +65,11 @@ class TurboLibiGWN {
     void UpdateGWNInfo(const float* i_Normals, const float* i_As, void* stream = nullptr) {
         check(dwg_octree_update_info(tree_, i_Normals, i_As, stream));
     }
-    // plain GWN (src/TurboLibiGWN.cu:899-910)
+    // plain GWN (src/TurboLibiGWN.cu:899-910); expansion_order 1 or 2 adds
+    // igl::fast_winding_number's far-field terms
     void TurboLibiGWNLaunch(const float* query_points, int query_size, float beta, float* out_gwn,
-                            void* stream = nullptr) {
-        dwg_gwn_params p{beta, 0.f, 0.0015f, 0, 0, 1};
+                            void* stream = nullptr, int expansion_order = 0) {
+        dwg_gwn_params p{beta, 0.f, 0.0015f, 0, 0, 1, 0, expansion_order};
         check(dwg_gwn_points(tree_, nullptr, nullptr, nullptr, query_points, query_size, &p, out_gwn, nullptr,
                              stream));
     }

@@ -261,10 +261,48 @@ static inline double term_plain(double dx, double dy, double dz, double dot_an) 
     return dot_an / (4.0 * PI_D * r * r * r + 1e-8);
 }
 
+/* higher-order far-field terms of igl::fast_winding_number's expansion_eval
+ * (deps/libigl/include/igl/fast_winding_number.cpp:187-241), loc = CM - q:
+ * order 1 adds sum_uv SecondDerivative(u,v) m1[u + 3v] with
+ * SecondDerivative = loc loc^T (-3 / (4 pi r^5)) + I / (4 pi r^3); order 2 adds
+ * sum_i sum_uv ThirdDerivative_i(u,v) m2[9i + u + 3v] with
+ * ThirdDerivative_i = 15 loc_i loc loc^T / (4 pi r^7)
+ *                     - 3 / (4 pi r^5) (loc_i I + e_i loc^T + loc e_i^T) */
+static double expansion_terms(double lx, double ly, double lz, const double* h, int order) {
+    const double loc[3] = {lx, ly, lz};
+    const double r = sqrt(lx * lx + ly * ly + lz * lz);
+    const double p3 = 4.0 * PI_D * r * r * r;
+    const double p5 = p3 * r * r;
+    const double d = 1.0 / p3;
+    double w = 0;
+    for (int v = 0; v < 3; v++)
+        for (int u = 0; u < 3; u++) {
+            double sd = loc[u] * loc[v] * (-3.0 / p5);
+            if (u == v) sd += d;
+            w += sd * h[u + 3 * v];
+        }
+    if (order >= 2) {
+        const double p7 = p5 * r * r;
+        for (int i = 0; i < 3; i++)
+            for (int v = 0; v < 3; v++)
+                for (int u = 0; u < 3; u++) {
+                    double rcd = 0;
+                    if (u == v) rcd += loc[i];
+                    if (u == i) rcd += loc[v];
+                    if (v == i) rcd += loc[u];
+                    const double td = 15.0 * loc[i] * (loc[u] * (loc[v] / p7)) + (-3.0 / p5) * rcd;
+                    w += td * h[9 + 9 * i + u + 3 * v];
+                }
+    }
+    return w;
+}
+
 typedef struct {
     const dwgo_octree* t;
     const float *P, *N, *A, *radii;
     const double *CM, *EC;
+    const double* HO; /* expansion coefficients, 36 per node (order >= 1) */
+    int order;
     float* CMf; /* float copies used for the opening decision */
     float* Rf;
     const float* Q;
@@ -339,7 +377,8 @@ static void bh_visit(const bh_ctx* c, int node, float qxf, float qyf, float qzf,
                         (*nt)++;
                     }
                 } else {
-                    *acc += term_plain(dx, dy, dz, dot);
+                    *acc += term_plain(dx, dy, dz, dot) +
+                            (c->order > 0 ? expansion_terms(dx, dy, dz, c->HO + (size_t)ch * 36, c->order) : 0.0);
                     (*nt)++;
                 }
             }
@@ -382,13 +421,15 @@ static void run_threads(void* (*fn)(void*), void* ctx, int nthreads) {
     free(th);
 }
 
-void dwgo_gwn_bh(const dwgo_octree* t, const float* P, const float* N,
-                 const float* A, const float* radii, const double* CM,
-                 const double* R, const double* EC, const float* Q, long long nq,
-                 float beta, float sigma, int screened, int use_radii,
-                 float screen, int nthreads, double* out, long long* terms) {
+static void gwn_bh_impl(const dwgo_octree* t, const float* P, const float* N,
+                        const float* A, const float* radii, const double* CM,
+                        const double* R, const double* EC, const double* HO, int order,
+                        const float* Q, long long nq, float beta, float sigma, int screened,
+                        int use_radii, float screen, int nthreads, double* out, long long* terms) {
     bh_ctx c;
     memset(&c, 0, sizeof(c));
+    c.HO = HO;
+    c.order = order;
     c.t = t;
     c.P = P;
     c.N = N;
@@ -414,6 +455,46 @@ void dwgo_gwn_bh(const dwgo_octree* t, const float* P, const float* N,
     pthread_mutex_destroy(&c.mu);
     free(c.CMf);
     free(c.Rf);
+}
+
+void dwgo_gwn_bh(const dwgo_octree* t, const float* P, const float* N,
+                 const float* A, const float* radii, const double* CM,
+                 const double* R, const double* EC, const float* Q, long long nq,
+                 float beta, float sigma, int screened, int use_radii,
+                 float screen, int nthreads, double* out, long long* terms) {
+    gwn_bh_impl(t, P, N, A, radii, CM, R, EC, NULL, 0, Q, nq, beta, sigma, screened, use_radii, screen,
+                nthreads, out, terms);
+}
+
+void dwgo_fwn(const dwgo_octree* t, const float* P, const float* N, const float* A,
+              const double* CM, const double* R, const double* EC, const double* HO, int order,
+              const float* Q, long long nq, float beta, int nthreads, double* out, long long* terms) {
+    gwn_bh_impl(t, P, N, A, NULL, CM, R, EC, HO, order, Q, nq, beta, 0.f, 0, 0, 0.f, nthreads, out, terms);
+}
+
+void dwgo_expansion(const dwgo_octree* t, const float* P, const float* N, const float* A,
+                    const double* CM, double* HO) {
+    for (int nd = 0; nd < t->n_nodes; nd++) {
+        double* h = HO + (size_t)nd * 36;
+        memset(h, 0, sizeof(double) * 36);
+        for (long long j = t->list_off[nd]; j < t->list_off[nd + 1]; j++) {
+            const int i = t->flat[j];
+            double a[3], an[3];
+            for (int d = 0; d < 3; d++) {
+                a[d] = (double)P[(size_t)i * 3 + d] - CM[(size_t)nd * 3 + d];
+                an[d] = (double)A[i] * (double)N[(size_t)i * 3 + d];
+            }
+            /* TempCoeffs = A point^T N (col-major), then 0.5 point(k) TempCoeffs
+             * (fast_winding_number.cpp:89-104) */
+            for (int v = 0; v < 3; v++)
+                for (int u = 0; u < 3; u++) {
+                    const double tc = (double)A[i] * a[u] * (double)N[(size_t)i * 3 + v];
+                    h[u + 3 * v] += tc;
+                    for (int k = 0; k < 3; k++) h[9 + 9 * k + u + 3 * v] += 0.5 * a[k] * tc;
+                }
+            (void)an;
+        }
+    }
 }
 
 typedef struct {

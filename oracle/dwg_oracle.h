@@ -52,6 +52,18 @@ void dwgo_gwn_bh(const dwgo_octree* t, const float* P, const float* N,
                  const double* R, const double* EC, const float* Q, long long nq,
                  float beta, float sigma, int screened, int use_radii,
                  float screen, int nthreads, double* out, long long* terms);
+/* igl::fast_winding_number's expansion coefficients of orders 1 and 2
+ * (deps/libigl/include/igl/fast_winding_number.cpp:87-105), 36 per node:
+ * m1[u + 3v] = sum A a_u n_v, m2[9i + u + 3v] = sum 0.5 a_i A a_u n_v with
+ * a = p - CM, summed directly over each node's points */
+void dwgo_expansion(const dwgo_octree* t, const float* P, const float* N, const float* A,
+                    const double* CM, double* HO);
+/* plain Barnes-Hut sum with far-field expansions of the given order (0-2):
+ * the DWG traversal and opening test, far internal nodes evaluated by
+ * expansion_eval (fast_winding_number.cpp:187-241) */
+void dwgo_fwn(const dwgo_octree* t, const float* P, const float* N, const float* A,
+              const double* CM, const double* R, const double* EC, const double* HO, int order,
+              const float* Q, long long nq, float beta, int nthreads, double* out, long long* terms);
 /* exact all-pairs sum of the same kernel (no far field) */
 void dwgo_gwn_exact(const float* P, const float* N, const float* A,
                     const float* radii, int n, const float* Q, long long nq,

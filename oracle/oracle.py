@@ -81,6 +81,9 @@ def lib():
     L.dwgo_load_normals.argtypes = [_i32p, C.c_int, C.c_longlong, _f32p, _f32p]
     L.dwgo_radii.argtypes = [_f32p, C.c_int, _i32p, C.c_int, _f32p]
     L.dwgo_outlier_filter.argtypes = [_f32p, C.c_int, C.c_float]
+    L.dwgo_expansion.argtypes = [vp, _f32p, _f32p, _f32p, _f64p, _f64p]
+    L.dwgo_fwn.argtypes = [vp, _f32p, _f32p, _f32p, _f64p, _f64p, _f64p, _f64p, C.c_int, _f32p, C.c_longlong,
+                           C.c_float, C.c_int, _f64p, _i64p]
     L.dwgo_pca_normals.argtypes = [_f32p, C.c_int, _i32p, C.c_int, _f32p, _f32p]
     L.dwgo_point_areas.argtypes = [_f32p, C.c_int, _i32p, C.c_int, _f32p, _f32p]
     L.dwgo_random_normals.argtypes = [C.c_int, _f32p]
@@ -151,6 +154,33 @@ class Octree:
         EC = np.empty((M, 3), np.float64)
         lib().dwgo_moments(self._h, _f32(P).reshape(-1), _f32(N).reshape(-1), _f32(A), CM, R, EC)
         return CM, R, EC
+
+    def expansion(self, P, N, A, CM):
+        """Expansion coefficients of orders 1 and 2 (fast_winding_number.cpp:87-105), (M, 36)."""
+        HO = np.empty((self.num_nodes, 36), np.float64)
+        lib().dwgo_expansion(self._h, _f32(P).reshape(-1), _f32(N).reshape(-1), _f32(A),
+                             np.ascontiguousarray(CM, np.float64), HO)
+        return HO
+
+    def fwn(self, P, N, A, Q, order, beta=2.0, moments=None, nthreads=None):
+        """Plain Barnes-Hut sum with far-field expansions of ``order`` (0-2),
+        igl::fast_winding_number's expansion_eval; FP64.  ``moments`` =
+        (CM, R, EC, HO) replaces the oracle's own.  Returns (w, terms)."""
+        P = _f32(P).reshape(-1, 3)
+        N = _f32(N).reshape(-1, 3)
+        A = _f32(A)
+        Q = _f32(Q).reshape(-1)
+        nq = len(Q) // 3
+        if moments is None:
+            CM, R, EC = self.moments(P, N, A)
+            HO = self.expansion(P, N, A, CM)
+        else:
+            CM, R, EC, HO = (np.ascontiguousarray(m, np.float64) for m in moments)
+        out = np.empty(max(nq, 1), np.float64)
+        terms = np.empty(max(nq, 1), np.int64)
+        lib().dwgo_fwn(self._h, P.reshape(-1), N.reshape(-1), A, np.ascontiguousarray(CM), np.ascontiguousarray(R),
+                       np.ascontiguousarray(EC), HO, int(order), Q, nq, float(beta), nthreads or NTHREADS, out, terms)
+        return out[:nq], terms[:nq]
 
     def gwn(self, P, N, A, Q, beta=2.3, sigma=0.0, screened=True, radii=None, screen=0.0015,
             moments=None, nthreads=None):

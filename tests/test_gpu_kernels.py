@@ -297,3 +297,76 @@ def test_pca_normals_and_point_areas_bit_exact(oracle_lib, kind):
     assert torch.isfinite(got3).all()
     with pytest.raises(capi.DwgError):
         turbo.point_areas(cu(P[:2000]), cu(oracle_lib.knn(P[:2000], P[:2000], 33)), cu(ref_n[:2000]))
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_fwn_expansion_matches_oracle(torus_tree, order, dwg_lib, oracle_lib):
+    # igl::fast_winding_number's far field of orders 1 and 2 on the plain sum
+    import ctypes as C
+    P, N, A, gt, ot = torus_tree
+    g = gt.export()
+    idx = match_nodes(g, ot)
+    CM, R, EC = ot.moments(P, N, A)
+    HO_ref = ot.expansion(P, N, A, CM)[idx]
+    HO = gt.expansion()
+    # FP64 coefficients: the GPU shifts children's sums to the parent's
+    # centre, the oracle sums each node's points directly
+    mass = g["pt_count"][:, None] * 2e-6
+    tol1 = 1e-11 * mass * g["radius"][:, None]
+    tol2 = 1e-11 * mass * g["radius"][:, None] ** 2
+    assert np.all(np.abs(HO[:, :9] - HO_ref[:, :9]) <= tol1 + 1e-30)
+    assert np.all(np.abs(HO[:, 9:] - HO_ref[:, 9:]) <= tol2 + 1e-30)
+    # the sums, with the oracle fed the GPU's moments (identical decisions)
+    M = ot.num_nodes
+    full = [np.zeros((M, 3)), np.zeros(M), np.zeros((M, 3)), np.zeros((M, 36))]
+    full[0][idx], full[1][idx], full[2][idx], full[3][idx] = g["cm"], g["radius"], g["ec"], HO
+    rng = np.random.default_rng(9)
+    Q = np.concatenate([P[rng.choice(len(P), 2000, replace=False)],
+                        rng.uniform(-0.6, 0.6, (4000, 3)).astype(np.float32)])
+    w_ref, t_ref = ot.fwn(P, N, A, Q, order, beta=2.0, moments=full)
+    out = torch.empty(len(Q), dtype=torch.float32, device=DEV)
+    terms = torch.empty(len(Q), dtype=torch.int32, device=DEV)
+    p = capi.gwn_params(beta=2.0, sigma=0.0, screened=False, precision=1, order=order)
+    Q_d = cu(Q)
+    capi.check(dwg_lib.dwg_gwn_points_counted(gt._h, None, None, None, capi.ptr(Q_d), len(Q), C.byref(p),
+                                              capi.ptr(out), capi.ptr(terms), None))
+    torch.cuda.synchronize()
+    assert gt.status() == 0
+    assert np.array_equal(terms.cpu().numpy(), t_ref)
+    w = out.cpu().numpy().astype(np.float64)
+    err = np.abs(w - w_ref)
+    wmax = np.abs(w_ref).max()
+    assert err.max() < 1e-5 * wmax and np.sqrt((err ** 2).mean()) < 1e-6 * wmax
+    # the grid path evaluates the same terms
+    res = np.array([17, 15, 9], np.int32)
+    org = np.array([-0.55, -0.5, -0.2], np.float32)
+    h = np.float32(0.06)
+    Qg = oracle_lib.grid_points(res, org, h)
+    wg_ref, _ = ot.fwn(P, N, A, Qg, order, beta=2.0, moments=full)
+    wg = gt.grid(res, org, h, beta=2.0, sigma=0.0, screened=False, precision=1, order=order).cpu().numpy()
+    assert np.max(np.abs(wg - wg_ref)) < 2e-5 * max(1e-3, np.abs(wg_ref).max())
+    # screened sums take order 0 only
+    with pytest.raises(capi.DwgError):
+        gt.grid(res, org, h, beta=2.0, sigma=10.0, screened=True, order=order)
+
+
+def test_fwn_order2_closer_to_exact_on_gpu(oracle_lib):
+    # a closed sphere: order-2 far field, as in igl::fast_winding_number's
+    # default, is several times closer to the exact sum than order 0
+    rng = np.random.default_rng(0)
+    n = 20000
+    v = rng.normal(size=(n, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    P = (v * 0.4).astype(np.float32)
+    N = v.astype(np.float32)
+    A = np.full(n, 4 * np.pi * 0.16 / n, np.float32)
+    Q = rng.uniform(-0.6, 0.6, (4000, 3)).astype(np.float32)
+    exact = oracle_lib.gwn_exact(P, N, A, Q, screened=False)
+    P_d, N_d, A_d, Q_d = cu(P), cu(N), cu(A), cu(Q)
+    gt = turbo.TurboLibiGWN(P_d, max_depth=8, areas=A_d)
+    gt.UpdateMassNormals(N_d, A_d)
+    rms = []
+    for order in (0, 2):
+        w = gt.TurboLibiGWNLaunch(Q_d, beta=2.0, order=order).cpu().numpy()
+        rms.append(np.sqrt(np.mean((w - exact) ** 2)))
+    assert rms[1] < rms[0] / 3

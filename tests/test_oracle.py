@@ -239,3 +239,51 @@ def test_oracle_pca_normals_face_the_viewpoint(oracle_lib):
         view = (centre + s * 5 * nrm).astype(np.float32)
         N = oracle_lib.pca_normals(P, knn, view)
         assert np.allclose(N, s * nrm[None, :], atol=1e-5)
+
+
+def test_oracle_fwn_expansion_converges(oracle_lib):
+    # igl::fast_winding_number's far-field expansion: on one cluster of
+    # dipoles the error against the direct sum falls with the order and with
+    # the distance (order p: ~ r^-(3+p))
+    rng = np.random.default_rng(1)
+    n = 200
+    P = (rng.normal(size=(n, 3)) * 0.05).astype(np.float32)
+    N = rng.normal(size=(n, 3))
+    N = (N / np.linalg.norm(N, axis=1, keepdims=True)).astype(np.float32)
+    A = rng.uniform(0.5, 1.5, n).astype(np.float32)
+    t = oracle_lib.Octree(P, 4)
+    CM, R, EC = t.moments(P, N, A)
+    dirs = rng.normal(size=(40, 3))
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    errs = {}
+    for dist in (0.6, 2.4):
+        Q = (CM[0] + dist * dirs).astype(np.float32)
+        exact = oracle_lib.gwn_exact(P, N, A, Q, screened=False)
+        # beta small against the query distances over R: the root's children
+        # (internal nodes) are far and take the expansion
+        for order in (0, 1, 2):
+            w, _ = t.fwn(P, N, A, Q, order, beta=0.5)
+            errs[(dist, order)] = np.abs(w - exact).mean()
+    for dist in (0.6, 2.4):
+        assert errs[(dist, 2)] < errs[(dist, 1)] < errs[(dist, 0)]
+    for order in (0, 1, 2):
+        assert errs[(2.4, order)] < errs[(0.6, order)] / 4 ** (1 + order)
+
+
+def test_oracle_fwn_sphere_order2_beats_order0(oracle_lib):
+    rng = np.random.default_rng(0)
+    n = 20000
+    v = rng.normal(size=(n, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    P = (v * 0.4).astype(np.float32)
+    N = v.astype(np.float32)
+    A = np.full(n, 4 * np.pi * 0.16 / n, np.float32)
+    Q = rng.uniform(-0.6, 0.6, (2000, 3)).astype(np.float32)
+    t = oracle_lib.Octree(P, 8)
+    exact = oracle_lib.gwn_exact(P, N, A, Q, screened=False)
+    w0, t0 = t.fwn(P, N, A, Q, 0, beta=2.0)
+    w2, t2 = t.fwn(P, N, A, Q, 2, beta=2.0)
+    assert np.array_equal(t0, t2)  # same traversal, richer far terms
+    rms0 = np.sqrt(np.mean((w0 - exact) ** 2))
+    rms2 = np.sqrt(np.mean((w2 - exact) ** 2))
+    assert rms2 < rms0 / 3
