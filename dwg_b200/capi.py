@@ -114,6 +114,7 @@ _SIGS = {
     "dwg_read_xyz": (_i, [C.c_char_p, _i, C.POINTER(C.POINTER(_f)), C.POINTER(C.POINTER(_f)), C.POINTER(_i)]),
     "dwg_free_host": (None, [_vp]),
     "dwg_write_stl": (_i, [C.c_char_p, _vp, _ll]),
+    "dwg_write_stl_device": (_i, [C.c_char_p, _vp, _ll, _vp]),
     "dwg_write_xyz": (_i, [C.c_char_p, _vp, _vp, _i]),
 }
 

@@ -126,8 +126,9 @@ int main(int argc, char** argv) {
             long long T = dwg.size("triangles");
             printf("Num triangles: %lld\n", T);
             if (output_mode == 1 || output_mode == 3) {
-                auto tris = dwg.get<float>("tris", (size_t)T * 9);
-                dwg::check(dwg_write_stl((out_full + ".stl").c_str(), tris.data(), T));
+                void* tris = nullptr;
+                dwg::check(dwg_pipeline_device_ptr(dwg.handle(), "tris", &tris));
+                dwg::check(dwg_write_stl_device((out_full + ".stl").c_str(), (const float*)tris, T, nullptr));
                 printf("Mesh saved to %s.stl (%lld triangle(s)).\n", out_full.c_str(), T);
             }
             if ((output_mode == 2 || output_mode == 3) && !prm.use_leaves_generate) {

@@ -803,120 +803,6 @@ int dwg_reconstruct_host(const float* points_host, const float* normals_host, in
     })
 }
 
-// ------------------------------------------------------------------ IO --
-// ReadPointandNormals (include/DWGProcess.h:53-97)
-int dwg_read_xyz(const char* path, int normalize, float** points, float** normals, int* n) {
-    API_GUARD({
-        DWG_REQUIRE(path && points && n, "read_xyz: null argument");
-        FILE* f = fopen(path, "r");
-        DWG_REQUIRE(f != nullptr, "read_xyz: cannot open '%s'", path);
-        std::vector<double> P, N;
-        char line[4096];
-        long long lineno = 0;
-        while (fgets(line, sizeof(line), f)) {
-            ++lineno;
-            double v[6];
-            int k = sscanf(line, "%lf %lf %lf %lf %lf %lf", &v[0], &v[1], &v[2], &v[3], &v[4], &v[5]);
-            if (k <= 0) continue;  // blank line
-            if (k < 3) {
-                fclose(f);
-                set_error("read_xyz: line %lld of '%s' has %d values (need 3 or 6)", lineno, path, k);
-                return DWG_ERR_INVALID;
-            }
-            for (int d = 0; d < 3; ++d) {
-                if (!std::isfinite(v[d])) {
-                    fclose(f);
-                    set_error("read_xyz: non-finite coordinate on line %lld of '%s'", lineno, path);
-                    return DWG_ERR_INVALID;
-                }
-                P.push_back(v[d]);
-            }
-            for (int d = 3; d < 6; ++d) N.push_back(k == 6 ? v[d] : 0.0);
-        }
-        fclose(f);
-        int cnt = (int)(P.size() / 3);
-        DWG_REQUIRE(cnt > 0, "read_xyz: no points in '%s'", path);
-        if (normalize) {
-            double c[3] = {0, 0, 0};
-            for (int i = 0; i < cnt; ++i)
-                for (int d = 0; d < 3; ++d) c[d] += P[(size_t)i * 3 + d];
-            for (int d = 0; d < 3; ++d) c[d] /= (1.0 * cnt);
-            double scale = 0;
-            for (int i = 0; i < cnt; ++i)
-                for (int d = 0; d < 3; ++d) {
-                    P[(size_t)i * 3 + d] -= c[d];
-                    scale = std::max(2.0 * std::fabs(P[(size_t)i * 3 + d]), scale);
-                }
-            if (scale == 0) scale = 1;
-            for (auto& x : P) x /= scale;
-        }
-        float* po = (float*)malloc(sizeof(float) * 3 * cnt);
-        float* no = normals ? (float*)malloc(sizeof(float) * 3 * cnt) : nullptr;
-        if (!po || (normals && !no)) {
-            free(po);
-            free(no);
-            set_error("read_xyz: host allocation failed");
-            return DWG_ERR_NOMEM;
-        }
-        for (size_t i = 0; i < P.size(); ++i) po[i] = (float)P[i];
-        if (no)
-            for (size_t i = 0; i < N.size(); ++i) no[i] = (float)N[i];
-        *points = po;
-        if (normals) *normals = no;
-        *n = cnt;
-        return DWG_OK;
-    })
-}
-
-void dwg_free_host(void* p) { free(p); }
-
-// save_binary_STL (src/TurboMC.cu:344-371): 80-byte header, uint32 count,
-// per triangle normal (cross / |cross|, 0 if degenerate), 3 vertices, uint16 0
-int dwg_write_stl(const char* path, const float* tris, long long T) {
-    API_GUARD({
-        DWG_REQUIRE(path && (tris || T == 0) && T >= 0 && T <= 0xffffffffll, "write_stl: bad arguments");
-        FILE* f = fopen(path, "wb");
-        DWG_REQUIRE(f != nullptr, "write_stl: cannot create '%s'", path);
-        char header[80] = {0};
-        uint32_t cnt = (uint32_t)T;
-        bool ok = fwrite(header, 1, 80, f) == 80 && fwrite(&cnt, 4, 1, f) == 1;
-        std::vector<unsigned char> rec(50);
-        for (long long t = 0; ok && t < T; ++t) {
-            const float* v = tris + t * 9;
-            float e1[3] = {v[3] - v[0], v[4] - v[1], v[5] - v[2]};
-            float e2[3] = {v[6] - v[0], v[7] - v[1], v[8] - v[2]};
-            float c[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]};
-            float len = std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
-            float nrm[3] = {0, 0, 0};
-            if (len > 0)
-                for (int d = 0; d < 3; ++d) nrm[d] = c[d] / len;
-            memcpy(rec.data(), nrm, 12);
-            memcpy(rec.data() + 12, v, 36);
-            rec[48] = rec[49] = 0;
-            ok = fwrite(rec.data(), 1, 50, f) == 50;
-        }
-        fclose(f);
-        DWG_REQUIRE(ok, "write_stl: cannot write '%s'", path);
-        return DWG_OK;
-    })
-}
-
-// oriented point cloud output (src/TurboDWG.cu:903-923)
-int dwg_write_xyz(const char* path, const float* P, const float* N, int n) {
-    API_GUARD({
-        DWG_REQUIRE(path && P && n >= 0, "write_xyz: bad arguments");
-        FILE* f = fopen(path, "w");
-        DWG_REQUIRE(f != nullptr, "write_xyz: cannot create '%s'", path);
-        for (int i = 0; i < n; ++i) {
-            if (N)
-                fprintf(f, "%g %g %g %g %g %g\n", P[i * 3], P[i * 3 + 1], P[i * 3 + 2], N[i * 3], N[i * 3 + 1],
-                        N[i * 3 + 2]);
-            else
-                fprintf(f, "%g %g %g\n", P[i * 3], P[i * 3 + 1], P[i * 3 + 2]);
-        }
-        fclose(f);
-        return DWG_OK;
-    })
-}
+// the file readers and writers are in io.cu
 
 }  // extern "C"

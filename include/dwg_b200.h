@@ -402,10 +402,17 @@ int dwg_reconstruct_host(const float* points_host, const float* normals_host, in
  * ------------------------------------------------------------------------ */
 /* Read "x y z [nx ny nz]" lines; returns the count in *n and malloc'd arrays
  * (free with dwg_free_host).  When `normalize` is set, centre on the mean and
- * divide by max 2|x| (FP64), as the reference reader does. */
+ * divide by max 2|x| (FP64), as the reference reader does.  Blank lines are
+ * skipped; a line with 1-2 numbers or a non-finite coordinate is an error
+ * naming the line.  Parsed on all host cores, with the doubles of %lf. */
 int dwg_read_xyz(const char* path, int normalize, float** points, float** normals, int* n);
 void dwg_free_host(void* p);
 int dwg_write_stl(const char* path, const float* tris_host, long long num_tris);
+/* The same STL file from triangles in device memory (9 floats each, e.g.
+ * dwg_pipeline_device_ptr "tris"): the 50-byte records are packed on the GPU
+ * in chunks of 2^20 triangles and written while the next chunk is packed.
+ * Synchronises `stream`. */
+int dwg_write_stl_device(const char* path, const float* tris_dev, long long num_tris, void* stream);
 int dwg_write_xyz(const char* path, const float* points_host, const float* normals_host, int n);
 
 #ifdef __cplusplus

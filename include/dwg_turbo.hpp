@@ -110,11 +110,9 @@ class TurboMC {
         int rc = dwg_marching_cubes(voxel_values, res, voxel_poses, origin, spacing, threshold, tris, mid_points,
                                     mid_normals, cap, nullptr, &T, stream);
         if (rc == DWG_OK && stl) {
-            std::vector<float> host((size_t)T * 9);
-            rc = copy_to_host_(host.data(), tris, host.size() * sizeof(float));
             std::string path = iterations == 123456 ? mesh_full_path + ".stl"
                                                     : mesh_path + std::to_string(iterations) + "iter.stl";
-            if (rc == DWG_OK) rc = dwg_write_stl(path.c_str(), host.data(), T);
+            rc = dwg_write_stl_device(path.c_str(), tris, T, stream);
         }
         if (tris) cudaFree_(tris);
         check(rc);
@@ -124,7 +122,6 @@ class TurboMC {
    private:
     static int cudaMalloc_(float** p, size_t bytes);
     static void cudaFree_(float* p);
-    static int copy_to_host_(float* dst, const float* src, size_t bytes);
 };
 
 // include/TurboDWG.h:14-27: GenerateKDTreeForDWG + CudaKNNWithKDTreeforDWG
@@ -178,6 +175,3 @@ class TurboDWG {
 
 inline int dwg::TurboMC::cudaMalloc_(float** p, size_t bytes) { return (int)::cudaMalloc((void**)p, bytes); }
 inline void dwg::TurboMC::cudaFree_(float* p) { ::cudaFree(p); }
-inline int dwg::TurboMC::copy_to_host_(float* dst, const float* src, size_t bytes) {
-    return ::cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost) == cudaSuccess ? DWG_OK : DWG_ERR_CUDA;
-}

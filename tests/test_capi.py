@@ -125,3 +125,64 @@ def test_write_xyz(dwg_lib, tmp_path):
     f = tmp_path / "o.xyz"
     assert dwg_lib.dwg_write_xyz(str(f).encode(), P.ctypes.data, N.ctypes.data, 1) == 0
     assert [float(x) for x in f.read_text().split()] == [0.5, 1, 2, 0, 0, 1]
+
+
+def test_read_xyz_chunked_parse_matches_python(dwg_lib, tmp_path):
+    # a file large enough to be parsed in several newline-aligned chunks:
+    # mixed 3/6-column lines, blank lines, signs, exponents, CRLF endings;
+    # every value must be the correctly rounded double (as %lf / float())
+    rng = np.random.default_rng(5)
+    rows, want_p, want_n = [], [], []
+    for i in range(60000):
+        if i % 997 == 0:
+            rows.append("")
+        p = rng.uniform(-50, 50, 3)
+        toks = [f"{x:+.7e}" if i % 3 == 0 else repr(float(x)) for x in p]
+        if i % 2:
+            nn = rng.standard_normal(3)
+            toks += [f"{x:.6f}" for x in nn]
+            want_n.append([float(t) for t in toks[3:]])
+        else:
+            want_n.append([0.0, 0.0, 0.0])
+        want_p.append([float(t) for t in toks[:3]])
+        rows.append(" \t".join(toks) + ("\r" if i % 5 == 0 else ""))
+    f = tmp_path / "big.xyz"
+    f.write_text("\n".join(rows) + "\n")
+    assert f.stat().st_size > 3 << 20
+    pts = C.POINTER(C.c_float)()
+    nrm = C.POINTER(C.c_float)()
+    n = C.c_int()
+    assert dwg_lib.dwg_read_xyz(str(f).encode(), 0, C.byref(pts), C.byref(nrm), C.byref(n)) == 0
+    got = np.ctypeslib.as_array(pts, (n.value, 3)).copy()
+    gotn = np.ctypeslib.as_array(nrm, (n.value, 3)).copy()
+    dwg_lib.dwg_free_host(C.cast(pts, C.c_void_p))
+    dwg_lib.dwg_free_host(C.cast(nrm, C.c_void_p))
+    assert n.value == len(want_p)
+    assert np.array_equal(got, np.array(want_p).astype(np.float32))
+    assert np.array_equal(gotn, np.array(want_n).astype(np.float32))
+    # an error far into the file is reported with its line number
+    rows2 = list(rows)
+    rows2[50001] = "1.0 2.0"
+    f.write_text("\n".join(rows2) + "\n")
+    assert dwg_lib.dwg_read_xyz(str(f).encode(), 0, C.byref(pts), None, C.byref(n)) == capi.DWG_ERR_INVALID
+    assert b"line 50002 " in dwg_lib.dwg_last_error()
+
+
+def test_write_stl_many_triangles_threaded(dwg_lib, tmp_path):
+    rng = np.random.default_rng(2)
+    T = 300000
+    tris = rng.uniform(-1, 1, (T, 9)).astype(np.float32)
+    tris[7, 3:6] = tris[7, 0:3]  # degenerate: zero normal
+    f = tmp_path / "m.stl"
+    assert dwg_lib.dwg_write_stl(str(f).encode(), tris.ctypes.data, T) == 0
+    b = f.read_bytes()
+    assert len(b) == 84 + 50 * T
+    rec = np.frombuffer(b[84:], dtype=np.dtype([("n", "<f4", 3), ("v", "<f4", 9), ("a", "<u2")]))
+    assert np.array_equal(rec["v"], tris) and not rec["a"].any()
+    e1, e2 = tris[:, 3:6] - tris[:, 0:3], tris[:, 6:9] - tris[:, 0:3]
+    c = np.cross(e1, e2)
+    with np.errstate(invalid="ignore"):
+        nn = c / np.linalg.norm(c, axis=1, keepdims=True)
+    ok = np.isfinite(nn).all(1)
+    assert np.allclose(rec["n"][ok], nn[ok], atol=1e-6)
+    assert not rec["n"][7].any()

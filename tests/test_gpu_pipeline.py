@@ -130,3 +130,48 @@ def test_pipeline_com_as_random_start_matches_oracle(oracle_lib):
     got = turbo.reconstruct(cu(Pn), **cfg)
     want = oracle_lib.random_normals(len(got["leaf_pos"]))
     assert np.allclose(got["leaf_nrm"], want, atol=1e-7)
+
+
+def test_write_stl_device_matches_host_writer(tmp_path):
+    import ctypes as C
+    from dwg_b200 import capi
+    lib = capi.load()
+    P, _ = D.torus(4000, seed=5)
+    Pn, _, _ = D.normalize(P)
+    got = turbo.reconstruct(cu(Pn), **dict(SMALL, total_iter=2))
+    tris = np.ascontiguousarray(got["tris"], np.float32)
+    # more than one 2^20-triangle chunk of the device writer
+    big = np.tile(tris, (int(np.ceil(2.5 * (1 << 20) / len(tris))), 1))[: int(2.5 * (1 << 20))]
+    for t in (tris, big):
+        fh, fd = tmp_path / "h.stl", tmp_path / "d.stl"
+        assert lib.dwg_write_stl(str(fh).encode(), t.ctypes.data, len(t)) == 0
+        td = cu(t)
+        capi.check(lib.dwg_write_stl_device(str(fd).encode(), capi.ptr(td), len(t), None))
+        assert fh.read_bytes() == fd.read_bytes()
+
+
+@pytest.mark.parametrize("com_as", [0, 1])
+def test_dwg_cuda_cli_end_to_end(tmp_path, com_as):
+    # the DWG_CUDA command line (src/main.cpp flags): read .xyz, reconstruct,
+    # write the binary STL (device packer) and the oriented .xyz
+    import os
+    import subprocess
+    import struct
+    exe = os.path.join(os.path.dirname(turbo.__file__), "bin", "DWG_CUDA")
+    P, N = D.torus(3000, seed=8)
+    with open(tmp_path / "t.xyz", "w") as fh:
+        for p, n in zip(P, N):
+            fh.write(f"{p[0]:.7f} {p[1]:.7f} {p[2]:.7f} {n[0]:.6f} {n[1]:.6f} {n[2]:.6f}\n")
+    out = tmp_path / "out"
+    out.mkdir()
+    r = subprocess.run([exe, "--in_path", str(tmp_path), "--in_name", "t.xyz", "--out_path", str(out),
+                        "--grid_reso", "40", "--final_reso", "40", "--total_iter", "2", "--max_depth", "7",
+                        "--output_mode", "3", "--com_As", str(com_as)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    stl = out / "t_md_7_gr_40_iter_2.stl"
+    b = stl.read_bytes()
+    T = struct.unpack("<I", b[80:84])[0]
+    assert T > 100 and len(b) == 84 + 50 * T
+    xyz = np.loadtxt(out / "t_md_7_gr_40_iter_2.xyz")
+    assert xyz.shape == (3000, 6)
+    assert np.allclose(np.linalg.norm(xyz[:, 3:], axis=1), 1, atol=1e-3)
