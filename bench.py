@@ -40,7 +40,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Mpts/s to converged mesh at RMS GWN err≤1e-4; pair-evals/s; learned vs plain iters"
 WORKLOAD = dict(workload="nonuniform torus 100k points, 256^3 grid, 30 DWG iterations",
-                points=100_000, grid_reso=256, final_reso=256, total_iter=30, precision="fp32-compensated",
+                points=100_000, grid_reso=256, final_reso=256, total_iter=30, precision="fp32-terms-fp64-sum",
                 beta=2.3, max_depth=10)
 
 
@@ -249,7 +249,7 @@ def run_ours(a, rank, world, local_rank):
         "dtype": "f32",
         "data": "synthetic (seeded procedural torus; no dataset)",
         "config": dict(WORKLOAD, points=a.points, grid_reso=a.grid, final_reso=a.grid, total_iter=a.iters,
-                       precision={0: "fp32", 1: "fp32-compensated", 2: "fp32-compensated-accurate-terms"}[
+                       precision={0: "fp32", 1: "fp32-terms-fp64-sum", 2: "fp32-accurate-terms-fp64-sum"}[
                            a.precision],
                        parallelism=f"replicas x{world}", l2="flushed (256 MB write) between timed steps",
                        triangles_final=int(final_tris)),
@@ -441,7 +441,7 @@ def precision_report(a, lib, capi, turbo, torch, dev):
     tree.UpdateMassNormals(lnd, Ad)
     out = {"state": "bench cloud after 2 DWG iterations, sigma 20, beta 2.3; grid: 20,000 seeded samples",
            "scale_rms": {"leaf": float(np.sqrt(np.mean(ref_leaf ** 2))), "grid": float(np.sqrt(np.mean(ref_grid ** 2)))}}
-    names = {0: "fp32", 1: "fp32-compensated", 2: "fp32-compensated-accurate-terms"}
+    names = {0: "fp32", 1: "fp32-terms-fp64-sum", 2: "fp32-accurate-terms-fp64-sum"}
     for prec in (0, 1, 2):
         wl = tree.TurboLibiScreenedGWNLaunch(lpd, i_Normals=None, i_As=None, beta=2.3, sigma=20.0,
                                              precision=prec).cpu().numpy().astype(np.float64)

@@ -7,8 +7,8 @@
 // carries the mask of lanes that opened the node, so each lane still takes
 // exactly the reference's per-query decisions -- a child is a dipole term
 // when |CM - q| > beta R, otherwise it is opened, and leaves are summed point
-// by point -- while node and point loads are warp-broadcast.  Sums are FP32
-// with an optional compensated (two-sum) accumulator per lane.
+// by point -- while node and point loads are warp-broadcast.  Terms are
+// FP32; each query's sum is FP32 (precision 0) or FP64 (precision >= 1).
 #include "gwn.cuh"
 
 #include <vector>
@@ -75,19 +75,16 @@ __device__ __forceinline__ bool gwn_term(float dx, float dy, float dz, float d, 
     return gwn_term_r2<SCREENED, PREC>(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), d, s, sigma, sigma_l2e, v);
 }
 
+// per-query accumulator: FP32 (PREC 0) or FP64 (PREC >= 1: each FP32 term
+// converted exactly and added in double, one conversion and one add per term)
 template <int PREC>
-__device__ __forceinline__ void acc_add(float& s, float& c, float v) {
-    if (PREC == 0) {
-        s += v;
-    } else {
-        // Knuth two-sum: s + v = t + err exactly
-        float t = __fadd_rn(s, v);
-        float bp = __fsub_rn(t, s);
-        float err = __fadd_rn(__fsub_rn(s, __fsub_rn(t, bp)), __fsub_rn(v, bp));
-        s = t;
-        c = __fadd_rn(c, err);
-    }
-}
+struct AccType {
+    using T = double;
+};
+template <>
+struct AccType<0> {
+    using T = float;
+};
 
 // brick shapes of 32 grid samples (x, y, z extents) a warp evaluates together
 template <int SHAPE>
@@ -279,12 +276,12 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
             }
         }
     }
-    float sum[NQ], cmp[NQ];
+    using Acc = typename AccType<PREC>::T;
+    Acc sum[NQ];
     int nt[NQ];
 #pragma unroll
     for (int u = 0; u < NQ; ++u) {
-        sum[u] = 0.f;
-        cmp[u] = 0.f;
+        sum[u] = 0;
         nt[u] = 0;
     }
 
@@ -297,7 +294,7 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
             const float sc = a.use_radii ? nn.w : a.screen;
             float v;
             if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, sc, sigma, sigma_l2e, v)) {
-                acc_add<PREC>(sum[u], cmp[u], v);
+                sum[u] += (Acc)v;
                 ++nt[u];
             }
         }
@@ -340,7 +337,8 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
         if (__any_sync(FULL, any)) {
 #pragma unroll
             for (int u = 0; u < NQ; ++u) {
-                const float dd = fmaf(dx[u], nb.x, fmaf(dy[u], nb.y, dz[u] * nb.z));
+                // x and y parts first: the samples of a lane share x and y
+                const float dd = fmaf(dz[u], nb.z, fmaf(dy[u], nb.y, dx[u] * nb.x));
                 bool k;
                 float v = gwn_term_masked<SCREENED, PREC>(take[u], d2[u], dd, a.screen, sigma, sigma_l2e, k);
                 if (ORDER > 0 && !SCREENED && !leaf) {
@@ -349,7 +347,7 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
                                                                 a.node_h + (size_t)cidx * 8);
                     v += take[u] ? c : 0.f;
                 }
-                if (k) acc_add<PREC>(sum[u], cmp[u], v);
+                sum[u] += (Acc)v;  // v is 0 where no term is taken
                 nt[u] += (int)k;
             }
         }
@@ -428,7 +426,7 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
 #pragma unroll
     for (int u = 0; u < NQ; ++u) {
         if (valid[u]) {
-            a.out[qi[u]] = (PREC == 0) ? sum[u] : __fadd_rn(sum[u], cmp[u]);
+            a.out[qi[u]] = (float)sum[u];
             if (a.per_query_terms) a.per_query_terms[qi[u]] = nt[u];
         }
         total += nt[u];

@@ -4,7 +4,7 @@
 // For one cloud: build the pipeline, run a few DWG iterations so that the
 // normals are realistic, then
 //   1. draw `samples` grid samples (seeded) and sum them exactly (every node
-//      opened; correctly rounded terms, compensated accumulation);
+//      opened; correctly rounded terms, FP64 accumulation);
 //   2. for each candidate opening ratio, the RMS and max error of the
 //      Barnes-Hut sums at those samples against the exact ones;
 //   3. among the ratios within `tol` (tol <= 0: within the error of the

@@ -97,8 +97,9 @@ typedef struct {
     float screen;    /* screen radius s when use_radii == 0, reference 0.0015 */
     int screened;    /* 1 screened kernel, 0 plain kernel */
     int use_radii;   /* 1: s = radii[i] for point terms (far field keeps `screen`) */
-    int precision;   /* 0 plain FP32 accumulation, 1 FP32 compensated (default),
-                        2 compensated with correctly rounded sqrt / exp / division */
+    int precision;   /* terms in FP32; 0 FP32 accumulation, 1 FP64 accumulation
+                        (default), 2 FP64 accumulation with correctly rounded
+                        sqrt / exp / division in the terms */
     int tile;        /* grid samples per warp: 0 4x4x2 (default), 1 8x4x1,
                         2 2x4x4, 3 8x2x2 (point queries ignore it) */
     int order;       /* far-field expansion order of the plain sum: 0 (the DWG

@@ -33,7 +33,7 @@ def test_pipeline_leaves_identical(small_runs):
 
 def test_pipeline_iso_and_counts_track_oracle(small_runs):
     Pn, ref, got = small_runs
-    # FP32-compensated sums vs FP64: the first iterations agree to ~1e-6;
+    # FP32 terms (FP64 sums) vs the FP64 oracle: the first iterations agree to ~1e-6;
     # later ones drift a little as single-precision ties flip a few cells
     assert np.allclose(got["iso"][:2], ref["iso"][:2], rtol=1e-5, atol=1e-10)
     assert np.allclose(got["iso"], ref["iso"], rtol=2e-2, atol=1e-8)
@@ -113,7 +113,7 @@ def test_pipeline_com_as_tracks_oracle(oracle_lib, in_normal):
     got = turbo.reconstruct(cu(Pn), **cfg)
     plain = turbo.reconstruct(cu(Pn), **dict(SMALL, total_iter=2, in_normal=3))
     assert np.array_equal(got["leaf_pos"], ref["leaf_pos"])
-    # the areas are bit-identical; the sums differ by FP32-compensated vs FP64
+    # the areas are bit-identical; the sums differ by FP32 terms vs FP64
     # rounding (relative to the terms, so more where the mean cancels)
     assert np.allclose(got["iso"], ref["iso"], rtol=2e-4, atol=1e-10)
     assert np.all(np.abs(got["tri_count"] - ref["tri_count"]) <= 0.002 * ref["tri_count"] + 4)
