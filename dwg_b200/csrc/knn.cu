@@ -602,6 +602,66 @@ __global__ void k_kb_local(KnnGrid g, const int* __restrict__ cell_start, const 
     kb[c] = cnt >= kKnnBoundK ? sqrtf(mx) * 1.00002f + 1e-7f : INFINITY;
 }
 
+// kb for the cells that hold queries: the 16th smallest distance from the
+// cell centre over the cells within Chebyshev radius r, r = 1, 2, 3 until 16
+// points are found (any 16 points bound the 16th nearest from above), +inf
+// when the radius-3 block holds fewer (those queries take the per-thread
+// search, which needs no bound)
+constexpr int kKbActiveRadius = 3;
+__global__ void k_kb_active(KnnGrid g, const int* __restrict__ cell_start, const float4* __restrict__ pts,
+                            const int* __restrict__ active, const int* __restrict__ misc, float* __restrict__ kb) {
+    const int na = misc[0];
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < na; t += gridDim.x * blockDim.x) {
+        const int c = active[t];
+        const int i = c % g.G0, j = (c / g.G0) % g.G1, k = c / (g.G0 * g.G1);
+        const float x = cell_mid(g.lo0, i, g.h), y = cell_mid(g.lo1, j, g.h), z = cell_mid(g.lo2, k, g.h);
+        float d[kKnnBoundK];
+#pragma unroll
+        for (int q = 0; q < kKnnBoundK; ++q) d[q] = INFINITY;
+        float mx = INFINITY;
+        int mpos = 0, cnt = 0;
+        for (int r = 0; r <= kKbActiveRadius; ++r) {
+            for (int dz = -r; dz <= r; ++dz) {
+                const int zz = k + dz;
+                if (zz < 0 || zz >= g.G2) continue;
+                for (int dy = -r; dy <= r; ++dy) {
+                    const int yy = j + dy;
+                    if (yy < 0 || yy >= g.G1) continue;
+                    for (int dx = -r; dx <= r; ++dx) {
+                        // the shell of radius r only
+                        if (max(abs(dx), max(abs(dy), abs(dz))) != r) continue;
+                        const int xx = i + dx;
+                        if (xx < 0 || xx >= g.G0) continue;
+                        const int cc = xx + g.G0 * (yy + g.G1 * zz);
+                        const int e = cell_start[cc + 1];
+                        for (int s = cell_start[cc]; s < e; ++s) {
+                            const float4 p = pts[s];
+                            const float ex = p.x - x, ey = p.y - y, ez = p.z - z;
+                            const float d2 = ex * ex + ey * ey + ez * ez;
+                            ++cnt;
+                            if (d2 < mx) {
+#pragma unroll
+                                for (int q = 0; q < kKnnBoundK; ++q)
+                                    if (q == mpos) d[q] = d2;
+                                mx = d[0];
+                                mpos = 0;
+#pragma unroll
+                                for (int q = 1; q < kKnnBoundK; ++q)
+                                    if (d[q] > mx) {
+                                        mx = d[q];
+                                        mpos = q;
+                                    }
+                            }
+                        }
+                    }
+                }
+            }
+            if (r >= 1 && cnt >= kKnnBoundK) break;
+        }
+        kb[c] = cnt >= kKnnBoundK ? sqrtf(mx) * 1.00002f + 1e-7f : INFINITY;
+    }
+}
+
 // one min-plus pass with the 26 neighbours at distance `step` cells:
 // kb[c] <= kb[c'] + |x_c - x_c'| (triangle inequality); len1..3 are the
 // neighbour distances rounded up
@@ -934,7 +994,7 @@ static int knn_launch(const KnnArgs& a, long long nq, cudaStream_t s) {
 
 // queries grouped by cell (k <= 16, no exclusion), see k_knn_cells
 static int knn_query_cells(const KnnIndex& ix, const KnnArgs& a0, long long nq, cudaStream_t s) {
-    if (!ix.kb_ready) DWG_TRY(build_kbound(ix, s));
+    if (!ix.kb_per_query && !ix.kb_ready) DWG_TRY(build_kbound(ix, s));
     const long long ncell = (long long)ix.G[0] * ix.G[1] * ix.G[2];
     DWG_TRY(ix.c_count.reserve(ncell + 1));
     DWG_TRY(ix.c_start.reserve(ncell + 1));
@@ -964,6 +1024,12 @@ static int knn_query_cells(const KnnIndex& ix, const KnnArgs& a0, long long nq, 
     DWG_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(ix.c_scratch.ptr, bytes, cin, cout, (int)(ncell + 1), s));
     DWG_CHECK_CUDA(cudaMemcpyAsync(ix.c_fill.ptr, ix.c_start.ptr, sizeof(int) * (ncell + 1), cudaMemcpyDeviceToDevice, s));
     k_cq_active<<<div_up(ncell, 256), 256, 0, s>>>(ix.c_count.ptr, ncell, ix.c_active.ptr, ix.c_misc.ptr);
+    if (ix.kb_per_query) {
+        DWG_TRY(ix.kb.reserve(ncell));
+        KnnGrid g{ix.G[0], ix.G[1], ix.G[2], ix.lo[0], ix.lo[1], ix.lo[2], ix.h, ix.inv_h};
+        k_kb_active<<<num_sms() * 4, 128, 0, s>>>(g, ix.cell_start.ptr, ix.pts.ptr, ix.c_active.ptr, ix.c_misc.ptr,
+                                                  ix.kb.ptr);
+    }
     k_cq_scatter<<<(unsigned)blocks, 256, 0, s>>>(a, ix.q_key.ptr, ix.c_fill.ptr, ix.q_order.ptr);
     DWG_CHECK_LAUNCH();
     static int bps = 0;
@@ -1043,8 +1109,15 @@ int knn_build_subset(const KnnIndex& full, const unsigned char* exclude, KnnInde
                                                   sub.cell_start.ptr, sub.pts.ptr);
     DWG_CHECK_LAUNCH();
     DWG_TRY(pyramid_fill(sub, s));
+    // the subset changes between queries.  The whole-grid bound (local blocks
+    // plus min-plus passes) costs in proportion to the grid, empty space
+    // included; past 2^22 cells the bounds of the queried cells alone are
+    // cheaper, at the price of sending the queries of sparse neighbourhoods
+    // to the per-thread search
     sub.kb_ready = false;
-    return build_kbound(sub, s);
+    sub.kb_per_query = ncell > (1ll << 22);
+    if (!sub.kb_per_query) return build_kbound(sub, s);
+    return DWG_OK;
 }
 
 constexpr int kKnnBuckets = 1 << 15;

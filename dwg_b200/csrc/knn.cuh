@@ -23,9 +23,12 @@ struct KnnIndex {
     long long loff[kMaxLevels] = {};
     DevBuf<unsigned char> occ;
     // kb[c] >= distance from the centre of cell c to its kKnnBoundK-th
-    // nearest point (built on the first cell-grouped query)
+    // nearest point: over the whole grid on the first cell-grouped query, or
+    // (kb_per_query, indexes rebuilt between queries) for the cells holding
+    // queries only, at every query
     mutable DevBuf<float> kb, kb_tmp;
     mutable bool kb_ready = false;
+    bool kb_per_query = false;
     // workspace of the cell-grouped queries
     mutable DevBuf<int> c_count, c_start, c_fill, c_active, c_misc, c_fb;
     mutable DevBuf<unsigned int> c_m;

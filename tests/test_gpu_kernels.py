@@ -370,3 +370,25 @@ def test_fwn_order2_closer_to_exact_on_gpu(oracle_lib):
         w = gt.TurboLibiGWNLaunch(Q_d, beta=2.0, order=order).cpu().numpy()
         rms.append(np.sqrt(np.mean((w - exact) ** 2)))
     assert rms[1] < rms[0] / 3
+
+
+def test_zero_repair_large_grid_bit_exact(oracle_lib, dwg_lib):
+    # a grid above 2^22 cells: the subset index bounds only the queried cells
+    # (radius-3 blocks, the rest to the per-thread search); a flagged cap of
+    # the sphere leaves its centre far from any unflagged point
+    rng = np.random.default_rng(12)
+    L = 600000
+    v = rng.standard_normal((L, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    Lpos = (0.45 * v).astype(np.float32)
+    N0 = rng.standard_normal((L, 3)).astype(np.float32)
+    N0 /= np.linalg.norm(N0, axis=1, keepdims=True)
+    isz = (v[:, 2] > 0.995) | (rng.random(L) < 0.002)
+    ref = oracle_lib.zero_repair(Lpos, N0, isz, 10)
+    pos_d, n_dev = cu(Lpos), cu(N0)
+    isz_d = cu(isz.astype(np.uint8))
+    zc = torch.tensor([int(isz.sum())], dtype=torch.int32, device=DEV)
+    ix = turbo.KnnIndex(pos_d)
+    capi.check(dwg_lib.dwg_zero_repair(ix._h, capi.ptr(n_dev), capi.ptr(isz_d), capi.ptr(zc), 10, 10, None))
+    torch.cuda.synchronize()
+    assert np.array_equal(n_dev.cpu().numpy(), ref)
