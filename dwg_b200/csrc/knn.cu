@@ -947,12 +947,32 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
                         cnt = a.cell_start[cell + 1] - s0;
                     }
                 }
-                const int mx = __reduce_max_sync(FULL, cnt);
-                for (int j = 0; j < mx; ++j) {
+                // the points of the 32 cells as one list that the lanes walk
+                // together, a lane per point (not a lane per cell, which
+                // would idle the warp on the fullest cell)
+                int incl = cnt;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(FULL, incl, o);
+                    if (lane >= o) incl += v;
+                }
+                const int excl = incl - cnt;
+                const int tot = __shfl_sync(FULL, incl, 31);
+                for (int pb = 0; pb < tot; pb += 32) {
+                    const int tp = pb + lane;
+                    // owner of list position tp: the last lane whose range starts at or before it
+                    int own = 0;
+#pragma unroll
+                    for (int st = 16; st > 0; st >>= 1) {
+                        const int e = __shfl_sync(FULL, excl, own + st);
+                        if (e <= tp) own += st;
+                    }
+                    const int os0 = __shfl_sync(FULL, s0, own);
+                    const int oex = __shfl_sync(FULL, excl, own);
                     bool keep = false;
                     float4 p = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (j < cnt) {
-                        p = a.pts[s0 + j];
+                    if (tp < tot) {
+                        p = a.pts[os0 + (tp - oex)];
                         const float px = p.x - x, py = p.y - y, pz = p.z - z;
                         keep = px * px + py * py + pz * pz <= R2;
                     }
