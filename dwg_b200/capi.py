@@ -91,6 +91,8 @@ _SIGS = {
     "dwg_pipeline_size": (_i, [_vp, C.c_char_p, C.POINTER(_ll)]),
     "dwg_pipeline_get": (_i, [_vp, C.c_char_p, _vp]),
     "dwg_pipeline_device_ptr": (_i, [_vp, C.c_char_p, C.POINTER(_vp)]),
+    "dwg_pipeline_create_sharded": (_i, [_vp, _vp, _i, C.POINTER(Params), _i, _i, _vp, _vp, _vp, C.POINTER(_vp)]),
+    "dwg_slab_range": (_i, [_i, _i, _i, C.POINTER(_i), C.POINTER(_i)]),
     "dwg_autotune": (_i, [_vp, _i, C.POINTER(Params), _f, _i, _i, _vp, C.POINTER(TuneResult)]),
     "dwg_batch_create": (_i, [_vp, _vp, _i, _vp, _vp, C.POINTER(_vp)]),
     "dwg_batch_destroy": (_i, [_vp]),
@@ -185,6 +187,10 @@ def default_params(**kw) -> Params:
             raise KeyError(k)
         setattr(p, k, v)
     return p
+
+
+# element-wise int64 sum over ranks: (user, buf_dev, count, stream) -> 0 on success
+EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p)
 
 
 def gwn_params(beta=2.3, sigma=10.0, screen=0.0015, screened=True, use_radii=False, precision=1,

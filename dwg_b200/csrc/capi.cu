@@ -451,6 +451,38 @@ int dwg_pipeline_create(const float* points_dev, const float* normals_dev, int n
     })
 }
 
+int dwg_pipeline_create_sharded(const float* points_dev, const float* normals_dev, int n, const dwg_params* params,
+                                int rank, int world, dwg_exchange_fn exchange, void* user, void* stream,
+                                dwg_pipeline** out) {
+    API_GUARD({
+        DWG_REQUIRE(out && params, "pipeline_create_sharded: null argument");
+        DWG_REQUIRE(world >= 1 && rank >= 0 && rank < world, "pipeline_create_sharded: bad rank %d of %d", rank,
+                    world);
+        *out = nullptr;
+        dwg_pipeline* o = new dwg_pipeline();
+        o->p.rank = rank;
+        o->p.world = world;
+        o->p.exchange = exchange;
+        o->p.exchange_user = user;
+        int st = o->p.setup(points_dev, normals_dev, n, *params, S(stream));
+        if (st != DWG_OK) {
+            delete o;
+            return st;
+        }
+        *out = o;
+        return DWG_OK;
+    })
+}
+
+int dwg_slab_range(int samples, int rank, int world, int* z0, int* nz) {
+    API_GUARD({
+        DWG_REQUIRE(z0 && nz && world >= 1 && rank >= 0 && rank < world && samples - 1 >= world,
+                    "slab_range: bad arguments (samples %d, rank %d of %d)", samples, rank, world);
+        slab_range(samples, rank, world, z0, nz);
+        return DWG_OK;
+    })
+}
+
 int dwg_pipeline_destroy(dwg_pipeline* p) {
     if (p) cudaStreamSynchronize(p->p.s);
     delete p;
@@ -481,10 +513,10 @@ int dwg_pipeline_size(dwg_pipeline* p, const char* what, long long* value) {
             *value = q.n;
         else if (!strcmp(what, "iterations"))
             *value = q.iter;
-        else if (!strcmp(what, "grid"))
-            *value = (long long)q.gres[0] * q.gres[1] * q.gres[2];
+        else if (!strcmp(what, "grid"))  // this rank's slab (the whole grid on one GPU)
+            *value = (long long)q.gres[0] * q.gres[1] * q.gnz;
         else if (!strcmp(what, "final_grid"))
-            *value = (long long)q.fres[0] * q.fres[1] * q.fres[2];
+            *value = (long long)q.fres[0] * q.fres[1] * q.fnz;
         else if (!strcmp(what, "triangles")) {
             DWG_REQUIRE(q.finalized, "pipeline_size: not finalized");
             unsigned long long T = 0;
@@ -515,7 +547,12 @@ int dwg_pipeline_get(dwg_pipeline* p, const char* what, void* dst) {
         if (!strcmp(what, "tri_count")) return it ? cp(q.tri_hist.ptr, sizeof(long long) * it) : DWG_OK;
         if (!strcmp(what, "zero_count")) return it ? cp(q.zero_hist.ptr, sizeof(int) * it) : DWG_OK;
         if (!strcmp(what, "terms")) return it ? cp(q.terms_hist.ptr, sizeof(unsigned long long) * it) : DWG_OK;
-        if (!strcmp(what, "field")) return cp(q.field.ptr, sizeof(float) * q.gres[0] * q.gres[1] * (size_t)q.gres[2]);
+        if (!strcmp(what, "field")) return cp(q.field.ptr, sizeof(float) * q.gres[0] * q.gres[1] * (size_t)q.gnz);
+        if (!strcmp(what, "slab")) {
+            const int v[4] = {q.gz0, q.gnz, q.fz0, q.fnz};
+            memcpy(dst, v, sizeof(v));
+            return DWG_OK;
+        }
         if (!strcmp(what, "grid_res")) {
             memcpy(dst, q.gres, sizeof(q.gres));
             return DWG_OK;
@@ -528,7 +565,7 @@ int dwg_pipeline_get(dwg_pipeline* p, const char* what, void* dst) {
         DWG_REQUIRE(q.finalized, "pipeline_get: '%s' needs finalize()", what);
         if (!strcmp(what, "point_nrm")) return cp(q.point_nrm.ptr, sizeof(float) * 3 * q.n);
         if (!strcmp(what, "final_field"))
-            return cp(q.final_field.ptr, sizeof(float) * q.fres[0] * q.fres[1] * (size_t)q.fres[2]);
+            return cp(q.final_field.ptr, sizeof(float) * q.fres[0] * q.fres[1] * (size_t)q.fnz);
         if (!strcmp(what, "final_iso")) return cp(q.final_iso.ptr, sizeof(float));
         if (!strcmp(what, "final_res")) {
             memcpy(dst, q.fres, sizeof(q.fres));

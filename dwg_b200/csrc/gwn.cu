@@ -125,6 +125,7 @@ struct GwnArgs {
     const float* __restrict__ q;
     long long nq;
     int rx, ry, rz;
+    int zoff;  // global z index of local sample 0 (grid slabs)
     float ox, oy, oz, h;
     int bx, by;  // bricks per row / column
     long long ngroups;
@@ -261,7 +262,7 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
             qi[u] = x + (long long)a.rx * (y + (long long)a.ry * z);
             qx[u] = fx;
             qy[u] = fy;
-            qz[u] = __fadd_rn(a.oz, __fmul_rn((float)z, a.h));
+            qz[u] = __fadd_rn(a.oz, __fmul_rn((float)(z + a.zoff), a.h));
         }
     } else {
 #pragma unroll
@@ -587,6 +588,7 @@ int gwn_eval(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, float*
         a.q = q.q;
         a.nq = q.nq;
         a.rx = a.ry = a.rz = 0;
+        a.zoff = 0;
         a.ox = a.oy = a.oz = a.h = 0.f;
         a.bx = a.by = 1;
         a.ngroups = (q.nq + 31) / 32;  // one point per lane
@@ -599,6 +601,7 @@ int gwn_eval(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, float*
     a.rx = q.res[0];
     a.ry = q.res[1];
     a.rz = q.res[2];
+    a.zoff = q.zoff;
     a.ox = q.origin[0];
     a.oy = q.origin[1];
     a.oz = q.origin[2];
@@ -630,6 +633,7 @@ static void fill_args(GwnArgs& a, const Octree& t, const GwnBatchItem& it, const
     a.rx = it.res[0];
     a.ry = it.res[1];
     a.rz = it.res[2];
+    a.zoff = 0;
     a.nq = (long long)a.rx * a.ry * a.rz;
     a.ox = it.origin[0];
     a.oy = it.origin[1];

@@ -13,6 +13,7 @@ struct GwnQuery {
     int res[3] = {0, 0, 0};
     float origin[3] = {0, 0, 0};
     float spacing = 0;
+    int zoff = 0;  // grid: z index of the first sample (a slab of a larger grid)
 };
 
 // out[i] = w(q_i); terms_total (nullable) += number of evaluated terms;

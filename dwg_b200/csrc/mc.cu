@@ -173,6 +173,7 @@ struct McArgs {
     int rx, ry, rz;
     long long ncell;
     float ox, oy, oz, h;
+    int zoff;  // global z index of local sample 0
     float iso;
     const float* iso_dev;
 };
@@ -249,7 +250,7 @@ __global__ void __launch_bounds__(kMcThreads)
         } else {
             p[c][0] = __fadd_rn(a.ox, __fmul_rn((float)gx, a.h));
             p[c][1] = __fadd_rn(a.oy, __fmul_rn((float)gy, a.h));
-            p[c][2] = __fadd_rn(a.oz, __fmul_rn((float)gz, a.h));
+            p[c][2] = __fadd_rn(a.oz, __fmul_rn((float)(gz + a.zoff), a.h));
         }
     }
     const unsigned emask = c_edges[ci];
@@ -322,6 +323,7 @@ int mc_run(const float* field, const McGrid& g, float iso, const float* iso_dev,
     a.ox = g.origin[0];
     a.oy = g.origin[1];
     a.oz = g.origin[2];
+    a.zoff = g.zoff;
     a.h = g.spacing;
     a.iso = iso;
     a.iso_dev = iso_dev;
@@ -445,6 +447,7 @@ extern "C" int dwg_marching_cubes_noalloc(const float* field_dev, const int res[
     a.ox = origin ? origin[0] : 0.f;
     a.oy = origin ? origin[1] : 0.f;
     a.oz = origin ? origin[2] : 0.f;
+    a.zoff = 0;
     a.h = spacing;
     a.iso = iso;
     a.iso_dev = nullptr;

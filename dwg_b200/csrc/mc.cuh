@@ -10,6 +10,7 @@ struct McGrid {
     float origin[3];
     float spacing;
     const float* positions = nullptr;  // optional materialised sample positions
+    int zoff = 0;                      // z index of the first sample (a slab of a larger grid)
 };
 
 struct McWorkspace {

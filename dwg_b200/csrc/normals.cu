@@ -83,19 +83,31 @@ __global__ void k_finalize(long long* __restrict__ acc, int L, float* __restrict
     if ((threadIdx.x & 31) == 0 && m && zero_count) atomicAdd(zero_count, __popc(m));
 }
 
-int diffuse_normals(const int* knn, const float* tn, long long T, const unsigned long long* Tdev, int k, int L,
-                    float* N, long long* acc, unsigned char* is_zero, int* zero_count, cudaStream_t s) {
-    DWG_REQUIRE(knn && tn && N && acc && L >= 1 && k >= 1, "diffuse_normals: bad arguments");
-    if (zero_count) DWG_CHECK_CUDA(cudaMemsetAsync(zero_count, 0, sizeof(int), s));
+int diffuse_scatter(const int* knn, const float* tn, long long T, const unsigned long long* Tdev, int k, int L,
+                    long long* acc, cudaStream_t s) {
+    DWG_REQUIRE(knn && tn && acc && L >= 1 && k >= 1, "diffuse_normals: bad arguments");
     if (T > 0) {
         long long blocks = (T * k + 255) / 256;
         long long cap = (long long)num_sms() * 16;
         if (blocks > cap) blocks = cap;
         k_scatter<<<(unsigned)blocks, 256, 0, s>>>(knn, tn, T, Tdev, k, L, (unsigned long long*)acc);
+        DWG_CHECK_LAUNCH();
     }
+    return DWG_OK;
+}
+
+int diffuse_finish(int L, float* N, long long* acc, unsigned char* is_zero, int* zero_count, cudaStream_t s) {
+    DWG_REQUIRE(N && acc && L >= 1, "diffuse_normals: bad arguments");
+    if (zero_count) DWG_CHECK_CUDA(cudaMemsetAsync(zero_count, 0, sizeof(int), s));
     k_finalize<<<div_up(L, 256), 256, 0, s>>>(acc, L, N, is_zero, zero_count);
     DWG_CHECK_LAUNCH();
     return DWG_OK;
+}
+
+int diffuse_normals(const int* knn, const float* tn, long long T, const unsigned long long* Tdev, int k, int L,
+                    float* N, long long* acc, unsigned char* is_zero, int* zero_count, cudaStream_t s) {
+    DWG_TRY(diffuse_scatter(knn, tn, T, Tdev, k, L, acc, s));
+    return diffuse_finish(L, N, acc, is_zero, zero_count, s);
 }
 
 // SimpleUpdateNonzeroNormals (src/TurboDWG.cu:322-359)

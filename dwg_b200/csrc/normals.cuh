@@ -15,6 +15,12 @@ int gauss_map(const float* P, int n, float* normals, cudaStream_t s);
 int diffuse_normals(const int* knn, const float* tri_normals, long long num_tris,
                     const unsigned long long* num_tris_dev, int k, int L, float* normals,
                     long long* acc, unsigned char* is_zero, int* zero_count, cudaStream_t s);
+// the two halves of diffuse_normals: the scatter into acc, and the
+// normalisation that reads and clears it; between them the accumulators of
+// several ranks can be summed (integers: the sum is exact in any order)
+int diffuse_scatter(const int* knn, const float* tri_normals, long long num_tris,
+                    const unsigned long long* num_tris_dev, int k, int L, long long* acc, cudaStream_t s);
+int diffuse_finish(int L, float* normals, long long* acc, unsigned char* is_zero, int* zero_count, cudaStream_t s);
 
 struct ZeroRepairWs {
     KnnIndex sub;  // the unflagged points, rebuilt per call

@@ -206,6 +206,22 @@ __global__ void k_iter_end(int* __restrict__ iter, const unsigned long long* __r
     *iter = t + 1;
 }
 
+__global__ void k_put_count(const unsigned long long* __restrict__ ntri, long long* __restrict__ slot) {
+    *slot = (long long)*ntri;
+}
+
+__global__ void k_get_count(long long* __restrict__ slot, unsigned long long* __restrict__ ntri) {
+    *ntri = (unsigned long long)*slot;
+    *slot = 0;
+}
+
+void slab_range(int samples, int rank, int world, int* z0, int* nz) {
+    const long long cells = samples - 1;
+    const long long c0 = cells * rank / world, c1 = cells * (rank + 1) / world;
+    *z0 = (int)c0;
+    *nz = (int)(c1 - c0 + 1);
+}
+
 // ------------------------------------------------------------------ setup --
 Pipeline::~Pipeline() {
     if (s) cudaStreamSynchronize(s);
@@ -304,6 +320,8 @@ int Pipeline::setup(const float* points_dev, const float* normals_dev, int n_poi
     const bool pca = p.com_as && p.in_normal != 1;
     DWG_REQUIRE(p.in_normal >= 3 || pca || normals_dev, "pipeline: in_normal %d needs input normals", p.in_normal);
     DWG_REQUIRE(p.in_normal != 4 || init_mlp, "pipeline: in_normal 4 needs a learned initialiser");
+    DWG_REQUIRE(world >= 1 && rank >= 0 && rank < world, "pipeline: bad rank %d of %d", rank, world);
+    DWG_REQUIRE(world == 1 || exchange, "pipeline: a sharded pipeline needs an exchange function");
     prm = p;
     caller = stream;
     DWG_CHECK_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
@@ -417,17 +435,26 @@ int Pipeline::setup(const float* points_dev, const float* normals_dev, int n_poi
     if (p.in_normal == 4) DWG_TRY(mlp_init_normals(*init_mlp, kidx, leaf_pos.ptr, L, leaf_nrm.ptr, s));
     k_set_nr<<<div_up(L, 256), 256, 0, s>>>(t2.nr.ptr, leaf_nrm.ptr, leaf_rad.ptr, L);
     DWG_CHECK_LAUNCH();
+    // this rank's z-slab of the grid (the whole grid on one GPU)
+    DWG_REQUIRE(world <= gres[2] - 1, "pipeline: %d ranks for %d grid cells in z", world, gres[2] - 1);
+    if (world > 1) {
+        slab_range(gres[2], rank, world, &gz0, &gnz);
+    } else {
+        gz0 = 0;
+        gnz = gres[2];
+    }
     // buffers of one iteration
     long long ng = (long long)gres[0] * gres[1] * gres[2];
     cap = ng / 2 > 1000000 ? ng / 2 : 1000000;  // src/TurboDWG.cu:466
-    DWG_TRY(field.reserve(ng));
+    DWG_TRY(field.reserve((size_t)gres[0] * gres[1] * gnz));
     DWG_TRY(wleaf.reserve(L));
     DWG_TRY(cent.reserve((size_t)cap * 3));
     DWG_TRY(tnrm.reserve((size_t)cap * 3));
     DWG_TRY(ntri.reserve(1));
     DWG_TRY(knn_buf.reserve((size_t)cap * p.knn_tri));
-    DWG_TRY(acc.reserve((size_t)L * 3));
-    DWG_CHECK_CUDA(cudaMemsetAsync(acc.ptr, 0, sizeof(long long) * 3 * L, s));
+    // 3 L fixed-point normal sums and, for the exchange, one triangle count
+    DWG_TRY(acc.reserve((size_t)L * 3 + 1));
+    DWG_CHECK_CUDA(cudaMemsetAsync(acc.ptr, 0, sizeof(long long) * (3 * (size_t)L + 1), s));
     DWG_TRY(is_zero.reserve(L));
     DWG_TRY(zero_count.reserve(1));
     DWG_CHECK_CUDA(cudaMemsetAsync(zero_count.ptr, 0, sizeof(int), s));
@@ -481,6 +508,8 @@ int Pipeline::iterate_grid() {
         qg.res[d] = gres[d];
         qg.origin[d] = gorg[d];
     }
+    qg.res[2] = gnz;
+    qg.zoff = gz0;
     qg.spacing = gh;
     return gwn_eval(t2, qg, gwn_params(), field.ptr, terms_cur.ptr, nullptr, s, cur_sigma.ptr);
 }
@@ -493,6 +522,8 @@ int Pipeline::iterate_post() {
         g.res[d] = gres[d];
         g.origin[d] = gorg[d];
     }
+    g.res[2] = gnz;
+    g.zoff = gz0;
     g.spacing = gh;
     DWG_TRY(mc_run(field.ptr, g, 0.f, iso_dev.ptr, nullptr, cent.ptr, tnrm.ptr, cap, ntri.ptr, mcws, s));
     // k nearest leaves of every triangle centroid (:560-569)
@@ -501,13 +532,35 @@ int Pipeline::iterate_post() {
     q.nq = cap;
     q.nq_dev = ntri.ptr;
     DWG_TRY(knn_query(kidx, q, prm.knn_tri, knn_buf.ptr, s));
-    // normal scatter + normalise (:571-583)
-    DWG_TRY(diffuse_normals(knn_buf.ptr, tnrm.ptr, cap, ntri.ptr, prm.knn_tri, L, leaf_nrm.ptr, acc.ptr,
-                            is_zero.ptr, zero_count.ptr, s));
+    // normal scatter + normalise (:571-583); sharded: the scatter of this
+    // rank's triangles, the sums of all ranks, then the normalisation
+    if (world > 1) {
+        DWG_TRY(diffuse_scatter(knn_buf.ptr, tnrm.ptr, cap, ntri.ptr, prm.knn_tri, L, acc.ptr, s));
+        DWG_TRY(exchange_sums());
+        DWG_TRY(diffuse_finish(L, leaf_nrm.ptr, acc.ptr, is_zero.ptr, zero_count.ptr, s));
+    } else {
+        DWG_TRY(diffuse_normals(knn_buf.ptr, tnrm.ptr, cap, ntri.ptr, prm.knn_tri, L, leaf_nrm.ptr, acc.ptr,
+                                is_zero.ptr, zero_count.ptr, s));
+    }
     // zero-normal repair when more than knn_zero points are zero (:585-644)
     DWG_TRY(zero_repair(kidx, leaf_pos.ptr, L, leaf_nrm.ptr, is_zero.ptr, prm.knn_zero, prm.knn_zero, zws, s));
     k_iter_end<<<1, 1, 0, s>>>(iter_dev.ptr, ntri.ptr, cap, zero_count.ptr, terms_cur.ptr, tri_hist.ptr,
                                zero_hist.ptr, terms_hist.ptr);
+    DWG_CHECK_LAUNCH();
+    return DWG_OK;
+}
+
+// the fixed-point normal sums and the triangle count of all ranks: acc[3L]
+// carries this rank's count out and the total back (the exchange is a host
+// call, so the stream is drained first)
+int Pipeline::exchange_sums() {
+    long long* slot = acc.ptr + 3 * (size_t)L;
+    k_put_count<<<1, 1, 0, s>>>(ntri.ptr, slot);
+    DWG_CHECK_LAUNCH();
+    DWG_CHECK_CUDA(cudaStreamSynchronize(s));
+    const int rc = exchange(exchange_user, acc.ptr, 3 * (long long)L + 1, (void*)s);
+    DWG_REQUIRE(rc == 0, "pipeline: the exchange of rank %d failed (%d)", rank, rc);
+    k_get_count<<<1, 1, 0, s>>>(slot, ntri.ptr);
     DWG_CHECK_LAUNCH();
     return DWG_OK;
 }
@@ -524,7 +577,8 @@ int Pipeline::iterate(int n_iters) {
     DWG_TRY(ensure_hist(iter + n_iters));
     DWG_TRY(join_in());
     for (int k = 0; k < n_iters; ++k) {
-        if (prm.use_graph && iter > 0) {
+        // a sharded iteration calls the host exchange: no graph
+        if (prm.use_graph && iter > 0 && world == 1) {
             if (!graph_exec) {
                 DWG_CHECK_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
                 int st = iterate_once();
@@ -643,12 +697,21 @@ int Pipeline::finalize() {
     ql.nq = nqp;
     DWG_TRY(gwn_eval(*tree, ql, gp, wfin.ptr, nullptr, nullptr, s));
     long long ng = (long long)fres[0] * fres[1] * fres[2];
-    DWG_TRY(final_field.reserve(ng));
+    DWG_REQUIRE(world <= fres[2] - 1, "pipeline: %d ranks for %d final grid cells in z", world, fres[2] - 1);
+    if (world > 1) {
+        slab_range(fres[2], rank, world, &fz0, &fnz);
+    } else {
+        fz0 = 0;
+        fnz = fres[2];
+    }
+    DWG_TRY(final_field.reserve((size_t)fres[0] * fres[1] * fnz));
     GwnQuery qg;
     for (int d = 0; d < 3; ++d) {
         qg.res[d] = fres[d];
         qg.origin[d] = forg[d];
     }
+    qg.res[2] = fnz;
+    qg.zoff = fz0;
     qg.spacing = fh;
     DWG_TRY(gwn_eval(*tree, qg, gp, final_field.ptr, nullptr, nullptr, s));
     DWG_TRY(mean_to_iso(wfin.ptr, nqp, final_iso.ptr, nullptr, nullptr, nullptr, partial, s));
@@ -659,6 +722,8 @@ int Pipeline::finalize() {
         g.res[d] = fres[d];
         g.origin[d] = forg[d];
     }
+    g.res[2] = fnz;
+    g.zoff = fz0;
     g.spacing = fh;
     DWG_TRY(mc_run(final_field.ptr, g, 0.f, final_iso.ptr, tris.ptr, nullptr, nullptr, final_cap, final_ntri.ptr,
                    mcws, s));

@@ -11,6 +11,15 @@
 
 namespace dwg {
 
+// element-wise int64 sum over the ranks of a sharded reconstruction, in place
+// (the same call on every rank, in the same order); 0 on success
+typedef int (*ExchangeFn)(void* user, long long* buf_dev, long long count, void* stream);
+
+// the z-slab of rank `rank` of `world` in a grid of `samples` z-samples: the
+// samples - 1 cells are split into contiguous runs, a run of cells c0 .. c1-1
+// needs samples c0 .. c1 (one shared boundary layer)
+void slab_range(int samples, int rank, int world, int* z0, int* nz);
+
 struct Pipeline {
     dwg_params prm;
     Mlp* init_mlp = nullptr;        // learned initialiser of in_normal 4 (used during setup only)
@@ -54,6 +63,14 @@ struct Pipeline {
     // final pass
     bool finalized = false;
     int fres[3] = {0, 0, 0};
+    // z-slab sharding: this rank evaluates and meshes the z-samples gz0 ..
+    // gz0 + gnz - 1 of the iteration grid (fz0, fnz: the final grid); the
+    // normal accumulators and the triangle count are summed over the ranks
+    // once per iteration, everything else is replicated
+    int rank = 0, world = 1;
+    ExchangeFn exchange = nullptr;
+    void* exchange_user = nullptr;
+    int gz0 = 0, gnz = 0, fz0 = 0, fnz = 0;
     float forg[3] = {0, 0, 0};
     float fh = 0;
     DevBuf<float> final_field, point_nrm, tris, wfin, p_sorted, pt_rad;
@@ -71,6 +88,7 @@ struct Pipeline {
     int iterate_pre();
     int iterate_grid();
     int iterate_post();
+    int exchange_sums();
     dwg_gwn_params gwn_params() const;
     int finalize();
     int ensure_hist(int total);

@@ -428,6 +428,99 @@ class LearnedNormalInit:
             pass
 
 
+class _DeviceInt64:
+    """__cuda_array_interface__ of an int64 device buffer (a torch view, no copy)."""
+
+    def __init__(self, ptr, count):
+        self.__cuda_array_interface__ = {"shape": (int(count),), "typestr": "<i8", "data": (int(ptr), False),
+                                         "version": 2}
+
+
+def exchange_tensor(t, group=None):
+    """Element-wise sum of an int64 tensor over the ranks of ``group``, in
+    place: NCCL sums device memory directly, other backends (gloo) a host copy."""
+    import torch.distributed as dist
+    if t.is_cuda and dist.get_backend(group) == "nccl":
+        dist.all_reduce(t, group=group)
+        torch.cuda.synchronize()
+    elif t.is_cuda:
+        h = t.cpu()
+        dist.all_reduce(h, group=group)
+        t.copy_(h)
+        torch.cuda.synchronize()
+    else:
+        dist.all_reduce(t, group=group)
+    return t
+
+
+def torch_exchange(group=None):
+    """The exchange function of a sharded pipeline over torch.distributed
+    (keep the returned object alive while the pipeline runs)."""
+    def fn(user, buf, count, stream):
+        try:
+            torch.cuda.synchronize()
+            exchange_tensor(torch.as_tensor(_DeviceInt64(buf, count), device="cuda"), group)
+            return 0
+        except Exception as e:  # reported as a failed exchange by the library
+            print(f"dwg_b200 exchange failed: {e}", flush=True)
+            return 1
+    return capi.EXCHANGE_FN(fn)
+
+
+def slab_range(samples, rank, world):
+    """z-samples (first, count) of rank ``rank``'s slab of a grid with ``samples`` z-samples."""
+    z0, nz = C.c_int(), C.c_int()
+    capi.check(capi.load().dwg_slab_range(int(samples), int(rank), int(world), C.byref(z0), C.byref(nz)))
+    return z0.value, nz.value
+
+
+def reconstruct_sharded(points, rank, world, exchange, normals=None, **flags):
+    """Rank ``rank`` of a z-slab sharded reconstruction of one cloud (one
+    process per GPU, ``exchange`` from :func:`torch_exchange`): leaf normals,
+    iso values and triangle counts are those of the whole run, ``tris`` and
+    ``final_field`` this rank's slab (``slab``: first z-sample and count of
+    the iteration grid, then of the final grid)."""
+    _req_cuda_f32(points, "points", 3)
+    prm = capi.default_params(**flags)
+    h = C.c_void_p()
+    lib = capi.load()
+    capi.check(lib.dwg_pipeline_create_sharded(capi.ptr(points), capi.ptr(normals), points.shape[0], C.byref(prm),
+                                               int(rank), int(world), exchange, None, capi.stream_ptr(),
+                                               C.byref(h)))
+    try:
+        capi.check(lib.dwg_pipeline_iterate(h, prm.total_iter))
+        capi.check(lib.dwg_pipeline_finalize(h))
+        out = {}
+
+        def get(what, shape, dtype):
+            a = np.empty(shape, dtype)
+            if a.size:
+                capi.check(lib.dwg_pipeline_get(h, what.encode(), a.ctypes.data))
+            return a
+
+        def size(what):
+            v = C.c_longlong()
+            capi.check(lib.dwg_pipeline_size(h, what.encode(), C.byref(v)))
+            return v.value
+
+        L, it = size("leaves"), size("iterations")
+        out["leaf_pos"] = get("leaf_pos", (L, 3), np.float32)
+        out["leaf_nrm"] = get("leaf_nrm", (L, 3), np.float32)
+        out["iso"] = get("iso", (it,), np.float32)
+        out["tri_count"] = get("tri_count", (it,), np.int64)
+        out["zero_count"] = get("zero_count", (it,), np.int32)
+        out["tris"] = get("tris", (size("triangles"), 9), np.float32)
+        out["final_iso"] = get("final_iso", (1,), np.float32)
+        out["final_res"] = get("final_res", (3,), np.int32)
+        out["final_field"] = get("final_field", (size("final_grid"),), np.float32)
+        out["slab"] = get("slab", (4,), np.int32)
+        if not prm.use_leaves_generate:
+            out["point_nrm"] = get("point_nrm", (size("points"), 3), np.float32)
+        return out
+    finally:
+        lib.dwg_pipeline_destroy(h)
+
+
 def reconstruct(points, normals=None, init_model=None, **flags):
     """Full reconstruction on the GPU; returns a dict of host arrays."""
     d = TurboDWG(points, normals, init_model=init_model, **flags)

@@ -305,6 +305,33 @@ int dwg_pipeline_get(dwg_pipeline* p, const char* what, void* dst_host);
 int dwg_pipeline_device_ptr(dwg_pipeline* p, const char* what, void** ptr);
 
 /* ------------------------------------------------------------------------
+ * One cloud on several GPUs: z-slab sharding (one process per GPU).  The
+ * reference runs one cloud on one GPU; here rank r of `world` evaluates the
+ * winding number and marching cubes only on its run of z-cells of each grid
+ * (the samples of the run and the shared boundary layer) and finds the
+ * neighbours of its own triangles; octrees, leaves, the leaf sums, the iso
+ * value and the zero repair are replicated.  Once per iteration the 3 L
+ * fixed-point normal sums and the triangle count (3 L + 1 int64) are summed
+ * over the ranks by `exchange`; integer sums are exact in any order, so every
+ * rank ends each iteration with the leaf normals of a one-GPU run, bit for
+ * bit, and the ranks' meshes concatenated in rank order are the one-GPU mesh.
+ * `exchange` is called on every rank in the same order with no pipeline work
+ * in flight; it must replace buf_dev[0..count) by the element-wise sum over
+ * the ranks before it returns (e.g. ncclAllReduce + stream synchronise) and
+ * return 0.  Iterations run without a CUDA graph.  Sizes and arrays of the
+ * pipeline ("grid", "field", "final_grid", "final_field", "triangles",
+ * "tris") are this rank's; "slab" (int32[4]: first z-sample and count of the
+ * iteration grid, then of the final grid) locates them; "tri_count" is the
+ * total. */
+typedef int (*dwg_exchange_fn)(void* user, long long* buf_dev, long long count, void* stream);
+int dwg_pipeline_create_sharded(const float* points_dev, const float* normals_dev, int n,
+                                const dwg_params* params, int rank, int world, dwg_exchange_fn exchange,
+                                void* user, void* stream, dwg_pipeline** out);
+/* the slab of rank `rank`: z-samples z0 .. z0 + nz - 1 of a grid of `samples`
+ * z-samples (the samples - 1 cells split into `world` contiguous runs) */
+int dwg_slab_range(int samples, int rank, int world, int* z0, int* nz);
+
+/* ------------------------------------------------------------------------
  * Batched reconstruction of many clouds (no counterpart in the reference,
  * which reconstructs one cloud per DWG_CUDA run).  Each cloud is a pipeline
  * with its own flags (params[i]; in_normal 3, one tile and one precision for
