@@ -204,7 +204,8 @@ int dwg_gwn_points(dwg_octree* tree, const float* normals_dev, const float* area
                    const float* queries_dev, long long num_queries, const dwg_gwn_params* params, float* out_dev,
                    unsigned long long* terms_dev, void* stream) {
     API_GUARD({
-        DWG_REQUIRE(queries_dev && num_queries >= 0, "gwn_points: bad queries");
+        DWG_REQUIRE(tree && params && num_queries >= 0 && (queries_dev || num_queries == 0), "gwn_points: bad queries");
+        if (num_queries == 0) return DWG_OK;  // an empty query set (its pointers may be null)
         GwnQuery q;
         q.q = queries_dev;
         q.nq = num_queries;
@@ -217,7 +218,8 @@ int dwg_gwn_points_counted(dwg_octree* tree, const float* normals_dev, const flo
                            const float* radii_dev, const float* queries_dev, long long num_queries,
                            const dwg_gwn_params* params, float* out_dev, int* per_query_terms_dev, void* stream) {
     API_GUARD({
-        DWG_REQUIRE(queries_dev && num_queries >= 0, "gwn_points: bad queries");
+        DWG_REQUIRE(tree && params && num_queries >= 0 && (queries_dev || num_queries == 0), "gwn_points: bad queries");
+        if (num_queries == 0) return DWG_OK;
         GwnQuery q;
         q.q = queries_dev;
         q.nq = num_queries;
@@ -314,8 +316,10 @@ int dwg_knn_destroy(dwg_knn_index* index) {
 int dwg_knn_query(dwg_knn_index* index, const float* queries_dev, long long num_queries, int k, int* out_dev,
                   void* stream) {
     API_GUARD({
-        DWG_REQUIRE(index && queries_dev && out_dev, "knn_query: null argument");
-        DWG_REQUIRE(k <= index->ix.n, "knn_query: k=%d exceeds the number of points %d", k, index->ix.n);
+        DWG_REQUIRE(index && num_queries >= 0 && ((queries_dev && out_dev) || num_queries == 0),
+                    "knn_query: null argument");
+        DWG_REQUIRE(k >= 1 && k <= index->ix.n, "knn_query: k=%d outside [1, %d points]", k, index->ix.n);
+        if (num_queries == 0) return DWG_OK;  // an empty query set (its pointers may be null)
         KnnQuery q;
         q.q = queries_dev;
         q.nq = num_queries;

@@ -129,6 +129,7 @@ static int build_pyramid(KnnIndex& ix, cudaStream_t s) {
 
 int knn_build(KnnIndex& ix, const float* P, int n, cudaStream_t s) {
     DWG_REQUIRE(P != nullptr && n >= 1, "knn: need at least one point (n=%d)", n);
+    DWG_TRY(require_finite(P, 3ll * n, "knn", s));
     ix.n = n;
     DWG_TRY(ix.bbox.reserve(6));
     DWG_TRY(bbox_device(P, n, ix.bbox.ptr, s));

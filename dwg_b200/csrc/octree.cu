@@ -72,6 +72,29 @@ int bbox_device(const float* points_dev, long long n, float* out_dev, cudaStream
 }
 
 // root cube: AABB centre, width = largest extent, in FP64 (octree.cpp:306-316)
+__global__ void k_nonfinite(const float* __restrict__ x, long long m, unsigned int* __restrict__ flag) {
+    unsigned int bad = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m; i += (long long)gridDim.x * blockDim.x)
+        bad |= isfinite(x[i]) ? 0u : 1u;
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1u);
+}
+
+int require_finite(const float* x, long long m, const char* what, cudaStream_t s) {
+    if (m <= 0) return DWG_OK;
+    DevBuf<unsigned int> flag;
+    DWG_TRY(flag.reserve(1));
+    DWG_CHECK_CUDA(cudaMemsetAsync(flag.ptr, 0, sizeof(unsigned int), s));
+    long long blocks = (m + 255) / 256;
+    if (blocks > (long long)num_sms() * 8) blocks = (long long)num_sms() * 8;
+    k_nonfinite<<<(unsigned)blocks, 256, 0, s>>>(x, m, flag.ptr);
+    DWG_CHECK_LAUNCH();
+    unsigned int h = 0;
+    DWG_CHECK_CUDA(cudaMemcpyAsync(&h, flag.ptr, sizeof(h), cudaMemcpyDeviceToHost, s));
+    DWG_CHECK_CUDA(cudaStreamSynchronize(s));
+    DWG_REQUIRE(h == 0, "%s: non-finite coordinate (NaN or infinity) in the input", what);
+    return DWG_OK;
+}
+
 __global__ void k_root(const float* __restrict__ bb, double* __restrict__ root) {
     double w = 0;
     for (int d = 0; d < 3; d++) {
@@ -522,6 +545,8 @@ static int cub_call(DevBuf<unsigned char>& scratch, F&& f) {
 int octree_build(Octree& t, const float* P, int n, int D, const float* A, cudaStream_t s) {
     DWG_REQUIRE(n >= 1, "octree: need at least one point (n=%d)", n);
     DWG_REQUIRE(D >= 1 && D <= kMaxDepth, "octree: max_depth must be in [1, %d] (got %d)", kMaxDepth, D);
+    DWG_REQUIRE(P != nullptr, "octree: null points");
+    DWG_TRY(require_finite(P, 3ll * n, "octree", s));
     t.n = n;
     t.max_depth = D;
     DevBuf<float> bb;

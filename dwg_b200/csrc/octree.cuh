@@ -86,6 +86,9 @@ int octree_set_beta(Octree& t, float beta, cudaStream_t s);
 int octree_leaf_centres(Octree& t, int min_count, DevBuf<float>& out_xyz, DevBuf<int>& out_node,
                         int* num_leaves, cudaStream_t s);
 
+// DWG_ERR_INVALID when x[0..m) holds a NaN or an infinity (synchronises s)
+int require_finite(const float* x, long long m, const char* what, cudaStream_t s);
+
 // bounding box of float3 points: out[0..2] = min, out[3..5] = max (device)
 int bbox_device(const float* points_dev, long long n, float* out_dev, cudaStream_t s);
 

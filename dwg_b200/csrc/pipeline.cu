@@ -363,6 +363,15 @@ int Pipeline::setup(const float* points_dev, const float* normals_dev, int n_poi
     DevBuf<int> raw_node;
     DWG_TRY(octree_leaf_centres(t1, p.min_num, raw_pos, raw_node, &L, s));
     DWG_REQUIRE(L >= 2, "pipeline: fewer than 2 octree leaves (%d)", L);
+    // every neighbour query needs at least k leaves (points for the final radii)
+    {
+        int kmax = p.knn_tri > p.knn_zero ? p.knn_tri : p.knn_zero;
+        if (!p.use_leaves_generate && p.normal_kw > kmax) kmax = p.normal_kw;
+        if (p.use_radii && p.kw > kmax) kmax = p.kw;
+        DWG_REQUIRE(L >= kmax, "pipeline: %d octree leaves, fewer than the %d neighbours a query needs", L, kmax);
+        DWG_REQUIRE(!p.use_radii || p.use_leaves_generate || n >= p.final_kw,
+                    "pipeline: %d points, fewer than final_kw = %d", n, p.final_kw);
+    }
     // octree on the leaves; its sorted order is the canonical leaf order
     DWG_TRY(leaf_area.reserve(L));
     k_fill<<<div_up(L, 256), 256, 0, s>>>(leaf_area.ptr, L, p.area);
