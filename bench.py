@@ -520,7 +520,8 @@ def farfield_report(a, lib, capi, turbo, torch, dev):
 
 
 def learned_report(a, lib, capi, turbo, torch, dev):
-    """Plain (Gauss map) vs learned start on the bench cloud: orientation
+    """Plain (Gauss map) vs learned start on the bench cloud, beside the true
+    normals as the start (the best any initialiser can do): orientation
     agreement of the initial leaf normals with the true normals, and the RMS
     distance of each iteration's grid field to the plain method's field after
     all iterations (sign-matched: the orientation flips every iteration)."""
@@ -539,10 +540,15 @@ def learned_report(a, lib, capi, turbo, torch, dev):
     nb = turbo.KnnIndex(Pd).query(leaves, 1).cpu().numpy()[:, 0]
     truth = Ntrue[nb]
     out = {"weights": os.path.relpath(DEFAULT_WEIGHTS, ROOT), "reference_field": f"plain start after {a.iters} iterations"}
-    for name, m in (("plain", None), ("learned", model)):
+    # the true normals as the start (in_normal 1) bound what any initialiser can gain
+    Nd = torch.from_numpy(np.ascontiguousarray(Ntrue, np.float32)).to(dev)
+    for name, m, nrm in (("plain", None, None), ("learned", model, None), ("true_normals", None, Nd)):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        d = turbo.TurboDWG(Pd, None, init_model=m, **flags)
+        if nrm is None:
+            d = turbo.TurboDWG(Pd, None, init_model=m, **flags)
+        else:
+            d = turbo.TurboDWG(Pd, nrm, **dict(flags, in_normal=1))
         torch.cuda.synchronize()
         create_ms = (time.perf_counter() - t0) * 1e3
         n0 = d.get("leaf_nrm")
