@@ -40,7 +40,7 @@ class Params(C.Structure):
         ("offset_1", C.c_float), ("offset_2", C.c_float), ("use_leaves_generate", C.c_int),
         ("total_iter", C.c_int), ("beta", C.c_float), ("area", C.c_float), ("screen", C.c_float),
         ("knn_tri", C.c_int), ("knn_zero", C.c_int), ("precision", C.c_int), ("use_graph", C.c_int),
-        ("tile", C.c_int), ("as_thres", C.c_float), ("com_as", C.c_int),
+        ("tile", C.c_int), ("as_thres", C.c_float), ("com_as", C.c_int), ("grid_lists", C.c_int),
     ]
 
 

@@ -437,6 +437,7 @@ void dwg_params_default(dwg_params* p) {
     p->tile = 0;
     p->as_thres = 0.f;
     p->com_as = 0;
+    p->grid_lists = 1;
 }
 
 int dwg_pipeline_create(const float* points_dev, const float* normals_dev, int n, const dwg_params* params,

@@ -11,6 +11,8 @@
 // FP32; each query's sum is FP32 (precision 0) or FP64 (precision >= 1).
 #include "gwn.cuh"
 
+#include <cub/cub.cuh>
+
 #include <vector>
 
 namespace dwg {
@@ -135,6 +137,11 @@ struct GwnArgs {
     unsigned int* work;  // [0] counter, [1] error flags (sticky)
     int num_nodes, num_points;
     const float4* __restrict__ node_h;  // expansion records, 8 float4 each (plain sums, order >= 1)
+    // interaction lists (grids): per-group entry counts (counting pass), the
+    // groups' first entries (ngroups + 1) and the entries
+    unsigned int* list_count;
+    const unsigned long long* __restrict__ list_off;
+    int4* list;
 };
 
 template <bool SCREENED, int PREC>
@@ -236,7 +243,69 @@ constexpr int kNqGrid = DWG_NQ_GRID;
 // lane's queries never split the warp; each query's terms keep their
 // depth-first order (its value does not depend on NQ or the brick shape).
 // Returns the lane's term count.
-template <bool GRID, bool SCREENED, int PREC, int SHAPE, int NQ, int ORDER>
+// the grid samples of group g for this lane: the brick of SHAPE stacked NQ
+// times in z
+template <int SHAPE, int NQ>
+__device__ __forceinline__ void grid_queries(const GwnArgs& a, unsigned long long g, int lane, bool* valid,
+                                             long long* qi, float* qx, float* qy, float* qz) {
+    using B = Brick<SHAPE>;
+    const long long bxi = (long long)(g % (unsigned long long)a.bx);
+    const unsigned long long t = g / (unsigned long long)a.bx;
+    const long long byi = (long long)(t % (unsigned long long)a.by);
+    const long long bzi = (long long)(t / (unsigned long long)a.by);
+    const long long x = bxi * B::X + (lane % B::X), y = byi * B::Y + ((lane / B::X) % B::Y);
+    const long long z0 = bzi * (NQ * B::Z) + lane / (B::X * B::Y);
+    const bool xy_ok = x < a.rx && y < a.ry;
+    const float fx = __fadd_rn(a.ox, __fmul_rn((float)x, a.h));
+    const float fy = __fadd_rn(a.oy, __fmul_rn((float)y, a.h));
+#pragma unroll
+    for (int u = 0; u < NQ; ++u) {
+        const long long z = z0 + u * B::Z;
+        valid[u] = xy_ok && z < a.rz;
+        qi[u] = x + (long long)a.rx * (y + (long long)a.ry * z);
+        qx[u] = fx;
+        qy[u] = fy;
+        qz[u] = __fadd_rn(a.oz, __fmul_rn((float)(z + a.zoff), a.h));
+    }
+}
+
+// the points of a leaf, one term each, for one query
+template <bool SCREENED, int PREC, typename Acc>
+__device__ __forceinline__ void leaf_terms(const GwnArgs& a, int start, int cnt, float qx, float qy, float qz,
+                                           float sigma, float sigma_l2e, Acc& sum, int& nt) {
+    for (int j = start; j < start + cnt; ++j) {
+        const float4 p = a.pa[j];
+        const float4 nn = a.nr[j];
+        const float dx = p.x - qx, dy = p.y - qy, dz = p.z - qz;
+        const float d = p.w * fmaf(dx, nn.x, fmaf(dy, nn.y, dz * nn.z));
+        const float sc = a.use_radii ? nn.w : a.screen;
+        float v;
+        if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, sc, sigma, sigma_l2e, v)) {
+            sum += (Acc)v;
+            ++nt;
+        }
+    }
+}
+
+// one far-node term, masked to the lanes that take it (shared by the
+// traversal and the replay of its interaction list, so both give the same bits)
+template <bool SCREENED, int PREC, typename Acc>
+__device__ __forceinline__ void node_term(const GwnArgs& a, const float4& na, const float4& nb, float dx, float dy,
+                                          float dz, float d2, bool take, float sigma, float sigma_l2e, Acc& sum,
+                                          int& nt) {
+    // x and y parts first: the samples of a lane share x and y
+    const float dd = fmaf(dz, nb.z, fmaf(dy, nb.y, dx * nb.x));
+    bool k;
+    const float v = gwn_term_masked<SCREENED, PREC>(take, d2, dd, a.screen, sigma, sigma_l2e, k);
+    sum += (Acc)v;  // v is 0 where no term is taken
+    nt += (int)k;
+}
+
+// MODE 0 sums; MODE 1 counts the group's interaction-list entries (visits
+// where some lane takes a term, and multi-point leaves); MODE 2 writes them:
+// (record, term masks per query slot) in visit order.  Modes 1 and 2 do the
+// traversal only.
+template <bool GRID, bool SCREENED, int PREC, int SHAPE, int NQ, int ORDER, int MODE = 0>
 __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g, int lane,
                                          int* __restrict__ stk_node, unsigned* __restrict__ stk_mask, float sigma,
                                          float sigma_l2e) {
@@ -245,25 +314,7 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
     long long qi[NQ];
     float qx[NQ], qy[NQ], qz[NQ];
     if (GRID) {
-        using B = Brick<SHAPE>;
-        const long long bxi = (long long)(g % (unsigned long long)a.bx);
-        const unsigned long long t = g / (unsigned long long)a.bx;
-        const long long byi = (long long)(t % (unsigned long long)a.by);
-        const long long bzi = (long long)(t / (unsigned long long)a.by);
-        const long long x = bxi * B::X + (lane % B::X), y = byi * B::Y + ((lane / B::X) % B::Y);
-        const long long z0 = bzi * (NQ * B::Z) + lane / (B::X * B::Y);
-        const bool xy_ok = x < a.rx && y < a.ry;
-        const float fx = __fadd_rn(a.ox, __fmul_rn((float)x, a.h));
-        const float fy = __fadd_rn(a.oy, __fmul_rn((float)y, a.h));
-#pragma unroll
-        for (int u = 0; u < NQ; ++u) {
-            const long long z = z0 + u * B::Z;
-            valid[u] = xy_ok && z < a.rz;
-            qi[u] = x + (long long)a.rx * (y + (long long)a.ry * z);
-            qx[u] = fx;
-            qy[u] = fy;
-            qz[u] = __fadd_rn(a.oz, __fmul_rn((float)(z + a.zoff), a.h));
-        }
+        grid_queries<SHAPE, NQ>(a, g, lane, valid, qi, qx, qy, qz);
     } else {
 #pragma unroll
         for (int u = 0; u < NQ; ++u) {
@@ -286,19 +337,16 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
         nt[u] = 0;
     }
 
+    static_assert(MODE == 0 || (GRID && NQ <= 3 && ORDER == 0), "interaction lists: grids, order 0");
+    unsigned rec = 0;  // list entries of this group (warp-uniform)
+    int4* const out_list = (MODE == 2) ? a.list + a.list_off[g] : nullptr;
     auto leaf_points = [&](int start, int cnt, int u) {
-        for (int j = start; j < start + cnt; ++j) {
-            const float4 p = a.pa[j];
-            const float4 nn = a.nr[j];
-            const float dx = p.x - qx[u], dy = p.y - qy[u], dz = p.z - qz[u];
-            const float d = p.w * fmaf(dx, nn.x, fmaf(dy, nn.y, dz * nn.z));
-            const float sc = a.use_radii ? nn.w : a.screen;
-            float v;
-            if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, sc, sigma, sigma_l2e, v)) {
-                sum[u] += (Acc)v;
-                ++nt[u];
-            }
-        }
+        leaf_terms<SCREENED, PREC>(a, start, cnt, qx[u], qy[u], qz[u], sigma, sigma_l2e, sum[u], nt[u]);
+    };
+    auto record = [&](int word, const unsigned* m) {
+        if (MODE == 2 && lane == 0)
+            out_list[rec] = make_int4(word, (int)m[0], NQ > 1 ? (int)m[1] : 0, NQ > 2 ? (int)m[2] : 0);
+        ++rec;
     };
 
     // one child record (level order).  A single-point leaf is always a term;
@@ -315,10 +363,15 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
             const int st = (int)(meta & kMetaIndex), cnt = __float_as_int(na.w);
             if (cnt < 0 || st + cnt > a.num_points) {
                 if (lane == 0) atomicOr(&a.work[1], 4u);
-            } else {
+            } else if (MODE == 0) {
 #pragma unroll
                 for (int u = 0; u < NQ; ++u)
                     if (act[u]) leaf_points(st, cnt, u);
+            } else {
+                unsigned m[NQ];
+#pragma unroll
+                for (int u = 0; u < NQ; ++u) m[u] = __ballot_sync(FULL, act[u]);
+                record(cidx | (int)0x80000000, m);
             }
             return;
         }
@@ -335,21 +388,35 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
             take[u] = act[u] && far[u];
             any = any || take[u];
         }
-        if (__any_sync(FULL, any)) {
+        if (MODE != 0) {
+            unsigned m[NQ];
+            unsigned anym = 0;
 #pragma unroll
             for (int u = 0; u < NQ; ++u) {
-                // x and y parts first: the samples of a lane share x and y
-                const float dd = fmaf(dz[u], nb.z, fmaf(dy[u], nb.y, dx[u] * nb.x));
-                bool k;
-                float v = gwn_term_masked<SCREENED, PREC>(take[u], d2[u], dd, a.screen, sigma, sigma_l2e, k);
-                if (ORDER > 0 && !SCREENED && !leaf) {
-                    // far internal node: add the expansion terms (leaves are exact)
-                    const float c = fwn_correction<ORDER, PREC>(dx[u], dy[u], dz[u], take[u] ? d2[u] : 1.0f,
-                                                                a.node_h + (size_t)cidx * 8);
-                    v += take[u] ? c : 0.f;
+                m[u] = __ballot_sync(FULL, take[u]);
+                anym |= m[u];
+            }
+            if (anym) record(cidx, m);
+        } else if (__any_sync(FULL, any)) {
+#pragma unroll
+            for (int u = 0; u < NQ; ++u) {
+                if (ORDER == 0) {
+                    node_term<SCREENED, PREC>(a, na, nb, dx[u], dy[u], dz[u], d2[u], take[u], sigma, sigma_l2e, sum[u],
+                                              nt[u]);
+                } else {
+                    // x and y parts first: the samples of a lane share x and y
+                    const float dd = fmaf(dz[u], nb.z, fmaf(dy[u], nb.y, dx[u] * nb.x));
+                    bool k;
+                    float v = gwn_term_masked<SCREENED, PREC>(take[u], d2[u], dd, a.screen, sigma, sigma_l2e, k);
+                    if (!SCREENED && !leaf) {
+                        // far internal node: add the expansion terms (leaves are exact)
+                        const float c = fwn_correction<ORDER, PREC>(dx[u], dy[u], dz[u], take[u] ? d2[u] : 1.0f,
+                                                                    a.node_h + (size_t)cidx * 8);
+                        v += take[u] ? c : 0.f;
+                    }
+                    sum[u] += (Acc)v;  // v is 0 where no term is taken
+                    nt[u] += (int)k;
                 }
-                sum[u] += (Acc)v;  // v is 0 where no term is taken
-                nt[u] += (int)k;
             }
         }
         unsigned nm[NQ];
@@ -423,6 +490,11 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
             nb = nb2;
         }
     }
+    if (MODE == 1) {
+        if (lane == 0) a.list_count[g] = rec;
+        return 0;
+    }
+    if (MODE == 2) return 0;
     int total = 0;
 #pragma unroll
     for (int u = 0; u < NQ; ++u) {
@@ -440,7 +512,7 @@ __host__ __device__ constexpr int nq_of() {
     return GRID ? kNqGrid : 1;
 }
 
-template <bool GRID, bool SCREENED, int PREC, int SHAPE, int ORDER>
+template <bool GRID, bool SCREENED, int PREC, int SHAPE, int ORDER, int MODE = 0>
 __global__ void __launch_bounds__(kGwnWarps * 32, (GRID && kNqGrid >= 4) ? 2 : 3) k_gwn(GwnArgs a) {
     constexpr int NQ = nq_of<GRID>();
     __shared__ int stk_node[kGwnWarps][kGwnStack];
@@ -456,8 +528,81 @@ __global__ void __launch_bounds__(kGwnWarps * 32, (GRID && kNqGrid >= 4) ? 2 : 3
         if (lane == 0) g = atomicAdd(&a.work[0], 1u);
         g = __shfl_sync(FULL, g, 0);
         if ((long long)g >= a.ngroups) break;
-        my_terms += (unsigned long long)gwn_group<GRID, SCREENED, PREC, SHAPE, NQ, ORDER>(a, g, lane, stk_node[w], stk_mask[w],
-                                                                                  sigma, sigma_l2e);
+        my_terms += (unsigned long long)gwn_group<GRID, SCREENED, PREC, SHAPE, NQ, ORDER, MODE>(
+            a, g, lane, stk_node[w], stk_mask[w], sigma, sigma_l2e);
+    }
+    if (a.terms_total) {
+        for (int o = 16; o > 0; o >>= 1) my_terms += __shfl_down_sync(FULL, my_terms, o);
+        if (lane == 0 && my_terms) atomicAdd(a.terms_total, my_terms);
+    }
+}
+
+// Replay of the recorded interaction lists of a grid: every group walks its
+// entries in visit order and evaluates exactly the terms (and multi-point
+// leaves) the traversal evaluated, with the same arithmetic, so the sums are
+// bit-identical; the traversal itself (stack, opening tests, votes) is gone.
+template <bool SCREENED, int PREC, int SHAPE>
+__global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_replay(GwnArgs a) {
+    constexpr int NQ = kNqGrid;
+    using Acc = typename AccType<PREC>::T;
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const float sigma = a.sigma_dev ? *a.sigma_dev : a.sigma;
+    const float sigma_l2e = sigma * 1.4426950408889634f;
+    unsigned long long my_terms = 0;
+    for (;;) {
+        unsigned g = 0;
+        if (lane == 0) g = atomicAdd(&a.work[0], 1u);
+        g = __shfl_sync(FULL, g, 0);
+        if ((long long)g >= a.ngroups) break;
+        bool valid[NQ];
+        long long qi[NQ];
+        float qx[NQ], qy[NQ], qz[NQ];
+        grid_queries<SHAPE, NQ>(a, g, lane, valid, qi, qx, qy, qz);
+        Acc sum[NQ];
+        int nt[NQ];
+#pragma unroll
+        for (int u = 0; u < NQ; ++u) {
+            sum[u] = 0;
+            nt[u] = 0;
+        }
+        const unsigned long long e0 = a.list_off[g], e1 = a.list_off[g + 1];
+        // the group's entries arrive 32 at a time in one coalesced load and
+        // are handed out by shuffles (no dependent global load per entry)
+        for (unsigned long long base = e0; base < e1; base += 32) {
+            const int4 mine = base + lane < e1 ? a.list[base + lane] : make_int4(0, 0, 0, 0);
+            const int cnt = e1 - base < 32 ? (int)(e1 - base) : 32;
+            for (int j = 0; j < cnt; ++j) {
+                const int ex = __shfl_sync(FULL, mine.x, j);
+                const unsigned m[3] = {(unsigned)__shfl_sync(FULL, mine.y, j), (unsigned)__shfl_sync(FULL, mine.z, j),
+                                       (unsigned)__shfl_sync(FULL, mine.w, j)};
+                if (ex < 0) {  // a multi-point leaf: its points for the lanes that reached it
+                    const int cidx = ex & 0x7fffffff;
+                    const unsigned meta = (unsigned)__float_as_int(a.node_b[cidx].w);
+                    const int st = (int)(meta & kMetaIndex), pc = __float_as_int(a.node_a[cidx].w);
+#pragma unroll
+                    for (int u = 0; u < NQ; ++u)
+                        if ((m[u] >> lane) & 1u)
+                            leaf_terms<SCREENED, PREC>(a, st, pc, qx[u], qy[u], qz[u], sigma, sigma_l2e, sum[u],
+                                                       nt[u]);
+                } else {
+                    const float4 na = a.node_a[ex], nb = a.node_b[ex];
+#pragma unroll
+                    for (int u = 0; u < NQ; ++u) {
+                        const float dx = __fsub_rn(na.x, qx[u]);
+                        const float dy = __fsub_rn(na.y, qy[u]);
+                        const float dz = __fsub_rn(na.z, qz[u]);
+                        node_term<SCREENED, PREC>(a, na, nb, dx, dy, dz, sq3_rn(dx, dy, dz),
+                                                  ((m[u] >> lane) & 1u) != 0, sigma, sigma_l2e, sum[u], nt[u]);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < NQ; ++u) {
+            if (valid[u]) a.out[qi[u]] = (float)sum[u];
+            my_terms += (unsigned long long)nt[u];
+        }
     }
     if (a.terms_total) {
         for (int o = 16; o > 0; o >>= 1) my_terms += __shfl_down_sync(FULL, my_terms, o);
@@ -550,17 +695,22 @@ static int dispatch(const GwnArgs& a, const dwg_gwn_params& p, cudaStream_t s) {
     return launch_plain<GRID, 2>(a, p, s);
 }
 
-int gwn_eval(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, float* out,
-             unsigned long long* terms_total, int* per_query_terms, cudaStream_t s,
-             const float* sigma_dev) {
+// the kernel arguments of a sum (everything but the launch); *empty is set
+// for an empty point query set
+static int make_args(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, float* out,
+                     unsigned long long* terms_total, int* per_query_terms, cudaStream_t s, const float* sigma_dev,
+                     GwnArgs& a, bool* empty) {
+    *empty = false;
     DWG_REQUIRE(t.M > 0, "gwn: octree is empty");
     DWG_REQUIRE(out != nullptr, "gwn: output is null");
     DWG_REQUIRE(p.order >= 0 && p.order <= 2, "gwn: expansion order must be 0, 1 or 2 (got %d)", p.order);
     DWG_REQUIRE(p.order == 0 || !p.screened, "gwn: expansion orders above 0 apply to the plain sum only");
-    GwnArgs a;
     a.info = t.info.ptr;
     DWG_TRY(octree_set_beta(const_cast<Octree&>(t), p.beta, s));
     a.node_h = nullptr;
+    a.list_count = nullptr;
+    a.list_off = nullptr;
+    a.list = nullptr;
     if (p.order > 0) {
         DWG_TRY(octree_update_expansion(const_cast<Octree&>(t), p.order, s));
         a.node_h = t.node_h.ptr;
@@ -592,8 +742,8 @@ int gwn_eval(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, float*
         a.ox = a.oy = a.oz = a.h = 0.f;
         a.bx = a.by = 1;
         a.ngroups = (q.nq + 31) / 32;  // one point per lane
-        if (a.ngroups == 0) return DWG_OK;
-        return dispatch<false>(a, p, s);
+        *empty = a.ngroups == 0;
+        return DWG_OK;
     }
     DWG_REQUIRE(q.res[0] > 0 && q.res[1] > 0 && q.res[2] > 0, "gwn: bad grid resolution");
     a.q = nullptr;
@@ -613,7 +763,111 @@ int gwn_eval(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, float*
     a.by = (q.res[1] + ey - 1) / ey;
     a.ngroups = (long long)a.bx * a.by * ((q.res[2] + kNqGrid * ez - 1) / (kNqGrid * ez));  // bricks stacked in z
     DWG_REQUIRE(a.ngroups < (1ll << 32), "gwn: grid too large");
-    return dispatch<true>(a, p, s);
+    return DWG_OK;
+}
+
+int gwn_eval(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, float* out,
+             unsigned long long* terms_total, int* per_query_terms, cudaStream_t s,
+             const float* sigma_dev) {
+    GwnArgs a;
+    bool empty = false;
+    DWG_TRY(make_args(t, q, p, out, terms_total, per_query_terms, s, sigma_dev, a, &empty));
+    if (empty) return DWG_OK;
+    return q.q ? dispatch<false>(a, p, s) : dispatch<true>(a, p, s);
+}
+
+// ------------------------------------------------------ interaction lists --
+GwnList::~GwnList() = default;
+
+__global__ void k_list_total(const unsigned int* __restrict__ count, unsigned long long* __restrict__ off,
+                             long long n) {
+    off[n] = off[n - 1] + count[n - 1];
+}
+
+template <bool SCREENED, int PREC, int SHAPE>
+static int listed_shape(GwnArgs& a, GwnList& L, const Octree& t, cudaStream_t s, size_t max_bytes, bool* fallback) {
+    static int bps = 0;
+    if (!bps) bps = blocks_for(k_gwn_replay<SCREENED, PREC, SHAPE>);
+    const long long grid_all = (long long)num_sms() * bps;
+    const unsigned grid = (unsigned)(a.ngroups < grid_all * kGwnWarps ? (a.ngroups + kGwnWarps - 1) / kGwnWarps
+                                                                      : grid_all);
+    *fallback = false;
+    if (!L.valid) {
+        // count the entries of every group, place them, record them
+        DWG_TRY(L.count.reserve(a.ngroups));
+        DWG_TRY(L.off.reserve(a.ngroups + 1));
+        GwnArgs c = a;
+        c.list_count = L.count.ptr;
+        c.out = nullptr;
+        c.terms_total = nullptr;
+        DWG_CHECK_CUDA(cudaMemsetAsync(t.work.ptr, 0, sizeof(unsigned int), s));
+        k_gwn<true, SCREENED, PREC, SHAPE, 0, 1><<<grid, kGwnWarps * 32, 0, s>>>(c);
+        DWG_CHECK_LAUNCH();
+        size_t bytes = 0;
+        DWG_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, L.count.ptr, L.off.ptr, (int)a.ngroups, s));
+        DWG_TRY(L.scratch.reserve(bytes + 256));
+        bytes = L.scratch.n;
+        DWG_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(L.scratch.ptr, bytes, L.count.ptr, L.off.ptr, (int)a.ngroups, s));
+        k_list_total<<<1, 1, 0, s>>>(L.count.ptr, L.off.ptr, a.ngroups);
+        DWG_CHECK_LAUNCH();
+        unsigned long long total = 0;
+        DWG_CHECK_CUDA(cudaMemcpyAsync(&total, L.off.ptr + a.ngroups, sizeof(total), cudaMemcpyDeviceToHost, s));
+        DWG_CHECK_CUDA(cudaStreamSynchronize(s));
+        if (total * sizeof(int4) > max_bytes) {  // too large to keep: traverse every time
+            L.too_big = true;
+            L.count.release();
+            L.off.release();
+            *fallback = true;
+            return DWG_OK;
+        }
+        DWG_TRY(L.ent.reserve(total ? total : 1));
+        c.list_off = L.off.ptr;
+        c.list = L.ent.ptr;
+        DWG_CHECK_CUDA(cudaMemsetAsync(t.work.ptr, 0, sizeof(unsigned int), s));
+        k_gwn<true, SCREENED, PREC, SHAPE, 0, 2><<<grid, kGwnWarps * 32, 0, s>>>(c);
+        DWG_CHECK_LAUNCH();
+        L.entries = total;
+        L.valid = true;
+    }
+    a.list_off = L.off.ptr;
+    a.list = L.ent.ptr;
+    DWG_CHECK_CUDA(cudaMemsetAsync(t.work.ptr, 0, sizeof(unsigned int), s));
+    k_gwn_replay<SCREENED, PREC, SHAPE><<<grid, kGwnWarps * 32, 0, s>>>(a);
+    DWG_CHECK_LAUNCH();
+    return DWG_OK;
+}
+
+template <bool SCREENED, int PREC>
+static int listed_prec(GwnArgs& a, GwnList& L, const Octree& t, int tile, cudaStream_t s, size_t max_bytes,
+                       bool* fallback) {
+    switch (tile) {
+        case 1: return listed_shape<SCREENED, PREC, 1>(a, L, t, s, max_bytes, fallback);
+        case 2: return listed_shape<SCREENED, PREC, 2>(a, L, t, s, max_bytes, fallback);
+        case 3: return listed_shape<SCREENED, PREC, 3>(a, L, t, s, max_bytes, fallback);
+        default: return listed_shape<SCREENED, PREC, 0>(a, L, t, s, max_bytes, fallback);
+    }
+}
+
+int gwn_eval_listed(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, GwnList& L, float* out,
+                    unsigned long long* terms_total, cudaStream_t s, const float* sigma_dev, size_t max_bytes) {
+    DWG_REQUIRE(!q.q && p.screened && p.order == 0, "gwn lists: screened grid sums only");
+    GwnArgs a;
+    bool empty = false;
+    DWG_TRY(make_args(t, q, p, out, terms_total, nullptr, s, sigma_dev, a, &empty));
+    if (L.valid && (L.ngroups != a.ngroups || L.tile != p.tile)) L.valid = false;  // another grid: record again
+    if (L.too_big) return dispatch<true>(a, p, s);
+    L.ngroups = a.ngroups;
+    L.tile = p.tile;
+    const int prec = p.precision < 0 ? 0 : (p.precision > 2 ? 2 : p.precision);
+    bool fallback = false;
+    if (prec == 0) DWG_TRY(listed_prec<true, 0>(a, L, t, p.tile, s, max_bytes, &fallback));
+    else if (prec == 1) DWG_TRY(listed_prec<true, 1>(a, L, t, p.tile, s, max_bytes, &fallback));
+    else DWG_TRY(listed_prec<true, 2>(a, L, t, p.tile, s, max_bytes, &fallback));
+    if (fallback) {
+        DWG_CHECK_CUDA(cudaMemsetAsync(t.work.ptr, 0, sizeof(unsigned int), s));
+        return dispatch<true>(a, p, s);
+    }
+    return DWG_OK;
 }
 
 // ------------------------------------------------------------- batches --

@@ -23,6 +23,35 @@ int gwn_eval(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, float*
              unsigned long long* terms_total, int* per_query_terms, cudaStream_t s,
              const float* sigma_dev = nullptr);
 
+// Interaction lists of a grid sum.  The Barnes-Hut decisions of a grid
+// sample depend only on the tree's positions, areas and opening thresholds
+// and on the sample, not on the normals or sigma, so in the DWG loop (fixed
+// leaves, fixed grid) every iteration repeats the same traversal.  The first
+// call records, per group of samples, the visits where some sample takes a
+// term -- (record, per-slot lane masks), 16 bytes each -- and every later
+// call replays them: the same terms in the same order, bit-identical sums,
+// without the traversal.  A list larger than max_bytes is not kept (the sums
+// then traverse every time).  The first call synchronises the stream.
+struct GwnList {
+    DevBuf<unsigned int> count;          // entries per group (recording)
+    DevBuf<unsigned long long> off;      // first entry of each group, ngroups + 1
+    DevBuf<int4> ent;                    // the entries
+    DevBuf<unsigned char> scratch;
+    long long ngroups = 0;
+    unsigned long long entries = 0;
+    int tile = -1;
+    bool valid = false, too_big = false;
+    GwnList() = default;
+    GwnList(const GwnList&) = delete;
+    GwnList& operator=(const GwnList&) = delete;
+    ~GwnList();
+};
+
+// screened grid sums through L (recorded on the first call); the caller
+// resets L.valid when the tree's positions, areas or beta, or the grid change
+int gwn_eval_listed(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, GwnList& L, float* out,
+                    unsigned long long* terms_total, cudaStream_t s, const float* sigma_dev, size_t max_bytes);
+
 // Grid sums of many clouds in one persistent launch (screened).  prepare()
 // records the clouds' octrees, grids and outputs once (host work, not
 // capturable); launch() is two stream operations and can be captured in a

@@ -456,6 +456,12 @@ int Pipeline::setup(const float* points_dev, const float* normals_dev, int n_poi
     long long ng = (long long)gres[0] * gres[1] * gres[2];
     cap = ng / 2 > 1000000 ? ng / 2 : 1000000;  // src/TurboDWG.cu:466
     DWG_TRY(field.reserve((size_t)gres[0] * gres[1] * gnz));
+    {
+        // the grid's interaction lists may take a quarter of the free memory, at most 16 GB
+        size_t fr = 0, tot = 0;
+        DWG_CHECK_CUDA(cudaMemGetInfo(&fr, &tot));
+        glist_budget = fr / 4 < ((size_t)16 << 30) ? fr / 4 : ((size_t)16 << 30);
+    }
     DWG_TRY(wleaf.reserve(L));
     DWG_TRY(cent.reserve((size_t)cap * 3));
     DWG_TRY(tnrm.reserve((size_t)cap * 3));
@@ -520,6 +526,8 @@ int Pipeline::iterate_grid() {
     qg.res[2] = gnz;
     qg.zoff = gz0;
     qg.spacing = gh;
+    if (prm.grid_lists)
+        return gwn_eval_listed(t2, qg, gwn_params(), glist, field.ptr, terms_cur.ptr, s, cur_sigma.ptr, glist_budget);
     return gwn_eval(t2, qg, gwn_params(), field.ptr, terms_cur.ptr, nullptr, s, cur_sigma.ptr);
 }
 

@@ -38,6 +38,8 @@ struct Pipeline {
     float gorg[3] = {0, 0, 0};
     float gh = 0;
     DevBuf<float> field, wleaf;
+    GwnList glist;               // interaction lists of the iteration grid (fixed leaves, fixed grid)
+    size_t glist_budget = 0;     // largest list kept, bytes
     long long cap = 0;
     DevBuf<float> cent, tnrm;
     DevBuf<unsigned long long> ntri;

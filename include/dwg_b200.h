@@ -278,6 +278,10 @@ typedef struct {
     int com_as;             /* --com_As (0): 1 = areas by dwg_point_areas (leaves, then points in the
                                final pass) and, unless in_normal is 1, PCA normals (k = 10) as the
                                input normals; in_normal 2 then starts from random leaf normals */
+    int grid_lists;         /* 1 (default): record the iteration grid's Barnes-Hut interaction
+                               lists in the first iteration and replay them afterwards (the same
+                               terms in the same order: bit-identical fields, no traversal); 0:
+                               traverse in every iteration */
 } dwg_params;
 
 void dwg_params_default(dwg_params* p);

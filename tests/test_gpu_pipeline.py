@@ -175,3 +175,15 @@ def test_dwg_cuda_cli_end_to_end(tmp_path, com_as):
     xyz = np.loadtxt(out / "t_md_7_gr_40_iter_2.xyz")
     assert xyz.shape == (3000, 6)
     assert np.allclose(np.linalg.norm(xyz[:, 3:], axis=1), 1, atol=1e-3)
+
+
+@pytest.mark.parametrize("tile", [0, 2])
+def test_interaction_lists_replay_bit_identical(tile):
+    # the recorded interaction lists replay exactly the traversal's terms
+    P, _ = D.torus(5000, seed=41)
+    Pn, _, _ = D.normalize(P)
+    cfg = dict(SMALL, total_iter=6, tile=tile)
+    a = turbo.reconstruct(cu(Pn), grid_lists=1, **cfg)
+    b = turbo.reconstruct(cu(Pn), grid_lists=0, **cfg)
+    for k in ("leaf_nrm", "iso", "tri_count", "zero_count", "terms", "tris", "point_nrm", "final_iso"):
+        assert np.array_equal(a[k], b[k]), k
