@@ -29,7 +29,7 @@ class DwgError(RuntimeError):
 class GwnParams(C.Structure):
     _fields_ = [("beta", C.c_float), ("sigma", C.c_float), ("screen", C.c_float),
                 ("screened", C.c_int), ("use_radii", C.c_int), ("precision", C.c_int), ("tile", C.c_int),
-                ("order", C.c_int)]
+                ("order", C.c_int), ("lists", C.c_int)]
 
 
 class Params(C.Structure):
@@ -194,5 +194,6 @@ EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_longlong, C.c_voi
 
 
 def gwn_params(beta=2.3, sigma=10.0, screen=0.0015, screened=True, use_radii=False, precision=1,
-               tile=0, order=0) -> GwnParams:
-    return GwnParams(beta, sigma, screen, int(screened), int(use_radii), int(precision), int(tile), int(order))
+               tile=0, order=0, lists=0) -> GwnParams:
+    return GwnParams(beta, sigma, screen, int(screened), int(use_radii), int(precision), int(tile), int(order),
+                     int(lists))

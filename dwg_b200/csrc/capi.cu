@@ -63,6 +63,7 @@ using namespace dwg;
 
 struct dwg_octree {
     Octree t;
+    GwnList list;  // interaction lists of dwg_gwn_grid with params->lists
 };
 struct dwg_knn_index {
     KnnIndex ix;
@@ -137,6 +138,7 @@ int dwg_octree_update_info(dwg_octree* tree, const float* normals_dev, const flo
         DWG_REQUIRE(tree, "octree_update_info: null tree");
         DWG_TRY(octree_set_point_data(tree->t, normals_dev, areas_dev, nullptr, S(stream)));
         DWG_TRY(octree_update_centres(tree->t, S(stream)));
+        tree->list.valid = false;  // new centres: new decisions
         return octree_update_normals(tree->t, S(stream));
     })
 }
@@ -239,6 +241,12 @@ int dwg_gwn_grid(dwg_octree* tree, const float* normals_dev, const float* areas_
             q.origin[d] = origin[d];
         }
         q.spacing = spacing;
+        if (params && params->lists && params->screened && params->order == 0) {
+            DWG_REQUIRE(tree && out_dev, "gwn_grid: null argument");
+            DWG_TRY(octree_set_point_data(tree->t, normals_dev, areas_dev, radii_dev, S(stream)));
+            if (normals_dev || areas_dev) DWG_TRY(octree_update_normals(tree->t, S(stream)));
+            return gwn_eval_listed(tree->t, q, *params, tree->list, out_dev, terms_dev, S(stream), nullptr, 0);
+        }
         return gwn_common(tree, normals_dev, areas_dev, radii_dev, q, params, out_dev, terms_dev, nullptr, stream);
     })
 }

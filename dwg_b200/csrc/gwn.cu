@@ -813,6 +813,11 @@ static int listed_shape(GwnArgs& a, GwnList& L, const Octree& t, cudaStream_t s,
         unsigned long long total = 0;
         DWG_CHECK_CUDA(cudaMemcpyAsync(&total, L.off.ptr + a.ngroups, sizeof(total), cudaMemcpyDeviceToHost, s));
         DWG_CHECK_CUDA(cudaStreamSynchronize(s));
+        if (!max_bytes) {  // no budget given: a quarter of the free memory
+            size_t fr = 0, tot = 0;
+            DWG_CHECK_CUDA(cudaMemGetInfo(&fr, &tot));
+            max_bytes = fr / 4;
+        }
         if (total * sizeof(int4) > max_bytes) {  // too large to keep: traverse every time
             L.too_big = true;
             L.count.release();
@@ -854,10 +859,25 @@ int gwn_eval_listed(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p,
     GwnArgs a;
     bool empty = false;
     DWG_TRY(make_args(t, q, p, out, terms_total, nullptr, s, sigma_dev, a, &empty));
-    if (L.valid && (L.ngroups != a.ngroups || L.tile != p.tile)) L.valid = false;  // another grid: record again
+    const bool same = L.ngroups == a.ngroups && L.tile == p.tile && L.res[0] == q.res[0] && L.res[1] == q.res[1] &&
+                      L.res[2] == q.res[2] && L.zoff == q.zoff && L.origin[0] == q.origin[0] &&
+                      L.origin[1] == q.origin[1] && L.origin[2] == q.origin[2] && L.spacing == q.spacing &&
+                      L.beta == p.beta && L.use_radii == p.use_radii;
+    if (!same) {  // another grid or other decisions: record again
+        L.valid = false;
+        L.too_big = false;
+    }
     if (L.too_big) return dispatch<true>(a, p, s);
     L.ngroups = a.ngroups;
     L.tile = p.tile;
+    for (int d = 0; d < 3; ++d) {
+        L.res[d] = q.res[d];
+        L.origin[d] = q.origin[d];
+    }
+    L.zoff = q.zoff;
+    L.spacing = q.spacing;
+    L.beta = p.beta;
+    L.use_radii = p.use_radii;
     const int prec = p.precision < 0 ? 0 : (p.precision > 2 ? 2 : p.precision);
     bool fallback = false;
     if (prec == 0) DWG_TRY(listed_prec<true, 0>(a, L, t, p.tile, s, max_bytes, &fallback));

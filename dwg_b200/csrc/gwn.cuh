@@ -39,7 +39,9 @@ struct GwnList {
     DevBuf<unsigned char> scratch;
     long long ngroups = 0;
     unsigned long long entries = 0;
-    int tile = -1;
+    // what the recorded decisions depend on besides the tree's centres
+    int tile = -1, res[3] = {0, 0, 0}, zoff = 0, use_radii = 0;
+    float origin[3] = {0, 0, 0}, spacing = 0, beta = 0;
     bool valid = false, too_big = false;
     GwnList() = default;
     GwnList(const GwnList&) = delete;
@@ -47,8 +49,10 @@ struct GwnList {
     ~GwnList();
 };
 
-// screened grid sums through L (recorded on the first call); the caller
-// resets L.valid when the tree's positions, areas or beta, or the grid change
+// screened grid sums through L (recorded on the first call, recorded again
+// when the grid, tile, beta or use_radii differ); the caller resets L.valid
+// when the tree's centres of mass change.  A list above max_bytes (0: a
+// quarter of the free memory when it is recorded) is not kept.
 int gwn_eval_listed(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, GwnList& L, float* out,
                     unsigned long long* terms_total, cudaStream_t s, const float* sigma_dev, size_t max_bytes);
 

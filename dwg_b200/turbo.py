@@ -114,7 +114,7 @@ class TurboLibiGWN:
         return self._launch(query_points, i_Normals, i_As, i_radii if use_radii else None, p, out_gwn)
 
     def grid(self, res, origin, spacing, i_Normals=None, i_As=None, beta=2.3, sigma=10.0, screened=True,
-             precision=1, out=None, terms=None, screen=0.0015, tile=0, order=0):
+             precision=1, out=None, terms=None, screen=0.0015, tile=0, order=0, lists=0):
         """GWN at the closed-form grid origin + index * spacing (x fastest);
         ``tile`` picks the brick of samples a warp evaluates together."""
         res = np.ascontiguousarray(res, np.int32)
@@ -123,7 +123,7 @@ class TurboLibiGWN:
         if out is None:
             out = torch.empty(n, dtype=torch.float32, device="cuda")
         p = capi.gwn_params(beta=beta, sigma=sigma, screen=screen, screened=screened, precision=precision,
-                            tile=tile, order=order)
+                            tile=tile, order=order, lists=lists)
         capi.check(capi.load().dwg_gwn_grid(self._h, capi.ptr(i_Normals), capi.ptr(i_As), None, res.ctypes.data,
                                             org.ctypes.data, float(spacing), C.byref(p), capi.ptr(out),
                                             capi.ptr(terms), capi.stream_ptr()))

@@ -107,6 +107,12 @@ typedef struct {
                         expansion_order, deps/libigl/include/igl/
                         fast_winding_number.cpp:9-120,187-241); screened sums
                         take 0 only */
+    int lists;       /* screened grid sums (dwg_gwn_grid): 1 records the
+                        Barnes-Hut interaction lists of the grid on the first
+                        call (synchronises) and replays them on later calls
+                        with the same grid, beta and tile until the centres
+                        change (dwg_octree_update_info): bit-identical values,
+                        no traversal; 0 traverses every call */
 } dwg_gwn_params;
 
 int dwg_gwn_points(dwg_octree* tree, const float* normals_dev, const float* areas_dev,

@@ -392,3 +392,31 @@ def test_zero_repair_large_grid_bit_exact(oracle_lib, dwg_lib):
     capi.check(dwg_lib.dwg_zero_repair(ix._h, capi.ptr(n_dev), capi.ptr(isz_d), capi.ptr(zc), 10, 10, None))
     torch.cuda.synchronize()
     assert np.array_equal(n_dev.cpu().numpy(), ref)
+
+
+@pytest.mark.parametrize("tile", [0, 2])
+def test_gwn_grid_lists_bit_identical(tile):
+    # dwg_gwn_grid with lists records the grid's interaction lists on its first
+    # call and replays them afterwards: same sums and term counts as the
+    # traversal, bit for bit, also after the normals change and for a new grid
+    P, N = cloud(20000, seed=9)
+    A = np.full(len(P), 2e-6, np.float32)
+    gt = turbo.TurboLibiGWN(cu(P), max_depth=8, areas=cu(A))
+    gt.UpdateMassNormals(cu(N), cu(A))
+    rng = np.random.default_rng(4)
+    N2 = rng.normal(size=N.shape).astype(np.float32)
+    N2 /= np.linalg.norm(N2, axis=1, keepdims=True)
+    for res, org, h in (([40, 36, 30], [-0.55, -0.5, -0.2], 0.03), ([23, 29, 17], [-0.6, -0.55, -0.25], 0.05)):
+        res = np.array(res, np.int32)
+        org = np.array(org, np.float32)
+        for step, nrm in enumerate((None, None, N2)):
+            if nrm is not None:
+                gt.UpdateMassNormals(cu(nrm), cu(A))
+            t0 = torch.zeros(1, dtype=torch.int64, device=DEV)
+            t1 = torch.zeros(1, dtype=torch.int64, device=DEV)
+            w0 = gt.grid(res, org, h, sigma=20.0, tile=tile, terms=t0, lists=0).cpu().numpy()
+            w1 = gt.grid(res, org, h, sigma=20.0, tile=tile, terms=t1, lists=1).cpu().numpy()
+            assert gt.status() == 0
+            assert np.array_equal(w0, w1), (tuple(res), step)
+            assert int(t0.item()) == int(t1.item()) > 0
+        gt.UpdateMassNormals(cu(N), cu(A))
