@@ -361,6 +361,11 @@ def gwn_roofline(a, lib, capi, turbo, torch, dev, P):
     t_trav, n_trav = timed(0)
     t, nterm = timed(1)
     assert nterm == n_trav, (nterm, n_trav)
+    # kept screening weights: 28 of the 30 iteration grids of a reconstruction
+    # (sigma 20 and 10 are each written once) read them instead of evaluating
+    t_w, n_w = timed(2)
+    assert n_w == n_trav, (n_w, n_trav)
+    entries, slots = tree.list_size()
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -378,23 +383,43 @@ def gwn_roofline(a, lib, capi, turbo, torch, dev, P):
             traffic = json.load(open(tp)).get("dram_bytes_per_launch")
         except Exception:
             traffic = None
+    nq = float(np.prod(res.astype(np.float64)))
+    # algorithmic bytes of a launch that reads kept weights: the weights (8 B
+    # per entry and lane), the list entries (16 B), the offsets (8 B per
+    # group of 64 samples) and the field (4 B per sample); node records
+    # (~5 MB) stay in L2 and are not counted
+    wbytes = entries * (32 * 8 + 16) + nq / 64 * 8 + nq * 4
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
     return {
-        "kernel": "k_gwn_replay<screened> (the iteration grid's sums from its recorded interaction lists; "
-                  "256^3 grid, iteration-0 state)",
-        "traversal_launch_ms": t_trav * 1e3,
-        "bound": "fp32",
-        "achieved": achieved,
-        "peak": fp32_peak,
-        "unit": "TFLOP/s",
-        "frac": achieved / fp32_peak,
+        "kernel": "k_gwn_replay<screened> reading kept screening weights (the iteration grid's sums in 28 of "
+                  "30 iterations; 256^3 grid, iteration-0 state)",
+        "bound": "hbm",
+        "achieved": wbytes / t_w / 1e9,
+        "peak": hbm,
+        "unit": "GB/s",
+        "frac": wbytes / t_w / 1e9 / hbm,
         "traffic": traffic,
-        "peak_source": ("nominal FP32 SIMT = SMs x 128 lanes x 2 x sm_max_mhz of MEASURED_PEAKS.json "
-                        "(the file measures HBM copy and bf16 GEMM only)"),
-        "launch_ms": t * 1e3,
+        "peak_source": "hbm_gbs of MEASURED_PEAKS.json (STREAM-style copy)" if "hbm_gbs" in peaks
+                       else "fallback 6650 GB/s",
+        "launch_ms": t_w * 1e3,
+        "algorithmic_bytes": wbytes,
+        "list_entries": entries,
+        "weight_slots": slots,
         "pair_terms": nterm,
-        "sfu": {"achieved_tops": 3.0 * nterm / t / 1e12, "peak_tops": mufu_peak,
-                "frac": 3.0 * nterm / t / 1e12 / mufu_peak},
-        "algorithmic": "20 FP32 flops + 3 MUFU per pair term (screened), terms counted in-kernel",
+        "algorithmic": "per launch: 272 B per list entry (weights of 32 lanes x 2 samples + the entry) + 4 B per "
+                       "sample written; terms counted in-kernel",
+        "evaluating_launches": {
+            "replay_ms": t * 1e3,
+            "traversal_ms": t_trav * 1e3,
+            "bound": "fp32 issue",
+            "achieved_tflops": 20.0 * nterm / t / 1e12,
+            "peak_tflops": fp32_peak,
+            "frac": achieved / fp32_peak,
+            "peak_source": ("nominal FP32 SIMT = SMs x 128 lanes x 2 x sm_max_mhz of MEASURED_PEAKS.json "
+                            "(the file measures HBM copy and bf16 GEMM only)"),
+            "sfu_frac": 3.0 * nterm / t / 1e12 / mufu_peak,
+            "algorithmic": "20 FP32 flops + 3 MUFU per pair term (screened)",
+        },
     }
 
 

@@ -64,6 +64,7 @@ _SIGS = {
     "dwg_octree_update_normals": (_i, [_vp, _vp, _vp, _vp]),
     "dwg_octree_update_info": (_i, [_vp, _vp, _vp, _vp]),
     "dwg_octree_status": (_i, [_vp, C.POINTER(C.c_uint)]),
+    "dwg_octree_list_size": (_i, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_int)]),
     "dwg_octree_export": (_i, [_vp] * 9),
     "dwg_octree_expansion": (_i, [_vp, _vp, _vp]),
     "dwg_gwn_points": (_i, [_vp, _vp, _vp, _vp, _vp, _ll, C.POINTER(GwnParams), _vp, _vp, _vp]),

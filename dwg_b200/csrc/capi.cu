@@ -143,6 +143,16 @@ int dwg_octree_update_info(dwg_octree* tree, const float* normals_dev, const flo
     })
 }
 
+int dwg_octree_list_size(const dwg_octree* tree, long long* entries, int* weight_slots) {
+    API_GUARD({
+        DWG_REQUIRE(tree && entries && weight_slots, "octree_list_size: null argument");
+        const bool kept = tree->list.valid && !tree->list.too_big;
+        *entries = kept ? (long long)tree->list.entries : 0;
+        *weight_slots = kept ? tree->list.nslots : 0;
+        return DWG_OK;
+    });
+}
+
 int dwg_octree_status(const dwg_octree* tree, unsigned int* flags) {
     API_GUARD({
         DWG_REQUIRE(tree && flags, "octree_status: null argument");
@@ -245,7 +255,8 @@ int dwg_gwn_grid(dwg_octree* tree, const float* normals_dev, const float* areas_
             DWG_REQUIRE(tree && out_dev, "gwn_grid: null argument");
             DWG_TRY(octree_set_point_data(tree->t, normals_dev, areas_dev, radii_dev, S(stream)));
             if (normals_dev || areas_dev) DWG_TRY(octree_update_normals(tree->t, S(stream)));
-            return gwn_eval_listed(tree->t, q, *params, tree->list, out_dev, terms_dev, S(stream), nullptr, 0);
+            return gwn_eval_listed(tree->t, q, *params, tree->list, out_dev, terms_dev, S(stream), nullptr, 0,
+                                   params->lists >= 2 ? 2 : 0);
         }
         return gwn_common(tree, normals_dev, areas_dev, radii_dev, q, params, out_dev, terms_dev, nullptr, stream);
     })
@@ -445,7 +456,7 @@ void dwg_params_default(dwg_params* p) {
     p->tile = 0;
     p->as_thres = 0.f;
     p->com_as = 0;
-    p->grid_lists = 1;
+    p->grid_lists = 2;
 }
 
 int dwg_pipeline_create(const float* points_dev, const float* normals_dev, int n, const dwg_params* params,

@@ -13,6 +13,7 @@
 
 #include <cub/cub.cuh>
 
+#include <algorithm>
 #include <vector>
 
 namespace dwg {
@@ -142,25 +143,47 @@ struct GwnArgs {
     unsigned int* list_count;
     const unsigned long long* __restrict__ list_off;
     int4* list;
+    // cached screening weights of the list's node entries (grids, NQ = 2):
+    // slot c holds, per entry and lane, the weights of the lane's two
+    // samples; wsel picks the launch's mode and slot on the device
+    float2* wbuf;
+    unsigned long long wstride;  // float2 per slot = entries * 32
+    GwnWeightState* wsel;
 };
+
+// The screening weight of a far-node term with the MUFU approximations:
+// g = |sigma rho + 1| / (e^{sigma rho} 4 pi rho^3 + 1e-7), 0 where no term is
+// taken; the term is g d.  g depends on the geometry and sigma only, so the
+// interaction-list replay can keep it across iterations with the same sigma
+// and still produce the same bits.
+__device__ __forceinline__ float screen_weight_masked(bool take, float r2, float s, float sigma, float sigma_l2e,
+                                                      bool& ok) {
+    ok = take && r2 > 1e-20f;  // |p - q| <= 1e-10 is skipped
+    const float r2s = ok ? r2 : 1.0f;
+    const float rho = fmaxf(r2s * rsqrt_ftz(r2s), s);
+    const float den = fmaf(ex2_ftz(rho * sigma_l2e), kFourPi * (rho * rho * rho), 1e-7f);
+    // the reference forces the sign of d onto the term
+    // (src/TurboLibiGWN.cu:550-584); den > 0 and |sigma rho + 1| > 0 do that
+    const float g = fabsf(fmaf(sigma, rho, 1.0f)) * rcp_ftz(den);
+    return ok ? g : 0.f;
+}
 
 template <bool SCREENED, int PREC>
 __device__ __forceinline__ float gwn_term_masked(bool take, float r2, float d, float s, float sigma,
                                                  float sigma_l2e, bool& counted) {
     float v = 0.f;
     counted = false;
-    if (SCREENED) {
+    if (SCREENED && PREC < 2) {
+        v = __fmul_rn(screen_weight_masked(take, r2, s, sigma, sigma_l2e, counted), d);
+    } else if (SCREENED) {
         const bool ok = take && r2 > 1e-20f;  // |p - q| <= 1e-10 is skipped
         const float r2s = ok ? r2 : 1.0f;
-        const float r = (PREC >= 2) ? sqrtf(r2s) : r2s * rsqrt_ftz(r2s);
-        const float rho = fmaxf(r, s);
-        const float e = (PREC >= 2) ? expf(sigma * rho) : ex2_ftz(rho * sigma_l2e);
-        const float den = fmaf(e, kFourPi * (rho * rho * rho), 1e-7f);
+        const float rho = fmaxf(sqrtf(r2s), s);
+        const float den = fmaf(expf(sigma * rho), kFourPi * (rho * rho * rho), 1e-7f);
         // the reference forces the sign of d onto the term
         // (src/TurboLibiGWN.cu:550-584); den > 0, so |sigma rho + 1| d does
         // that (an operand modifier, no extra instruction)
-        const float num = fabsf(fmaf(sigma, rho, 1.0f)) * d;
-        const float t = (PREC >= 2) ? __fdiv_rn(num, den) : num * rcp_ftz(den);
+        const float t = __fdiv_rn(fabsf(fmaf(sigma, rho, 1.0f)) * d, den);
         v = ok ? t : 0.f;
         counted = ok;
     } else {
@@ -287,18 +310,31 @@ __device__ __forceinline__ void leaf_terms(const GwnArgs& a, int start, int cnt,
     }
 }
 
+// (A n) . (p - q) of a node for one sample
+__device__ __forceinline__ float node_dot(const float4& nb, float dx, float dy, float dz) {
+    return fmaf(dz, nb.z, fmaf(dy, nb.y, dx * nb.x));
+}
+
 // one far-node term, masked to the lanes that take it (shared by the
 // traversal and the replay of its interaction list, so both give the same bits)
+// (returns the screening weight g of the term for PREC < 2, 0 otherwise)
 template <bool SCREENED, int PREC, typename Acc>
-__device__ __forceinline__ void node_term(const GwnArgs& a, const float4& na, const float4& nb, float dx, float dy,
-                                          float dz, float d2, bool take, float sigma, float sigma_l2e, Acc& sum,
-                                          int& nt) {
+__device__ __forceinline__ float node_term(const GwnArgs& a, const float4& na, const float4& nb, float dx, float dy,
+                                           float dz, float d2, bool take, float sigma, float sigma_l2e, Acc& sum,
+                                           int& nt) {
     // x and y parts first: the samples of a lane share x and y
-    const float dd = fmaf(dz, nb.z, fmaf(dy, nb.y, dx * nb.x));
+    const float dd = node_dot(nb, dx, dy, dz);
     bool k;
-    const float v = gwn_term_masked<SCREENED, PREC>(take, d2, dd, a.screen, sigma, sigma_l2e, k);
+    float v, g = 0.f;
+    if (SCREENED && PREC < 2) {
+        g = screen_weight_masked(take, d2, a.screen, sigma, sigma_l2e, k);
+        v = __fmul_rn(g, dd);  // never contracted into the sum: a kept g gives the same bits
+    } else {
+        v = gwn_term_masked<SCREENED, PREC>(take, d2, dd, a.screen, sigma, sigma_l2e, k);
+    }
     sum += (Acc)v;  // v is 0 where no term is taken
     nt += (int)k;
+    return g;
 }
 
 // MODE 0 sums; MODE 1 counts the group's interaction-list entries (visits
@@ -541,15 +577,26 @@ __global__ void __launch_bounds__(kGwnWarps * 32, (GRID && kNqGrid >= 4) ? 2 : 3
 // entries in visit order and evaluates exactly the terms (and multi-point
 // leaves) the traversal evaluated, with the same arithmetic, so the sums are
 // bit-identical; the traversal itself (stack, opening tests, votes) is gone.
+// With weight slots (a.wsel), mode 1 also writes the screening weight of
+// every node entry and sample; in mode 2 the launch returns at once and
+// k_gwn_wread reads them back.
 template <bool SCREENED, int PREC, int SHAPE>
 __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_replay(GwnArgs a) {
     constexpr int NQ = kNqGrid;
+    static_assert(NQ == 2, "weight slots hold two samples per lane");
     using Acc = typename AccType<PREC>::T;
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const float sigma = a.sigma_dev ? *a.sigma_dev : a.sigma;
     const float sigma_l2e = sigma * 1.4426950408889634f;
-    unsigned long long my_terms = 0;
+    int wmode = 0;
+    float2* wp = nullptr;
+    if (SCREENED && PREC < 2 && a.wsel) {
+        wmode = a.wsel->mode;
+        if (wmode == 2) return;  // k_gwn_wread reads the kept weights
+        wp = a.wbuf + (size_t)a.wsel->slot * a.wstride;
+    }
+    unsigned long long my_terms = 0, my_node_terms = 0;
     for (;;) {
         unsigned g = 0;
         if (lane == 0) g = atomicAdd(&a.work[0], 1u);
@@ -560,7 +607,7 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_replay(GwnArgs a) {
         float qx[NQ], qy[NQ], qz[NQ];
         grid_queries<SHAPE, NQ>(a, g, lane, valid, qi, qx, qy, qz);
         Acc sum[NQ];
-        int nt[NQ];
+        int nt[NQ], ntn = 0;
 #pragma unroll
         for (int u = 0; u < NQ; ++u) {
             sum[u] = 0;
@@ -587,14 +634,19 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_replay(GwnArgs a) {
                                                        nt[u]);
                 } else {
                     const float4 na = a.node_a[ex], nb = a.node_b[ex];
+                    float gw[NQ];
 #pragma unroll
                     for (int u = 0; u < NQ; ++u) {
                         const float dx = __fsub_rn(na.x, qx[u]);
                         const float dy = __fsub_rn(na.y, qy[u]);
                         const float dz = __fsub_rn(na.z, qz[u]);
-                        node_term<SCREENED, PREC>(a, na, nb, dx, dy, dz, sq3_rn(dx, dy, dz),
-                                                  ((m[u] >> lane) & 1u) != 0, sigma, sigma_l2e, sum[u], nt[u]);
+                        const int before = nt[u];
+                        gw[u] = node_term<SCREENED, PREC>(a, na, nb, dx, dy, dz, sq3_rn(dx, dy, dz),
+                                                          ((m[u] >> lane) & 1u) != 0, sigma, sigma_l2e, sum[u],
+                                                          nt[u]);
+                        ntn += nt[u] - before;
                     }
+                    if (wmode == 1) __stcs(wp + (base + j) * 32 + lane, make_float2(gw[0], gw[1]));
                 }
             }
         }
@@ -603,10 +655,244 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_replay(GwnArgs a) {
             if (valid[u]) a.out[qi[u]] = (float)sum[u];
             my_terms += (unsigned long long)nt[u];
         }
+        my_node_terms += (unsigned long long)ntn;
     }
     if (a.terms_total) {
         for (int o = 16; o > 0; o >>= 1) my_terms += __shfl_down_sync(FULL, my_terms, o);
         if (lane == 0 && my_terms) atomicAdd(a.terms_total, my_terms);
+    }
+    if (wmode == 1) {
+        for (int o = 16; o > 0; o >>= 1) my_node_terms += __shfl_down_sync(FULL, my_node_terms, o);
+        if (lane == 0 && my_node_terms) atomicAdd(&a.wsel->node_terms[a.wsel->slot], my_node_terms);
+    }
+}
+
+// Replay that reads the kept screening weights of this sigma (mode 2; other
+// modes return at once): per node entry one dot product and one product per
+// sample, g (A n).(p - q), with the replay's roundings, so the sums keep
+// their bits.  The kernel is bound by the weights' HBM stream (256 bytes per
+// entry), so each warp streams its group's entries and weights through a
+// ring of kWreadRing chunks of kWreadChunk entries in shared memory with
+// cp.async (16-byte pieces, L2 only), two chunks in flight while it sums the
+// third.  The node terms a slot stands for were counted when it was written.
+constexpr int kWreadChunk = 8;
+
+// the points of a multi-point leaf for one sample, out of line (rare in the
+// read path; its registers stay off the loop).  The running sum goes in and
+// comes back, so the points add to it in order, as in leaf_terms.
+template <typename Acc>
+struct LeafSum {
+    Acc sum;
+    int nt;
+};
+template <bool SCREENED, int PREC, typename Acc>
+__device__ __noinline__ LeafSum<Acc> leaf_points_ool(const float4* __restrict__ pa, const float4* __restrict__ nr,
+                                                     int use_radii, float screen, int start, int cnt, float qx,
+                                                     float qy, float qz, float sigma, float sigma_l2e, Acc sum) {
+    LeafSum<Acc> r{sum, 0};
+    for (int j = start; j < start + cnt; ++j) {
+        const float4 p = pa[j];
+        const float4 nn = nr[j];
+        const float dx = p.x - qx, dy = p.y - qy, dz = p.z - qz;
+        const float d = p.w * fmaf(dx, nn.x, fmaf(dy, nn.y, dz * nn.z));
+        const float sc = use_radii ? nn.w : screen;
+        float v;
+        if (gwn_term<SCREENED, PREC>(dx, dy, dz, d, sc, sigma, sigma_l2e, v)) {
+            r.sum += (Acc)v;
+            ++r.nt;
+        }
+    }
+    return r;
+}
+constexpr int kWreadRing = 3;
+constexpr int kWreadWarpBytes = kWreadRing * kWreadChunk * (32 * 8 + 16);
+constexpr int kWreadSmem = kGwnWarps * kWreadWarpBytes;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// chunk c of entries [e0, e1) into ring slot r: the weights (2 KB, 16-byte
+// pieces spread over the lanes) and the entries (lanes 0..7)
+__device__ __forceinline__ void wread_issue(const float2* __restrict__ wp, const int4* __restrict__ list,
+                                            unsigned long long e0, unsigned long long e1, unsigned long long c,
+                                            float2* ws, int4* ls, int lane) {
+    const unsigned long long first = e0 + c * kWreadChunk;
+    if (first < e1) {
+        constexpr int kPieces = kWreadChunk * 32 * 8 / 16;  // 16-byte pieces of a chunk's weights
+#pragma unroll
+        for (int r = 0; r < kPieces / 32; ++r) {
+            const int piece = lane + 32 * r;
+            const int k = piece / 16;  // entry of the piece (16 pieces per entry)
+            if (first + k < e1)
+                cp_async16(reinterpret_cast<char*>(ws) + piece * 16,
+                           reinterpret_cast<const char*>(wp + first * 32) + piece * 16);
+        }
+        if (lane < kWreadChunk && first + lane < e1) cp_async16(ls + lane, list + first + lane);
+    }
+    cp_async_commit();  // one group per chunk, empty past the end
+}
+
+template <bool SCREENED, int PREC, int SHAPE>
+__global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_wread(GwnArgs a) {
+    constexpr int NQ = kNqGrid;
+    constexpr int C = kWreadChunk;
+    using Acc = typename AccType<PREC>::T;
+    extern __shared__ __align__(16) unsigned char wread_smem[];
+    const unsigned FULL = 0xffffffffu;
+    GwnWeightState* const wst = a.wsel;
+    if (wst->mode != 2) return;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    float2* const wring = reinterpret_cast<float2*>(wread_smem + warp * kWreadWarpBytes);
+    int4* const lring = reinterpret_cast<int4*>(wread_smem + warp * kWreadWarpBytes + kWreadRing * C * 32 * 8);
+    const float2* const wp = a.wbuf + (size_t)wst->slot * a.wstride;
+    if (a.terms_total && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(a.terms_total, wst->node_terms[wst->slot]);
+    const float sigma = a.sigma_dev ? *a.sigma_dev : a.sigma;
+    const float sigma_l2e = sigma * 1.4426950408889634f;
+    unsigned long long my_terms = 0;
+    for (;;) {
+        unsigned g = 0;
+        if (lane == 0) g = atomicAdd(&wst->work, 1u);
+        g = __shfl_sync(FULL, g, 0);
+        if ((long long)g >= a.ngroups) break;
+        bool valid[NQ];
+        long long qi[NQ];
+        float qx[NQ], qy[NQ], qz[NQ];
+        grid_queries<SHAPE, NQ>(a, g, lane, valid, qi, qx, qy, qz);
+        Acc sum[NQ];
+        int nt[NQ];
+#pragma unroll
+        for (int u = 0; u < NQ; ++u) {
+            sum[u] = 0;
+            nt[u] = 0;
+        }
+        const unsigned long long e0 = a.list_off[g], e1 = a.list_off[g + 1];
+        const unsigned long long nchunk = (e1 - e0 + C - 1) / C;
+        __syncwarp();  // the ring's last readers (previous group) are done
+#pragma unroll
+        for (int c = 0; c < kWreadRing - 1; ++c)
+            wread_issue(wp, a.list, e0, e1, c, wring + c * C * 32, lring + c * C, lane);
+        for (unsigned long long c = 0; c < nchunk; ++c) {
+            cp_async_wait_1();  // chunk c has landed (c + 1 may be in flight)
+            __syncwarp();
+            const int r = (int)(c % kWreadRing);
+            const float2* wc = wring + r * C * 32;
+            const int4* lc = lring + r * C;
+            const unsigned long long first = e0 + c * C;
+            const int cnt = e1 - first < (unsigned long long)C ? (int)(e1 - first) : C;
+            // a full chunk of node entries (the common case): unrolled, the
+            // next entry's node record loaded while this one is summed
+            const bool full = cnt == C && __ballot_sync(FULL, lc[lane & (C - 1)].x < 0) == 0;
+            if (full) {
+                float4 na = a.node_a[lc[0].x], nb = a.node_b[lc[0].x];
+#pragma unroll
+                for (int k = 0; k < C; ++k) {
+                    float4 na_n = na, nb_n = nb;
+                    if (k + 1 < C) {
+                        const int xn = lc[k + 1].x;
+                        na_n = a.node_a[xn];
+                        nb_n = a.node_b[xn];
+                    }
+                    const float2 w = wc[k * 32 + lane];
+                    const float wu[2] = {w.x, w.y};
+#pragma unroll
+                    for (int u = 0; u < NQ; ++u) {
+                        const float dd = node_dot(nb, __fsub_rn(na.x, qx[u]), __fsub_rn(na.y, qy[u]),
+                                                  __fsub_rn(na.z, qz[u]));
+                        sum[u] += (Acc)__fmul_rn(wu[u], dd);
+                    }
+                    na = na_n;
+                    nb = nb_n;
+                }
+            }
+            for (int k = full ? C : 0; k < cnt; ++k) {
+                const int4 e = lc[k];
+                if (e.x < 0) {  // a multi-point leaf: its points for the lanes that reached it
+                    const int cidx = e.x & 0x7fffffff;
+                    const unsigned meta = (unsigned)__float_as_int(a.node_b[cidx].w);
+                    const int st = (int)(meta & kMetaIndex), pc = __float_as_int(a.node_a[cidx].w);
+#pragma unroll
+                    for (int u = 0; u < NQ; ++u) {
+                        if (((unsigned)(u ? e.z : e.y) >> lane) & 1u) {
+                            const LeafSum<Acc> r = leaf_points_ool<SCREENED, PREC, Acc>(
+                                a.pa, a.nr, a.use_radii, a.screen, st, pc, qx[u], qy[u], qz[u], sigma, sigma_l2e,
+                                sum[u]);
+                            sum[u] = r.sum;
+                            nt[u] += r.nt;
+                        }
+                    }
+                } else {
+                    const float4 na = a.node_a[e.x], nb = a.node_b[e.x];
+                    const float2 w = wc[k * 32 + lane];
+                    const float wu[2] = {w.x, w.y};
+#pragma unroll
+                    for (int u = 0; u < NQ; ++u) {
+                        const float dd = node_dot(nb, __fsub_rn(na.x, qx[u]), __fsub_rn(na.y, qy[u]),
+                                                  __fsub_rn(na.z, qz[u]));
+                        sum[u] += (Acc)__fmul_rn(wu[u], dd);
+                    }
+                }
+            }
+            __syncwarp();  // ring slot (c + 2) % 3 = (c - 1) % 3 was read in the previous pass
+            const unsigned long long nx = c + kWreadRing - 1;
+            const int rn = (int)(nx % kWreadRing);
+            wread_issue(wp, a.list, e0, e1, nx, wring + rn * C * 32, lring + rn * C, lane);
+        }
+#pragma unroll
+        for (int u = 0; u < NQ; ++u) {
+            if (valid[u]) a.out[qi[u]] = (float)sum[u];
+            my_terms += (unsigned long long)nt[u];
+        }
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");  // no copy outlives the block
+    if (a.terms_total) {
+        for (int o = 16; o > 0; o >>= 1) my_terms += __shfl_down_sync(FULL, my_terms, o);
+        if (lane == 0 && my_terms) atomicAdd(a.terms_total, my_terms);
+    }
+}
+
+// Chooses the weight slot of the next replay launch on the device: a launch
+// that wrote a slot has completed when this runs (same stream), so its slot
+// becomes valid; then a valid slot with this (sigma, screen) is read, else
+// the first free slot is written, else the terms are evaluated as usual.
+__global__ void k_weight_select(GwnWeightState* __restrict__ w, const float* __restrict__ sigma_dev, float sigma,
+                                float screen) {
+    if (w->mode == 1) w->valid[w->slot] = 1;
+    const float sg = sigma_dev ? *sigma_dev : sigma;
+    w->mode = 0;
+    w->slot = 0;
+    w->work = 0;
+    for (int c = 0; c < w->nslots; ++c)
+        if (w->valid[c] && w->sigma[c] == sg && w->screen[c] == screen) {
+            w->mode = 2;
+            w->slot = c;
+            return;
+        }
+    for (int c = 0; c < w->nslots; ++c)
+        if (!w->valid[c]) {
+            w->mode = 1;
+            w->slot = c;
+            w->sigma[c] = sg;
+            w->screen[c] = screen;
+            w->node_terms[c] = 0;
+            return;
+        }
+}
+
+__global__ void k_weight_reset(GwnWeightState* __restrict__ w, int nslots) {
+    w->mode = 0;
+    w->slot = 0;
+    w->nslots = nslots;
+    w->work = 0;
+    for (int c = 0; c < kGwnWeightSlots; ++c) {
+        w->valid[c] = 0;
+        w->sigma[c] = 0.f;
+        w->screen[c] = 0.f;
+        w->node_terms[c] = 0;
     }
 }
 
@@ -711,6 +997,9 @@ static int make_args(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p
     a.list_count = nullptr;
     a.list_off = nullptr;
     a.list = nullptr;
+    a.wbuf = nullptr;
+    a.wstride = 0;
+    a.wsel = nullptr;
     if (p.order > 0) {
         DWG_TRY(octree_update_expansion(const_cast<Octree&>(t), p.order, s));
         a.node_h = t.node_h.ptr;
@@ -833,12 +1122,49 @@ static int listed_shape(GwnArgs& a, GwnList& L, const Octree& t, cudaStream_t s,
         DWG_CHECK_LAUNCH();
         L.entries = total;
         L.valid = true;
+        // weight slots: 8 bytes per entry and lane each, together at most a
+        // third of the free memory and 64 GB
+        L.nslots = 0;
+        if (SCREENED && PREC < 2 && L.wslots > 0 && total > 0) {
+            size_t fr = 0, tot = 0;
+            DWG_CHECK_CUDA(cudaMemGetInfo(&fr, &tot));
+            const unsigned long long per = total * 32ull * sizeof(float2);
+            const unsigned long long cap = std::min<unsigned long long>(fr / 3, 64ull << 30);
+            int n = (int)std::min<unsigned long long>((unsigned long long)std::min(L.wslots, kGwnWeightSlots),
+                                                      cap / per);
+            if (n > 0 && L.w.reserve((size_t)n * total * 32) != DWG_OK) n = 0;
+            L.nslots = n;
+            DWG_TRY(L.wstate.reserve(1));
+            k_weight_reset<<<1, 1, 0, s>>>(L.wstate.ptr, n);
+            DWG_CHECK_LAUNCH();
+        }
     }
     a.list_off = L.off.ptr;
     a.list = L.ent.ptr;
+    if (L.nslots > 0) {
+        a.wbuf = L.w.ptr;
+        a.wstride = L.entries * 32ull;
+        a.wsel = L.wstate.ptr;
+        k_weight_select<<<1, 1, 0, s>>>(L.wstate.ptr, a.sigma_dev, a.sigma, a.screen);
+        DWG_CHECK_LAUNCH();
+    }
     DWG_CHECK_CUDA(cudaMemsetAsync(t.work.ptr, 0, sizeof(unsigned int), s));
     k_gwn_replay<SCREENED, PREC, SHAPE><<<grid, kGwnWarps * 32, 0, s>>>(a);
     DWG_CHECK_LAUNCH();
+    if (L.nslots > 0) {
+        static int bpw = 0;
+        if (!bpw) {
+            DWG_CHECK_CUDA(cudaFuncSetAttribute(k_gwn_wread<SCREENED, PREC, SHAPE>,
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, kWreadSmem));
+            DWG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpw, k_gwn_wread<SCREENED, PREC, SHAPE>,
+                                                                         kGwnWarps * 32, kWreadSmem));
+            if (bpw < 1) bpw = 1;
+        }
+        const long long all = (long long)num_sms() * bpw;
+        const unsigned gw = (unsigned)(a.ngroups < all * kGwnWarps ? (a.ngroups + kGwnWarps - 1) / kGwnWarps : all);
+        k_gwn_wread<SCREENED, PREC, SHAPE><<<gw, kGwnWarps * 32, kWreadSmem, s>>>(a);
+        DWG_CHECK_LAUNCH();
+    }
     return DWG_OK;
 }
 
@@ -854,7 +1180,8 @@ static int listed_prec(GwnArgs& a, GwnList& L, const Octree& t, int tile, cudaSt
 }
 
 int gwn_eval_listed(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, GwnList& L, float* out,
-                    unsigned long long* terms_total, cudaStream_t s, const float* sigma_dev, size_t max_bytes) {
+                    unsigned long long* terms_total, cudaStream_t s, const float* sigma_dev, size_t max_bytes,
+                    int wslots) {
     DWG_REQUIRE(!q.q && p.screened && p.order == 0, "gwn lists: screened grid sums only");
     GwnArgs a;
     bool empty = false;
@@ -862,7 +1189,7 @@ int gwn_eval_listed(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p,
     const bool same = L.ngroups == a.ngroups && L.tile == p.tile && L.res[0] == q.res[0] && L.res[1] == q.res[1] &&
                       L.res[2] == q.res[2] && L.zoff == q.zoff && L.origin[0] == q.origin[0] &&
                       L.origin[1] == q.origin[1] && L.origin[2] == q.origin[2] && L.spacing == q.spacing &&
-                      L.beta == p.beta && L.use_radii == p.use_radii;
+                      L.beta == p.beta && L.use_radii == p.use_radii && L.wslots == wslots;
     if (!same) {  // another grid or other decisions: record again
         L.valid = false;
         L.too_big = false;
@@ -878,6 +1205,7 @@ int gwn_eval_listed(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p,
     L.spacing = q.spacing;
     L.beta = p.beta;
     L.use_radii = p.use_radii;
+    L.wslots = wslots;
     const int prec = p.precision < 0 ? 0 : (p.precision > 2 ? 2 : p.precision);
     bool fallback = false;
     if (prec == 0) DWG_TRY(listed_prec<true, 0>(a, L, t, p.tile, s, max_bytes, &fallback));
@@ -923,6 +1251,12 @@ static void fill_args(GwnArgs& a, const Octree& t, const GwnBatchItem& it, const
     a.per_query_terms = nullptr;
     a.work = t.work.ptr;  // error word at [1]
     a.node_h = nullptr;
+    a.list_count = nullptr;
+    a.list_off = nullptr;
+    a.list = nullptr;
+    a.wbuf = nullptr;
+    a.wstride = 0;
+    a.wsel = nullptr;
     a.num_nodes = t.M;
     a.num_points = t.n;
 }

@@ -32,11 +32,33 @@ int gwn_eval(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, float*
 // call replays them: the same terms in the same order, bit-identical sums,
 // without the traversal.  A list larger than max_bytes is not kept (the sums
 // then traverse every time).  The first call synchronises the stream.
+//
+// Screening weights: a far-node term is g (A n).(p - q) with
+// g = |sigma rho + 1| / (e^{sigma rho} 4 pi rho^3 + 1e-7), which depends on
+// the geometry and sigma only.  With weight slots, the replay also keeps g
+// per node entry and sample (8 bytes per entry and lane) for up to
+// kGwnWeightSlots values of (sigma, screen): a launch whose sigma has a slot
+// reads g and skips the screening arithmetic (same bits); one without writes
+// the next free slot while it evaluates.  The choice is made on the device
+// (GwnWeightState), so CUDA graph replays with a device sigma work.
+constexpr int kGwnWeightSlots = 4;
+struct GwnWeightState {
+    int mode, slot, nslots, pad;  // mode: 0 evaluate, 1 evaluate and write slot, 2 read slot
+    int valid[kGwnWeightSlots];
+    float sigma[kGwnWeightSlots], screen[kGwnWeightSlots];
+    unsigned long long node_terms[kGwnWeightSlots];  // node terms a slot stands for
+    unsigned int work;                               // group counter of the reading launch
+};
+
 struct GwnList {
     DevBuf<unsigned int> count;          // entries per group (recording)
     DevBuf<unsigned long long> off;      // first entry of each group, ngroups + 1
     DevBuf<int4> ent;                    // the entries
     DevBuf<unsigned char> scratch;
+    DevBuf<float2> w;                    // weight slots, nslots * entries * 32
+    DevBuf<GwnWeightState> wstate;
+    int wslots = 0;                      // weight slots wanted (0: none)
+    int nslots = 0;                      // weight slots held
     long long ngroups = 0;
     unsigned long long entries = 0;
     // what the recorded decisions depend on besides the tree's centres
@@ -52,9 +74,14 @@ struct GwnList {
 // screened grid sums through L (recorded on the first call, recorded again
 // when the grid, tile, beta or use_radii differ); the caller resets L.valid
 // when the tree's centres of mass change.  A list above max_bytes (0: a
-// quarter of the free memory when it is recorded) is not kept.
+// quarter of the free memory when it is recorded) is not kept.  wslots > 0
+// keeps screening weights for up to that many (sigma, screen) values (at most
+// kGwnWeightSlots; slots that do not fit in a third of the free memory, or
+// 64 GB, are dropped) when the terms use the MUFU approximations (precision
+// 0 or 1).
 int gwn_eval_listed(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, GwnList& L, float* out,
-                    unsigned long long* terms_total, cudaStream_t s, const float* sigma_dev, size_t max_bytes);
+                    unsigned long long* terms_total, cudaStream_t s, const float* sigma_dev, size_t max_bytes,
+                    int wslots = 0);
 
 // Grid sums of many clouds in one persistent launch (screened).  prepare()
 // records the clouds' octrees, grids and outputs once (host work, not

@@ -526,8 +526,23 @@ int Pipeline::iterate_grid() {
     qg.res[2] = gnz;
     qg.zoff = gz0;
     qg.spacing = gh;
-    if (prm.grid_lists)
-        return gwn_eval_listed(t2, qg, gwn_params(), glist, field.ptr, terms_cur.ptr, s, cur_sigma.ptr, glist_budget);
+    if (prm.grid_lists) {
+        // grid_lists 2 also keeps the screening weights of every sigma of the
+        // schedule's first total_iter iterations (20, then lambda and 10)
+        int wslots = 0;
+        if (prm.grid_lists >= 2) {
+            float seen[kGwnWeightSlots];
+            const int iters = prm.total_iter > 0 ? prm.total_iter : 1;
+            for (int t = 0; t < iters && wslots < kGwnWeightSlots; ++t) {
+                const float sg = sigma_at(t, prm.lambda);
+                bool dup = false;
+                for (int c = 0; c < wslots; ++c) dup = dup || seen[c] == sg;
+                if (!dup) seen[wslots++] = sg;
+            }
+        }
+        return gwn_eval_listed(t2, qg, gwn_params(), glist, field.ptr, terms_cur.ptr, s, cur_sigma.ptr, glist_budget,
+                               wslots);
+    }
     return gwn_eval(t2, qg, gwn_params(), field.ptr, terms_cur.ptr, nullptr, s, cur_sigma.ptr);
 }
 

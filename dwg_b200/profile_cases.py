@@ -2,7 +2,7 @@
 and a summariser of a profiler launch list.
 
     python -m dwg_b200.profile_cases step     [--points N --grid R --iters T --reps K --shape torus|sq_union]
-    python -m dwg_b200.profile_cases gwn_grid [--points N --grid R --launches K --lists]
+    python -m dwg_b200.profile_cases gwn_grid [--points N --grid R --launches K --lists [1|2]]
     python -m dwg_b200.profile_cases knn_tri  [--points N --grid R --launches K]
     python -m dwg_b200.profile_cases mc       [--points N --grid R --launches K]
     python -m dwg_b200.profile_cases summarize launches.csv
@@ -12,8 +12,10 @@ non-uniform torus and prints per-phase host timings.  The single-kernel cases
 first run one plain DWG iteration to obtain a realistic state (leaf normals,
 iteration-0 field and triangles), then launch only the named kernel
 ``--launches`` times, so that a capture filtered by kernel name and launch
-count sees warm, representative launches.  ``gwn_grid --lists`` records the
-grid's interaction lists in its first call and replays them in the others.
+count sees warm, representative launches.  ``gwn_grid --lists 1`` records the
+grid's interaction lists in its first call and replays them in the others;
+``--lists 2`` also writes the screening weights in the first call and reads
+them in the others.
 ``summarize`` turns a CSV launch
 list (``gpu__time_duration.sum`` per launch) into per-kernel launches, total
 time and share.
@@ -102,7 +104,7 @@ def case_gwn_grid(a):
     res, org = st["res"], st["org"]
     out = torch.empty(int(np.prod(res)), device="cuda")
     for _ in range(a.launches):
-        tree.grid(res, org[:3], float(org[3]), sigma=20.0, precision=1, out=out, lists=int(a.lists))
+        tree.grid(res, org[:3], float(org[3]), sigma=20.0, precision=1, out=out, lists=a.lists)
     torch.cuda.synchronize()
     print("gwn_grid", res.tolist(), L, tree.status())
 
@@ -183,7 +185,7 @@ def main(argv=None):
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--launches", type=int, default=2)
     ap.add_argument("--shape", choices=["torus", "sq_union"], default="torus")
-    ap.add_argument("--lists", action="store_true")
+    ap.add_argument("--lists", type=int, nargs="?", const=1, default=0, choices=[0, 1, 2])
     a = ap.parse_args(argv)
     global _SHAPE
     _SHAPE = a.shape

@@ -129,6 +129,13 @@ class TurboLibiGWN:
                                             capi.ptr(terms), capi.stream_ptr()))
         return out
 
+    def list_size(self):
+        """(entries, weight slots) of the kept interaction list of grid()."""
+        e = C.c_longlong()
+        w = C.c_int()
+        capi.check(capi.load().dwg_octree_list_size(self._h, C.byref(e), C.byref(w)))
+        return e.value, w.value
+
     def status(self):
         """Sticky traversal error flags (0 = none); raises on a set flag."""
         f = C.c_uint()

@@ -72,6 +72,11 @@ int dwg_octree_update_info(dwg_octree* tree, const float* normals_dev, const flo
  * range outside the point array, bit 3 an opening threshold that failed its
  * self-check.  Any set bit makes the call return DWG_ERR_DEVICE. */
 int dwg_octree_status(const dwg_octree* tree, unsigned int* flags);
+/* Size of the interaction list dwg_gwn_grid keeps (params->lists >= 1): its
+ * entries (16 bytes each) and the weight slots it holds (8 bytes per entry
+ * and lane each); 0 and 0 when none is kept.  No reference counterpart: the
+ * lists are this library's own cache of the Barnes-Hut decisions. */
+int dwg_octree_list_size(const dwg_octree* tree, long long* entries, int* weight_slots);
 /* Copy the node table to host memory (for checking).  Arrays may be NULL.
  * Nodes are in depth-first pre-order; points are in the octree's sorted
  * order, perm_host[i] = input index of sorted point i.
@@ -112,7 +117,11 @@ typedef struct {
                         call (synchronises) and replays them on later calls
                         with the same grid, beta and tile until the centres
                         change (dwg_octree_update_info): bit-identical values,
-                        no traversal; 0 traverses every call */
+                        no traversal; 2 also keeps the terms' screening
+                        weights for two (sigma, screen) values (precision 0
+                        and 1): later calls with one of them read the weights
+                        instead of evaluating them, same bits; 0 traverses
+                        every call */
 } dwg_gwn_params;
 
 int dwg_gwn_points(dwg_octree* tree, const float* normals_dev, const float* areas_dev,
@@ -284,10 +293,14 @@ typedef struct {
     int com_as;             /* --com_As (0): 1 = areas by dwg_point_areas (leaves, then points in the
                                final pass) and, unless in_normal is 1, PCA normals (k = 10) as the
                                input normals; in_normal 2 then starts from random leaf normals */
-    int grid_lists;         /* 1 (default): record the iteration grid's Barnes-Hut interaction
-                               lists in the first iteration and replay them afterwards (the same
-                               terms in the same order: bit-identical fields, no traversal); 0:
-                               traverse in every iteration */
+    int grid_lists;         /* 1: record the iteration grid's Barnes-Hut interaction lists in the
+                               first iteration and replay them afterwards (the same terms in the
+                               same order: bit-identical fields, no traversal); 2 (default): also
+                               keep each term's screening weight for every sigma of the schedule
+                               and read it back in later iterations with that sigma (the same
+                               bits; 8 bytes per list entry and lane per sigma, dropped when it
+                               does not fit in a third of the free memory); 0: traverse in every
+                               iteration */
 } dwg_params;
 
 void dwg_params_default(dwg_params* p);

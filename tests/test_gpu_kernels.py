@@ -397,8 +397,10 @@ def test_zero_repair_large_grid_bit_exact(oracle_lib, dwg_lib):
 @pytest.mark.parametrize("tile", [0, 2])
 def test_gwn_grid_lists_bit_identical(tile):
     # dwg_gwn_grid with lists records the grid's interaction lists on its first
-    # call and replays them afterwards: same sums and term counts as the
-    # traversal, bit for bit, also after the normals change and for a new grid
+    # call and replays them afterwards; lists=2 also keeps the screening
+    # weights of two sigmas.  Same sums and term counts as the traversal, bit
+    # for bit: after the normals change, for a sigma without a slot, on a
+    # second grid
     P, N = cloud(20000, seed=9)
     A = np.full(len(P), 2e-6, np.float32)
     gt = turbo.TurboLibiGWN(cu(P), max_depth=8, areas=cu(A))
@@ -409,14 +411,21 @@ def test_gwn_grid_lists_bit_identical(tile):
     for res, org, h in (([40, 36, 30], [-0.55, -0.5, -0.2], 0.03), ([23, 29, 17], [-0.6, -0.55, -0.25], 0.05)):
         res = np.array(res, np.int32)
         org = np.array(org, np.float32)
-        for step, nrm in enumerate((None, None, N2)):
-            if nrm is not None:
-                gt.UpdateMassNormals(cu(nrm), cu(A))
-            t0 = torch.zeros(1, dtype=torch.int64, device=DEV)
-            t1 = torch.zeros(1, dtype=torch.int64, device=DEV)
-            w0 = gt.grid(res, org, h, sigma=20.0, tile=tile, terms=t0, lists=0).cpu().numpy()
-            w1 = gt.grid(res, org, h, sigma=20.0, tile=tile, terms=t1, lists=1).cpu().numpy()
-            assert gt.status() == 0
-            assert np.array_equal(w0, w1), (tuple(res), step)
-            assert int(t0.item()) == int(t1.item()) > 0
-        gt.UpdateMassNormals(cu(N), cu(A))
+        runs = {}
+        for lists in (0, 2, 1):
+            gt.UpdateMassNormals(cu(N), cu(A))
+            runs[lists] = []
+            # slots: 20 written, read; 10 written; both read; 5 has no slot
+            for sigma, nrm in ((20.0, None), (20.0, None), (10.0, None), (20.0, N2), (10.0, None), (5.0, None),
+                               (10.0, N)):
+                if nrm is not None:
+                    gt.UpdateMassNormals(cu(nrm), cu(A))
+                t = torch.zeros(1, dtype=torch.int64, device=DEV)
+                w = gt.grid(res, org, h, sigma=sigma, tile=tile, terms=t, lists=lists).cpu().numpy()
+                assert gt.status() == 0
+                runs[lists].append((w, int(t.item())))
+        for lists in (1, 2):
+            for step, ((w0, t0), (w, t)) in enumerate(zip(runs[0], runs[lists])):
+                assert t0 > 0
+                assert np.array_equal(w0, w), (tuple(res), lists, step)
+                assert t == t0, (tuple(res), lists, step)
