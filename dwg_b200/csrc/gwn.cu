@@ -292,6 +292,44 @@ __device__ __forceinline__ void grid_queries(const GwnArgs& a, unsigned long lon
     }
 }
 
+// the samples of group g: a grid brick, or 32 * NQ consecutive points
+template <bool GRID, int SHAPE, int NQ>
+__device__ __forceinline__ void group_queries(const GwnArgs& a, unsigned long long g, int lane, bool* valid,
+                                              long long* qi, float* qx, float* qy, float* qz) {
+    if (GRID) {
+        grid_queries<SHAPE, NQ>(a, g, lane, valid, qi, qx, qy, qz);
+    } else {
+#pragma unroll
+        for (int u = 0; u < NQ; ++u) {
+            qi[u] = (long long)g * (32 * NQ) + u * 32 + lane;
+            valid[u] = qi[u] < a.nq;
+            qx[u] = qy[u] = qz[u] = 0.f;
+            if (valid[u]) {
+                qx[u] = a.q[qi[u] * 3];
+                qy[u] = a.q[qi[u] * 3 + 1];
+                qz[u] = a.q[qi[u] * 3 + 2];
+            }
+        }
+    }
+}
+
+// kept screening weights of one lane and list entry: one per sample slot
+template <int NQ>
+struct WeightOf {
+    using T = float2;
+    __device__ static T pack(const float* g) { return make_float2(g[0], g[1]); }
+    __device__ static void unpack(const T& w, float* g) {
+        g[0] = w.x;
+        g[1] = w.y;
+    }
+};
+template <>
+struct WeightOf<1> {
+    using T = float;
+    __device__ static T pack(const float* g) { return g[0]; }
+    __device__ static void unpack(const T& w, float* g) { g[0] = w; }
+};
+
 // the points of a leaf, one term each, for one query
 template <bool SCREENED, int PREC, typename Acc>
 __device__ __forceinline__ void leaf_terms(const GwnArgs& a, int start, int cnt, float qx, float qy, float qz,
@@ -349,21 +387,7 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
     bool valid[NQ];
     long long qi[NQ];
     float qx[NQ], qy[NQ], qz[NQ];
-    if (GRID) {
-        grid_queries<SHAPE, NQ>(a, g, lane, valid, qi, qx, qy, qz);
-    } else {
-#pragma unroll
-        for (int u = 0; u < NQ; ++u) {
-            qi[u] = (long long)g * (32 * NQ) + u * 32 + lane;
-            valid[u] = qi[u] < a.nq;
-            qx[u] = qy[u] = qz[u] = 0.f;
-            if (valid[u]) {
-                qx[u] = a.q[qi[u] * 3];
-                qy[u] = a.q[qi[u] * 3 + 1];
-                qz[u] = a.q[qi[u] * 3 + 2];
-            }
-        }
-    }
+    group_queries<GRID, SHAPE, NQ>(a, g, lane, valid, qi, qx, qy, qz);
     using Acc = typename AccType<PREC>::T;
     Acc sum[NQ];
     int nt[NQ];
@@ -373,7 +397,7 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
         nt[u] = 0;
     }
 
-    static_assert(MODE == 0 || (GRID && NQ <= 3 && ORDER == 0), "interaction lists: grids, order 0");
+    static_assert(MODE == 0 || (NQ <= 3 && ORDER == 0), "interaction lists: order 0, at most 3 slots");
     unsigned rec = 0;  // list entries of this group (warp-uniform)
     int4* const out_list = (MODE == 2) ? a.list + a.list_off[g] : nullptr;
     auto leaf_points = [&](int start, int cnt, int u) {
@@ -580,21 +604,22 @@ __global__ void __launch_bounds__(kGwnWarps * 32, (GRID && kNqGrid >= 4) ? 2 : 3
 // With weight slots (a.wsel), mode 1 also writes the screening weight of
 // every node entry and sample; in mode 2 the launch returns at once and
 // k_gwn_wread reads them back.
-template <bool SCREENED, int PREC, int SHAPE>
+template <bool GRID, bool SCREENED, int PREC, int SHAPE>
 __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_replay(GwnArgs a) {
-    constexpr int NQ = kNqGrid;
-    static_assert(NQ == 2, "weight slots hold two samples per lane");
+    constexpr int NQ = nq_of<GRID>();
+    using WT = WeightOf<NQ>;
+    using W = typename WT::T;
     using Acc = typename AccType<PREC>::T;
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const float sigma = a.sigma_dev ? *a.sigma_dev : a.sigma;
     const float sigma_l2e = sigma * 1.4426950408889634f;
     int wmode = 0;
-    float2* wp = nullptr;
+    W* wp = nullptr;
     if (SCREENED && PREC < 2 && a.wsel) {
         wmode = a.wsel->mode;
         if (wmode == 2) return;  // k_gwn_wread reads the kept weights
-        wp = a.wbuf + (size_t)a.wsel->slot * a.wstride;
+        wp = reinterpret_cast<W*>(a.wbuf) + (size_t)a.wsel->slot * a.wstride;
     }
     unsigned long long my_terms = 0, my_node_terms = 0;
     for (;;) {
@@ -605,7 +630,7 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_replay(GwnArgs a) {
         bool valid[NQ];
         long long qi[NQ];
         float qx[NQ], qy[NQ], qz[NQ];
-        grid_queries<SHAPE, NQ>(a, g, lane, valid, qi, qx, qy, qz);
+        group_queries<GRID, SHAPE, NQ>(a, g, lane, valid, qi, qx, qy, qz);
         Acc sum[NQ];
         int nt[NQ], ntn = 0;
 #pragma unroll
@@ -646,7 +671,7 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_replay(GwnArgs a) {
                                                           nt[u]);
                         ntn += nt[u] - before;
                     }
-                    if (wmode == 1) __stcs(wp + (base + j) * 32 + lane, make_float2(gw[0], gw[1]));
+                    if (wmode == 1) __stcs(wp + (base + j) * 32 + lane, WT::pack(gw));
                 }
             }
         }
@@ -715,18 +740,20 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
-// chunk c of entries [e0, e1) into ring slot r: the weights (2 KB, 16-byte
+// chunk c of entries [e0, e1) into ring slot r: the weights (16-byte
 // pieces spread over the lanes) and the entries (lanes 0..7)
-__device__ __forceinline__ void wread_issue(const float2* __restrict__ wp, const int4* __restrict__ list,
+template <typename W>
+__device__ __forceinline__ void wread_issue(const W* __restrict__ wp, const int4* __restrict__ list,
                                             unsigned long long e0, unsigned long long e1, unsigned long long c,
-                                            float2* ws, int4* ls, int lane) {
+                                            W* ws, int4* ls, int lane) {
     const unsigned long long first = e0 + c * kWreadChunk;
     if (first < e1) {
-        constexpr int kPieces = kWreadChunk * 32 * 8 / 16;  // 16-byte pieces of a chunk's weights
+        constexpr int kPerEntry = 32 * (int)sizeof(W) / 16;  // 16-byte pieces per entry
+        constexpr int kPieces = kWreadChunk * kPerEntry;
 #pragma unroll
         for (int r = 0; r < kPieces / 32; ++r) {
             const int piece = lane + 32 * r;
-            const int k = piece / 16;  // entry of the piece (16 pieces per entry)
+            const int k = piece / kPerEntry;  // entry of the piece
             if (first + k < e1)
                 cp_async16(reinterpret_cast<char*>(ws) + piece * 16,
                            reinterpret_cast<const char*>(wp + first * 32) + piece * 16);
@@ -736,10 +763,13 @@ __device__ __forceinline__ void wread_issue(const float2* __restrict__ wp, const
     cp_async_commit();  // one group per chunk, empty past the end
 }
 
-template <bool SCREENED, int PREC, int SHAPE>
+template <bool GRID, bool SCREENED, int PREC, int SHAPE>
 __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_wread(GwnArgs a) {
-    constexpr int NQ = kNqGrid;
+    constexpr int NQ = nq_of<GRID>();
     constexpr int C = kWreadChunk;
+    using WT = WeightOf<NQ>;
+    using W = typename WT::T;
+    static_assert(sizeof(W) <= 8, "ring sized for two samples per lane");
     using Acc = typename AccType<PREC>::T;
     extern __shared__ __align__(16) unsigned char wread_smem[];
     const unsigned FULL = 0xffffffffu;
@@ -747,9 +777,9 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_wread(GwnArgs a) {
     if (wst->mode != 2) return;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    float2* const wring = reinterpret_cast<float2*>(wread_smem + warp * kWreadWarpBytes);
+    W* const wring = reinterpret_cast<W*>(wread_smem + warp * kWreadWarpBytes);
     int4* const lring = reinterpret_cast<int4*>(wread_smem + warp * kWreadWarpBytes + kWreadRing * C * 32 * 8);
-    const float2* const wp = a.wbuf + (size_t)wst->slot * a.wstride;
+    const W* const wp = reinterpret_cast<const W*>(a.wbuf) + (size_t)wst->slot * a.wstride;
     if (a.terms_total && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(a.terms_total, wst->node_terms[wst->slot]);
     const float sigma = a.sigma_dev ? *a.sigma_dev : a.sigma;
     const float sigma_l2e = sigma * 1.4426950408889634f;
@@ -762,7 +792,7 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_wread(GwnArgs a) {
         bool valid[NQ];
         long long qi[NQ];
         float qx[NQ], qy[NQ], qz[NQ];
-        grid_queries<SHAPE, NQ>(a, g, lane, valid, qi, qx, qy, qz);
+        group_queries<GRID, SHAPE, NQ>(a, g, lane, valid, qi, qx, qy, qz);
         Acc sum[NQ];
         int nt[NQ];
 #pragma unroll
@@ -780,7 +810,7 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_wread(GwnArgs a) {
             cp_async_wait_1();  // chunk c has landed (c + 1 may be in flight)
             __syncwarp();
             const int r = (int)(c % kWreadRing);
-            const float2* wc = wring + r * C * 32;
+            const W* wc = wring + r * C * 32;
             const int4* lc = lring + r * C;
             const unsigned long long first = e0 + c * C;
             const int cnt = e1 - first < (unsigned long long)C ? (int)(e1 - first) : C;
@@ -797,8 +827,8 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_wread(GwnArgs a) {
                         na_n = a.node_a[xn];
                         nb_n = a.node_b[xn];
                     }
-                    const float2 w = wc[k * 32 + lane];
-                    const float wu[2] = {w.x, w.y};
+                    float wu[NQ];
+                    WT::unpack(wc[k * 32 + lane], wu);
 #pragma unroll
                     for (int u = 0; u < NQ; ++u) {
                         const float dd = node_dot(nb, __fsub_rn(na.x, qx[u]), __fsub_rn(na.y, qy[u]),
@@ -817,7 +847,7 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_wread(GwnArgs a) {
                     const int st = (int)(meta & kMetaIndex), pc = __float_as_int(a.node_a[cidx].w);
 #pragma unroll
                     for (int u = 0; u < NQ; ++u) {
-                        if (((unsigned)(u ? e.z : e.y) >> lane) & 1u) {
+                        if (((unsigned)(u == 0 ? e.y : (u == 1 ? e.z : e.w)) >> lane) & 1u) {
                             const LeafSum<Acc> r = leaf_points_ool<SCREENED, PREC, Acc>(
                                 a.pa, a.nr, a.use_radii, a.screen, st, pc, qx[u], qy[u], qz[u], sigma, sigma_l2e,
                                 sum[u]);
@@ -827,8 +857,8 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_wread(GwnArgs a) {
                     }
                 } else {
                     const float4 na = a.node_a[e.x], nb = a.node_b[e.x];
-                    const float2 w = wc[k * 32 + lane];
-                    const float wu[2] = {w.x, w.y};
+                    float wu[NQ];
+                    WT::unpack(wc[k * 32 + lane], wu);
 #pragma unroll
                     for (int u = 0; u < NQ; ++u) {
                         const float dd = node_dot(nb, __fsub_rn(na.x, qx[u]), __fsub_rn(na.y, qy[u]),
@@ -1073,10 +1103,12 @@ __global__ void k_list_total(const unsigned int* __restrict__ count, unsigned lo
     off[n] = off[n - 1] + count[n - 1];
 }
 
-template <bool SCREENED, int PREC, int SHAPE>
+template <bool GRID, bool SCREENED, int PREC, int SHAPE>
 static int listed_shape(GwnArgs& a, GwnList& L, const Octree& t, cudaStream_t s, size_t max_bytes, bool* fallback) {
+    constexpr int NQ = nq_of<GRID>();
+    using W = typename WeightOf<NQ>::T;
     static int bps = 0;
-    if (!bps) bps = blocks_for(k_gwn_replay<SCREENED, PREC, SHAPE>);
+    if (!bps) bps = blocks_for(k_gwn_replay<GRID, SCREENED, PREC, SHAPE>);
     const long long grid_all = (long long)num_sms() * bps;
     const unsigned grid = (unsigned)(a.ngroups < grid_all * kGwnWarps ? (a.ngroups + kGwnWarps - 1) / kGwnWarps
                                                                       : grid_all);
@@ -1090,7 +1122,7 @@ static int listed_shape(GwnArgs& a, GwnList& L, const Octree& t, cudaStream_t s,
         c.out = nullptr;
         c.terms_total = nullptr;
         DWG_CHECK_CUDA(cudaMemsetAsync(t.work.ptr, 0, sizeof(unsigned int), s));
-        k_gwn<true, SCREENED, PREC, SHAPE, 0, 1><<<grid, kGwnWarps * 32, 0, s>>>(c);
+        k_gwn<GRID, SCREENED, PREC, SHAPE, 0, 1><<<grid, kGwnWarps * 32, 0, s>>>(c);
         DWG_CHECK_LAUNCH();
         size_t bytes = 0;
         DWG_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, L.count.ptr, L.off.ptr, (int)a.ngroups, s));
@@ -1118,7 +1150,7 @@ static int listed_shape(GwnArgs& a, GwnList& L, const Octree& t, cudaStream_t s,
         c.list_off = L.off.ptr;
         c.list = L.ent.ptr;
         DWG_CHECK_CUDA(cudaMemsetAsync(t.work.ptr, 0, sizeof(unsigned int), s));
-        k_gwn<true, SCREENED, PREC, SHAPE, 0, 2><<<grid, kGwnWarps * 32, 0, s>>>(c);
+        k_gwn<GRID, SCREENED, PREC, SHAPE, 0, 2><<<grid, kGwnWarps * 32, 0, s>>>(c);
         DWG_CHECK_LAUNCH();
         L.entries = total;
         L.valid = true;
@@ -1128,11 +1160,11 @@ static int listed_shape(GwnArgs& a, GwnList& L, const Octree& t, cudaStream_t s,
         if (SCREENED && PREC < 2 && L.wslots > 0 && total > 0) {
             size_t fr = 0, tot = 0;
             DWG_CHECK_CUDA(cudaMemGetInfo(&fr, &tot));
-            const unsigned long long per = total * 32ull * sizeof(float2);
+            const unsigned long long per = total * 32ull * sizeof(W);
             const unsigned long long cap = std::min<unsigned long long>(fr / 3, 64ull << 30);
             int n = (int)std::min<unsigned long long>((unsigned long long)std::min(L.wslots, kGwnWeightSlots),
                                                       cap / per);
-            if (n > 0 && L.w.reserve((size_t)n * total * 32) != DWG_OK) n = 0;
+            if (n > 0 && L.w.reserve(((size_t)n * per + sizeof(float2) - 1) / sizeof(float2)) != DWG_OK) n = 0;
             L.nslots = n;
             DWG_TRY(L.wstate.reserve(1));
             k_weight_reset<<<1, 1, 0, s>>>(L.wstate.ptr, n);
@@ -1149,54 +1181,76 @@ static int listed_shape(GwnArgs& a, GwnList& L, const Octree& t, cudaStream_t s,
         DWG_CHECK_LAUNCH();
     }
     DWG_CHECK_CUDA(cudaMemsetAsync(t.work.ptr, 0, sizeof(unsigned int), s));
-    k_gwn_replay<SCREENED, PREC, SHAPE><<<grid, kGwnWarps * 32, 0, s>>>(a);
+    k_gwn_replay<GRID, SCREENED, PREC, SHAPE><<<grid, kGwnWarps * 32, 0, s>>>(a);
     DWG_CHECK_LAUNCH();
     if (L.nslots > 0) {
         static int bpw = 0;
         if (!bpw) {
-            DWG_CHECK_CUDA(cudaFuncSetAttribute(k_gwn_wread<SCREENED, PREC, SHAPE>,
+            DWG_CHECK_CUDA(cudaFuncSetAttribute(k_gwn_wread<GRID, SCREENED, PREC, SHAPE>,
                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kWreadSmem));
-            DWG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpw, k_gwn_wread<SCREENED, PREC, SHAPE>,
+            DWG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpw, k_gwn_wread<GRID, SCREENED, PREC, SHAPE>,
                                                                          kGwnWarps * 32, kWreadSmem));
             if (bpw < 1) bpw = 1;
         }
         const long long all = (long long)num_sms() * bpw;
         const unsigned gw = (unsigned)(a.ngroups < all * kGwnWarps ? (a.ngroups + kGwnWarps - 1) / kGwnWarps : all);
-        k_gwn_wread<SCREENED, PREC, SHAPE><<<gw, kGwnWarps * 32, kWreadSmem, s>>>(a);
+        k_gwn_wread<GRID, SCREENED, PREC, SHAPE><<<gw, kGwnWarps * 32, kWreadSmem, s>>>(a);
         DWG_CHECK_LAUNCH();
     }
     return DWG_OK;
 }
 
-template <bool SCREENED, int PREC>
+template <bool GRID, int PREC>
 static int listed_prec(GwnArgs& a, GwnList& L, const Octree& t, int tile, cudaStream_t s, size_t max_bytes,
                        bool* fallback) {
+    if (!GRID) return listed_shape<GRID, true, PREC, 0>(a, L, t, s, max_bytes, fallback);
     switch (tile) {
-        case 1: return listed_shape<SCREENED, PREC, 1>(a, L, t, s, max_bytes, fallback);
-        case 2: return listed_shape<SCREENED, PREC, 2>(a, L, t, s, max_bytes, fallback);
-        case 3: return listed_shape<SCREENED, PREC, 3>(a, L, t, s, max_bytes, fallback);
-        default: return listed_shape<SCREENED, PREC, 0>(a, L, t, s, max_bytes, fallback);
+        case 1: return listed_shape<GRID, true, PREC, 1>(a, L, t, s, max_bytes, fallback);
+        case 2: return listed_shape<GRID, true, PREC, 2>(a, L, t, s, max_bytes, fallback);
+        case 3: return listed_shape<GRID, true, PREC, 3>(a, L, t, s, max_bytes, fallback);
+        default: return listed_shape<GRID, true, PREC, 0>(a, L, t, s, max_bytes, fallback);
     }
+}
+
+template <bool GRID>
+static int listed_dispatch(GwnArgs& a, GwnList& L, const Octree& t, const dwg_gwn_params& p, cudaStream_t s,
+                           size_t max_bytes) {
+    const int prec = p.precision < 0 ? 0 : (p.precision > 2 ? 2 : p.precision);
+    bool fallback = false;
+    if (prec == 0) DWG_TRY(listed_prec<GRID, 0>(a, L, t, p.tile, s, max_bytes, &fallback));
+    else if (prec == 1) DWG_TRY(listed_prec<GRID, 1>(a, L, t, p.tile, s, max_bytes, &fallback));
+    else DWG_TRY(listed_prec<GRID, 2>(a, L, t, p.tile, s, max_bytes, &fallback));
+    if (fallback) {
+        DWG_CHECK_CUDA(cudaMemsetAsync(t.work.ptr, 0, sizeof(unsigned int), s));
+        return dispatch<GRID>(a, p, s);
+    }
+    return DWG_OK;
 }
 
 int gwn_eval_listed(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, GwnList& L, float* out,
                     unsigned long long* terms_total, cudaStream_t s, const float* sigma_dev, size_t max_bytes,
                     int wslots) {
-    DWG_REQUIRE(!q.q && p.screened && p.order == 0, "gwn lists: screened grid sums only");
+    DWG_REQUIRE(p.screened && p.order == 0, "gwn lists: screened sums only");
     GwnArgs a;
     bool empty = false;
     DWG_TRY(make_args(t, q, p, out, terms_total, nullptr, s, sigma_dev, a, &empty));
-    const bool same = L.ngroups == a.ngroups && L.tile == p.tile && L.res[0] == q.res[0] && L.res[1] == q.res[1] &&
+    if (empty) return DWG_OK;
+    const bool grid = !q.q;
+    const bool same = L.ngroups == a.ngroups && L.grid == grid && L.qptr == q.q && L.nq == a.nq &&
+                      L.tile == (grid ? p.tile : 0) && L.res[0] == q.res[0] && L.res[1] == q.res[1] &&
                       L.res[2] == q.res[2] && L.zoff == q.zoff && L.origin[0] == q.origin[0] &&
                       L.origin[1] == q.origin[1] && L.origin[2] == q.origin[2] && L.spacing == q.spacing &&
                       L.beta == p.beta && L.use_radii == p.use_radii && L.wslots == wslots;
-    if (!same) {  // another grid or other decisions: record again
+    if (!same) {  // other samples or other decisions: record again
         L.valid = false;
         L.too_big = false;
     }
-    if (L.too_big) return dispatch<true>(a, p, s);
+    if (L.too_big) return grid ? dispatch<true>(a, p, s) : dispatch<false>(a, p, s);
     L.ngroups = a.ngroups;
-    L.tile = p.tile;
+    L.grid = grid;
+    L.qptr = q.q;
+    L.nq = a.nq;
+    L.tile = grid ? p.tile : 0;
     for (int d = 0; d < 3; ++d) {
         L.res[d] = q.res[d];
         L.origin[d] = q.origin[d];
@@ -1206,16 +1260,7 @@ int gwn_eval_listed(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p,
     L.beta = p.beta;
     L.use_radii = p.use_radii;
     L.wslots = wslots;
-    const int prec = p.precision < 0 ? 0 : (p.precision > 2 ? 2 : p.precision);
-    bool fallback = false;
-    if (prec == 0) DWG_TRY(listed_prec<true, 0>(a, L, t, p.tile, s, max_bytes, &fallback));
-    else if (prec == 1) DWG_TRY(listed_prec<true, 1>(a, L, t, p.tile, s, max_bytes, &fallback));
-    else DWG_TRY(listed_prec<true, 2>(a, L, t, p.tile, s, max_bytes, &fallback));
-    if (fallback) {
-        DWG_CHECK_CUDA(cudaMemsetAsync(t.work.ptr, 0, sizeof(unsigned int), s));
-        return dispatch<true>(a, p, s);
-    }
-    return DWG_OK;
+    return grid ? listed_dispatch<true>(a, L, t, p, s, max_bytes) : listed_dispatch<false>(a, L, t, p, s, max_bytes);
 }
 
 // ------------------------------------------------------------- batches --

@@ -61,7 +61,12 @@ struct GwnList {
     int nslots = 0;                      // weight slots held
     long long ngroups = 0;
     unsigned long long entries = 0;
-    // what the recorded decisions depend on besides the tree's centres
+    // what the recorded decisions depend on besides the tree's centres (the
+    // positions of point queries are the caller's to keep: same pointer, same
+    // points)
+    bool grid = true;
+    const float* qptr = nullptr;
+    long long nq = 0;
     int tile = -1, res[3] = {0, 0, 0}, zoff = 0, use_radii = 0;
     float origin[3] = {0, 0, 0}, spacing = 0, beta = 0;
     bool valid = false, too_big = false;
@@ -71,9 +76,10 @@ struct GwnList {
     ~GwnList();
 };
 
-// screened grid sums through L (recorded on the first call, recorded again
-// when the grid, tile, beta or use_radii differ); the caller resets L.valid
-// when the tree's centres of mass change.  A list above max_bytes (0: a
+// screened sums at a grid or at points through L (recorded on the first
+// call, recorded again when the grid, the query pointer or count, tile, beta
+// or use_radii differ); the caller resets L.valid when the tree's centres of
+// mass or the query points change.  A list above max_bytes (0: a
 // quarter of the free memory when it is recorded) is not kept.  wslots > 0
 // keeps screening weights for up to that many (sigma, screen) values (at most
 // kGwnWeightSlots; slots that do not fit in a third of the free memory, or

@@ -498,6 +498,23 @@ dwg_gwn_params Pipeline::gwn_params() const {
     return gp;
 }
 
+// grid_lists 2 also keeps the screening weights of every sigma of the
+// schedule's first total_iter iterations (20, then lambda and 10)
+int Pipeline::weight_slots() const {
+    int n = 0;
+    if (prm.grid_lists >= 2) {
+        float seen[kGwnWeightSlots];
+        const int iters = prm.total_iter > 0 ? prm.total_iter : 1;
+        for (int t = 0; t < iters && n < kGwnWeightSlots; ++t) {
+            const float sg = sigma_at(t, prm.lambda);
+            bool dup = false;
+            for (int c = 0; c < n; ++c) dup = dup || seen[c] == sg;
+            if (!dup) seen[n++] = sg;
+        }
+    }
+    return n;
+}
+
 // moments, GWN at the leaves, mean iso
 int Pipeline::iterate_pre() {
     k_iter_begin<<<1, 1, 0, s>>>(iter_dev.ptr, sigma_tab.ptr, half_tab.ptr, cur_sigma.ptr, cur_half.ptr,
@@ -511,7 +528,11 @@ int Pipeline::iterate_pre() {
     GwnQuery ql;
     ql.q = leaf_pos.ptr;
     ql.nq = L;
-    DWG_TRY(gwn_eval(t2, ql, gp, wleaf.ptr, terms_cur.ptr, nullptr, s, cur_sigma.ptr));
+    if (prm.grid_lists)
+        DWG_TRY(gwn_eval_listed(t2, ql, gp, llist, wleaf.ptr, terms_cur.ptr, s, cur_sigma.ptr, glist_budget,
+                                weight_slots()));
+    else
+        DWG_TRY(gwn_eval(t2, ql, gp, wleaf.ptr, terms_cur.ptr, nullptr, s, cur_sigma.ptr));
     // mean iso value, halved every 5th iteration (:541-550)
     return mean_to_iso(wleaf.ptr, L, iso_dev.ptr, cur_half.ptr, iso_hist.ptr, iter_dev.ptr, partial, s);
 }
@@ -526,23 +547,9 @@ int Pipeline::iterate_grid() {
     qg.res[2] = gnz;
     qg.zoff = gz0;
     qg.spacing = gh;
-    if (prm.grid_lists) {
-        // grid_lists 2 also keeps the screening weights of every sigma of the
-        // schedule's first total_iter iterations (20, then lambda and 10)
-        int wslots = 0;
-        if (prm.grid_lists >= 2) {
-            float seen[kGwnWeightSlots];
-            const int iters = prm.total_iter > 0 ? prm.total_iter : 1;
-            for (int t = 0; t < iters && wslots < kGwnWeightSlots; ++t) {
-                const float sg = sigma_at(t, prm.lambda);
-                bool dup = false;
-                for (int c = 0; c < wslots; ++c) dup = dup || seen[c] == sg;
-                if (!dup) seen[wslots++] = sg;
-            }
-        }
+    if (prm.grid_lists)
         return gwn_eval_listed(t2, qg, gwn_params(), glist, field.ptr, terms_cur.ptr, s, cur_sigma.ptr, glist_budget,
-                               wslots);
-    }
+                               weight_slots());
     return gwn_eval(t2, qg, gwn_params(), field.ptr, terms_cur.ptr, nullptr, s, cur_sigma.ptr);
 }
 

@@ -39,6 +39,8 @@ struct Pipeline {
     float gh = 0;
     DevBuf<float> field, wleaf;
     GwnList glist;               // interaction lists of the iteration grid (fixed leaves, fixed grid)
+    GwnList llist;               // interaction lists of the sums at the leaves (fixed leaves)
+    int weight_slots() const;    // sigmas of the schedule whose screening weights are kept
     size_t glist_budget = 0;     // largest list kept, bytes
     long long cap = 0;
     DevBuf<float> cent, tnrm;
