@@ -47,7 +47,7 @@ WORKLOAD = dict(workload="nonuniform torus 100k points, 256^3 grid, 30 DWG itera
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--points", type=int, default=WORKLOAD["points"])

@@ -303,7 +303,8 @@ struct TopK {
         mx = T;
         mpos = 0;
     }
-    // replace the maximum by v (v < mx) and find the new maximum
+    // replace the maximum by v (v < mx) and find the new maximum (a warp's
+    // lanes take the same steps whether or not their slots are all filled)
     __device__ __forceinline__ void replace_max(unsigned long long v) {
 #pragma unroll
         for (int q = 0; q < KMAX; ++q)
@@ -582,8 +583,21 @@ __global__ void k_kb_local(KnnGrid g, const int* __restrict__ cell_start, const 
                     const float4 p = pts[t];
                     const float ex = p.x - x, ey = p.y - y, ez = p.z - z;
                     const float d2 = ex * ex + ey * ey + ez * ez;
-                    ++cnt;
-                    if (d2 < mx) {
+                    if (cnt < kKnnBoundK) {  // the first keys fill the slots; the maximum once they are full
+#pragma unroll
+                        for (int q = 0; q < kKnnBoundK; ++q)
+                            if (q == cnt) d[q] = d2;
+                        if (cnt == kKnnBoundK - 1) {
+                            mx = d[0];
+                            mpos = 0;
+#pragma unroll
+                            for (int q = 1; q < kKnnBoundK; ++q)
+                                if (d[q] > mx) {
+                                    mx = d[q];
+                                    mpos = q;
+                                }
+                        }
+                    } else if (d2 < mx) {
 #pragma unroll
                         for (int q = 0; q < kKnnBoundK; ++q)
                             if (q == mpos) d[q] = d2;
@@ -596,6 +610,7 @@ __global__ void k_kb_local(KnnGrid g, const int* __restrict__ cell_start, const 
                                 mpos = q;
                             }
                     }
+                    ++cnt;
                 }
             }
         }
@@ -639,8 +654,21 @@ __global__ void k_kb_active(KnnGrid g, const int* __restrict__ cell_start, const
                             const float4 p = pts[s];
                             const float ex = p.x - x, ey = p.y - y, ez = p.z - z;
                             const float d2 = ex * ex + ey * ey + ez * ez;
-                            ++cnt;
-                            if (d2 < mx) {
+                            if (cnt < kKnnBoundK) {  // fill, then the maximum once
+#pragma unroll
+                                for (int q = 0; q < kKnnBoundK; ++q)
+                                    if (q == cnt) d[q] = d2;
+                                if (cnt == kKnnBoundK - 1) {
+                                    mx = d[0];
+                                    mpos = 0;
+#pragma unroll
+                                    for (int q = 1; q < kKnnBoundK; ++q)
+                                        if (d[q] > mx) {
+                                            mx = d[q];
+                                            mpos = q;
+                                        }
+                                }
+                            } else if (d2 < mx) {
 #pragma unroll
                                 for (int q = 0; q < kKnnBoundK; ++q)
                                     if (q == mpos) d[q] = d2;
@@ -653,6 +681,7 @@ __global__ void k_kb_active(KnnGrid g, const int* __restrict__ cell_start, const
                                         mpos = q;
                                     }
                             }
+                            ++cnt;
                         }
                     }
                 }
