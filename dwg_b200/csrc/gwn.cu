@@ -1139,14 +1139,15 @@ static int listed_shape(GwnArgs& a, GwnList& L, const Octree& t, cudaStream_t s,
             DWG_CHECK_CUDA(cudaMemGetInfo(&fr, &tot));
             max_bytes = fr / 4;
         }
-        if (total * sizeof(int4) > max_bytes) {  // too large to keep: traverse every time
+        // too large to keep, or no room for it: traverse every time
+        if (total * sizeof(int4) > max_bytes || L.ent.reserve(total ? total : 1) != DWG_OK) {
             L.too_big = true;
             L.count.release();
             L.off.release();
+            L.ent.release();
             *fallback = true;
             return DWG_OK;
         }
-        DWG_TRY(L.ent.reserve(total ? total : 1));
         c.list_off = L.off.ptr;
         c.list = L.ent.ptr;
         DWG_CHECK_CUDA(cudaMemsetAsync(t.work.ptr, 0, sizeof(unsigned int), s));

@@ -1042,6 +1042,26 @@ static int knn_launch(const KnnArgs& a, long long nq, cudaStream_t s) {
     return DWG_OK;
 }
 
+template <int KMAX>
+static int cells_launch(const KnnIndex& ix, const KnnArgs& a, long long nq, cudaStream_t s) {
+    static int bps = 0;
+    if (!bps) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_knn_cells<KMAX>, kCqWarps * 32, 0);
+        if (bps <= 0) bps = 1;
+    }
+    const long long grid = (long long)num_sms() * bps;
+    k_knn_cells<KMAX><<<(unsigned)grid, kCqWarps * 32, 0, s>>>(
+        a, ix.c_active.ptr, ix.c_misc.ptr, ix.c_start.ptr, ix.c_count.ptr, ix.c_m.ptr, ix.kb.ptr, ix.q_order.ptr,
+        ix.c_misc.ptr + 1, ix.c_fb.ptr);
+    DWG_CHECK_LAUNCH();
+    // the queries of cells whose candidate sets did not fit
+    KnnArgs f = a;
+    f.order = ix.c_fb.ptr;
+    f.nq_dev_i32 = ix.c_misc.ptr + 2;
+    f.kb = ix.kb.ptr;
+    return knn_launch<KMAX>(f, nq, s);
+}
+
 // queries grouped by cell (k <= 16, no exclusion), see k_knn_cells
 static int knn_query_cells(const KnnIndex& ix, const KnnArgs& a0, long long nq, cudaStream_t s) {
     if (!ix.kb_per_query && !ix.kb_ready) DWG_TRY(build_kbound(ix, s));
@@ -1082,22 +1102,9 @@ static int knn_query_cells(const KnnIndex& ix, const KnnArgs& a0, long long nq, 
     }
     k_cq_scatter<<<(unsigned)blocks, 256, 0, s>>>(a, ix.q_key.ptr, ix.c_fill.ptr, ix.q_order.ptr);
     DWG_CHECK_LAUNCH();
-    static int bps = 0;
-    if (!bps) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_knn_cells<16>, kCqWarps * 32, 0);
-        if (bps <= 0) bps = 1;
-    }
-    const long long grid = (long long)num_sms() * bps;
-    k_knn_cells<16><<<(unsigned)grid, kCqWarps * 32, 0, s>>>(
-        a, ix.c_active.ptr, ix.c_misc.ptr, ix.c_start.ptr, ix.c_count.ptr, ix.c_m.ptr, ix.kb.ptr, ix.q_order.ptr,
-        ix.c_misc.ptr + 1, ix.c_fb.ptr);
-    DWG_CHECK_LAUNCH();
-    // the queries of cells whose candidate sets did not fit
-    KnnArgs f = a;
-    f.order = ix.c_fb.ptr;
-    f.nq_dev_i32 = ix.c_misc.ptr + 2;
-    f.kb = ix.kb.ptr;
-    return knn_launch<16>(f, nq, s);
+    // k = 15 (the triangle and zero-repair queries) keeps 15 slots per lane
+    // instead of 16: every maximum search and the final sort are shorter
+    return a.k == 15 ? cells_launch<15>(ix, a, nq, s) : cells_launch<16>(ix, a, nq, s);
 }
 
 // ------------------------------------------------------------- subsets --
