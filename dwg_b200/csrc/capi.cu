@@ -24,6 +24,79 @@ void set_error(const char* fmt, ...) {
     va_end(ap);
 }
 
+size_t device_free_bytes() {
+    static std::mutex mu;
+    static size_t cached[64] = {0};
+    static bool have[64] = {false};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!have[dev]) {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) cached[dev] = fr;
+        have[dev] = true;
+    }
+    return cached[dev];
+}
+
+namespace {
+std::mutex g_recycle_mu;
+std::vector<std::pair<int, cudaStream_t>> g_streams;
+std::vector<std::pair<int, cudaEvent_t>> g_events;
+}  // namespace
+
+cudaStream_t stream_acquire() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    {
+        std::lock_guard<std::mutex> lock(g_recycle_mu);
+        for (size_t i = 0; i < g_streams.size(); ++i)
+            if (g_streams[i].first == dev) {
+                cudaStream_t s = g_streams[i].second;
+                g_streams.erase(g_streams.begin() + (long)i);
+                return s;
+            }
+    }
+    cudaStream_t s = nullptr;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+    return s;
+}
+
+void stream_release(cudaStream_t s) {
+    if (!s) return;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(g_recycle_mu);
+    if (g_streams.size() < 64) g_streams.emplace_back(dev, s);
+    else cudaStreamDestroy(s);
+}
+
+cudaEvent_t event_acquire() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    {
+        std::lock_guard<std::mutex> lock(g_recycle_mu);
+        for (size_t i = 0; i < g_events.size(); ++i)
+            if (g_events[i].first == dev) {
+                cudaEvent_t e = g_events[i].second;
+                g_events.erase(g_events.begin() + (long)i);
+                return e;
+            }
+    }
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+    return e;
+}
+
+void event_release(cudaEvent_t e) {
+    if (!e) return;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(g_recycle_mu);
+    if (g_events.size() < 64) g_events.emplace_back(dev, e);
+    else cudaEventDestroy(e);
+}
+
 int pool_alloc(void** p, size_t bytes) {
     static std::mutex mu;
     static bool configured[64] = {false};

@@ -54,6 +54,18 @@ struct Status {
 int pool_alloc(void** p, size_t bytes);
 void pool_free(void* p);
 
+// Free device memory as first seen by this process on the current device
+// (cached: blocks this library frees stay in its pool, so the first figure
+// is what its budgets can count on, and no driver query runs per pipeline).
+size_t device_free_bytes();
+
+// Streams and events recycled across pipelines (creating them per cloud
+// costs driver calls that other processes' monitoring can hold up).
+cudaStream_t stream_acquire();
+void stream_release(cudaStream_t s);
+cudaEvent_t event_acquire();
+void event_release(cudaEvent_t e);
+
 // Grow-only device buffer; owner frees.
 template <typename T>
 struct DevBuf {

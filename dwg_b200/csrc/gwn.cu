@@ -699,7 +699,8 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_replay(GwnArgs a) {
 // entry), so each warp streams its group's entries and weights through a
 // ring of kWreadRing chunks of kWreadChunk entries in shared memory with
 // cp.async (16-byte pieces, L2 only), two chunks in flight while it sums the
-// third.  The node terms a slot stands for were counted when it was written.
+// third; four 256-thread blocks per SM (64 registers, 52 KB of ring each).
+// The node terms a slot stands for were counted when it was written.
 constexpr int kWreadChunk = 8;
 
 // the points of a multi-point leaf for one sample, out of line (rare in the
@@ -764,7 +765,7 @@ __device__ __forceinline__ void wread_issue(const W* __restrict__ wp, const int4
 }
 
 template <bool GRID, bool SCREENED, int PREC, int SHAPE>
-__global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_wread(GwnArgs a) {
+__global__ void __launch_bounds__(kGwnWarps * 32, 4) k_gwn_wread(GwnArgs a) {
     constexpr int NQ = nq_of<GRID>();
     constexpr int C = kWreadChunk;
     using WT = WeightOf<NQ>;
@@ -1134,11 +1135,7 @@ static int listed_shape(GwnArgs& a, GwnList& L, const Octree& t, cudaStream_t s,
         unsigned long long total = 0;
         DWG_CHECK_CUDA(cudaMemcpyAsync(&total, L.off.ptr + a.ngroups, sizeof(total), cudaMemcpyDeviceToHost, s));
         DWG_CHECK_CUDA(cudaStreamSynchronize(s));
-        if (!max_bytes) {  // no budget given: a quarter of the free memory
-            size_t fr = 0, tot = 0;
-            DWG_CHECK_CUDA(cudaMemGetInfo(&fr, &tot));
-            max_bytes = fr / 4;
-        }
+        if (!max_bytes) max_bytes = device_free_bytes() / 4;  // no budget given: a quarter of the free memory
         // too large to keep, or no room for it: traverse every time
         if (total * sizeof(int4) > max_bytes || L.ent.reserve(total ? total : 1) != DWG_OK) {
             L.too_big = true;
@@ -1159,8 +1156,7 @@ static int listed_shape(GwnArgs& a, GwnList& L, const Octree& t, cudaStream_t s,
         // third of the free memory and 64 GB
         L.nslots = 0;
         if (SCREENED && PREC < 2 && L.wslots > 0 && total > 0) {
-            size_t fr = 0, tot = 0;
-            DWG_CHECK_CUDA(cudaMemGetInfo(&fr, &tot));
+            const size_t fr = device_free_bytes();
             const unsigned long long per = total * 32ull * sizeof(W);
             const unsigned long long cap = std::min<unsigned long long>(fr / 3, 64ull << 30);
             int n = (int)std::min<unsigned long long>((unsigned long long)std::min(L.wslots, kGwnWeightSlots),

@@ -227,8 +227,8 @@ Pipeline::~Pipeline() {
     if (s) cudaStreamSynchronize(s);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (graph) cudaGraphDestroy(graph);
-    if (ev) cudaEventDestroy(ev);
-    if (s) cudaStreamDestroy(s);
+    event_release(ev);
+    stream_release(s);
 }
 
 int Pipeline::join_in() {
@@ -324,8 +324,9 @@ int Pipeline::setup(const float* points_dev, const float* normals_dev, int n_poi
     DWG_REQUIRE(world == 1 || exchange, "pipeline: a sharded pipeline needs an exchange function");
     prm = p;
     caller = stream;
-    DWG_CHECK_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
-    DWG_CHECK_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    s = stream_acquire();
+    ev = event_acquire();
+    DWG_REQUIRE(s && ev, "pipeline: no CUDA stream or event");
     DWG_TRY(join_in());
     n = n_points;
     DWG_TRY(mc_upload_tables());
@@ -458,8 +459,7 @@ int Pipeline::setup(const float* points_dev, const float* normals_dev, int n_poi
     DWG_TRY(field.reserve((size_t)gres[0] * gres[1] * gnz));
     {
         // the grid's interaction lists may take a quarter of the free memory, at most 16 GB
-        size_t fr = 0, tot = 0;
-        DWG_CHECK_CUDA(cudaMemGetInfo(&fr, &tot));
+        const size_t fr = device_free_bytes();
         glist_budget = fr / 4 < ((size_t)16 << 30) ? fr / 4 : ((size_t)16 << 30);
     }
     DWG_TRY(wleaf.reserve(L));
