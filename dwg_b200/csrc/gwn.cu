@@ -1181,7 +1181,12 @@ static int listed_shape(GwnArgs& a, GwnList& L, const Octree& t, cudaStream_t s,
     k_gwn_replay<GRID, SCREENED, PREC, SHAPE><<<grid, kGwnWarps * 32, 0, s>>>(a);
     DWG_CHECK_LAUNCH();
     if (L.nslots > 0) {
-        static int bpw = 0;
+        // the ring's shared memory is opted into per device
+        static int bpw_dev[64] = {0};
+        int dev = 0;
+        DWG_CHECK_CUDA(cudaGetDevice(&dev));
+        DWG_REQUIRE(dev >= 0 && dev < 64, "gwn: device %d out of range", dev);
+        int& bpw = bpw_dev[dev];
         if (!bpw) {
             DWG_CHECK_CUDA(cudaFuncSetAttribute(k_gwn_wread<GRID, SCREENED, PREC, SHAPE>,
                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kWreadSmem));

@@ -120,8 +120,9 @@ typedef struct {
                         no traversal; 2 also keeps the terms' screening
                         weights for two (sigma, screen) values (precision 0
                         and 1): later calls with one of them read the weights
-                        instead of evaluating them, same bits; 0 traverses
-                        every call */
+                        instead of evaluating them, same bits (the calls of
+                        one octree must then follow each other on one
+                        stream); 0 traverses every call */
 } dwg_gwn_params;
 
 int dwg_gwn_points(dwg_octree* tree, const float* normals_dev, const float* areas_dev,
