@@ -424,6 +424,9 @@ def test_gwn_grid_lists_bit_identical(tile):
                 w = gt.grid(res, org, h, sigma=sigma, tile=tile, terms=t, lists=lists).cpu().numpy()
                 assert gt.status() == 0
                 runs[lists].append((w, int(t.item())))
+            if lists:  # the list kept for this grid, and its weight slots
+                entries, slots = gt.list_size()
+                assert entries > 0 and slots == (2 if lists == 2 else 0), (lists, entries, slots)
         for lists in (1, 2):
             for step, ((w0, t0), (w, t)) in enumerate(zip(runs[0], runs[lists])):
                 assert t0 > 0
