@@ -52,6 +52,9 @@ int Batch::setup(const float* const* points_dev, const int* counts, int n, const
             set_error("batch: cloud %d: %s", i, msg.c_str());
             return st;
         }
+        // the batch's persistent launch sums the grids of later iterations;
+        // lists of the first iteration's grid would only hold memory
+        clouds.back()->p.grid_batched = true;
     }
     // the grid sums of every cloud, one work list
     std::vector<GwnBatchItem> items((size_t)n);

@@ -8,6 +8,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "batch.cuh"
@@ -24,19 +25,26 @@ void set_error(const char* fmt, ...) {
     va_end(ap);
 }
 
+namespace {
+// bytes this library holds per device (pool blocks it has not freed), and
+// the memory it could count on when first asked: free then + held then
+std::mutex g_mem_mu;
+size_t g_live[64] = {0};
+size_t g_base[64] = {0};
+bool g_have_base[64] = {false};
+std::unordered_map<void*, std::pair<int, size_t>> g_sizes;
+}  // namespace
+
 size_t device_free_bytes() {
-    static std::mutex mu;
-    static size_t cached[64] = {0};
-    static bool have[64] = {false};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
-    std::lock_guard<std::mutex> lock(mu);
-    if (!have[dev]) {
+    std::lock_guard<std::mutex> lock(g_mem_mu);
+    if (!g_have_base[dev]) {
         size_t fr = 0, tot = 0;
-        if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) cached[dev] = fr;
-        have[dev] = true;
+        if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) g_base[dev] = fr + g_live[dev];
+        g_have_base[dev] = true;
     }
-    return cached[dev];
+    return g_base[dev] > g_live[dev] ? g_base[dev] - g_live[dev] : 0;
 }
 
 namespace {
@@ -116,15 +124,33 @@ int pool_alloc(void** p, size_t bytes) {
     cudaError_t e = cudaMallocAsync(p, bytes, cudaStreamLegacy);
     if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
     if (e != cudaSuccess) {
+        // the code is returned; a failed allocation must not stay behind as
+        // the runtime's last error (callers that fall back would meet it at
+        // their next launch check)
+        if (e == cudaErrorMemoryAllocation) cudaGetLastError();
         set_error("device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
         *p = nullptr;
         return e == cudaErrorMemoryAllocation ? DWG_ERR_NOMEM : DWG_ERR_CUDA;
+    }
+    if (dev >= 0 && dev < 64) {
+        std::lock_guard<std::mutex> lock(g_mem_mu);
+        g_live[dev] += bytes;
+        g_sizes[*p] = {dev, bytes};
     }
     return DWG_OK;
 }
 
 void pool_free(void* p) {
     if (!p) return;
+    {
+        std::lock_guard<std::mutex> lock(g_mem_mu);
+        auto it = g_sizes.find(p);
+        if (it != g_sizes.end()) {
+            const int dev = it->second.first;
+            g_live[dev] -= std::min(g_live[dev], it->second.second);
+            g_sizes.erase(it);
+        }
+    }
     // wait for every stream's use of the block, then return it to the pool
     if (cudaDeviceSynchronize() != cudaSuccess) return;
     cudaFreeAsync(p, cudaStreamLegacy);

@@ -54,9 +54,10 @@ struct Status {
 int pool_alloc(void** p, size_t bytes);
 void pool_free(void* p);
 
-// Free device memory as first seen by this process on the current device
-// (cached: blocks this library frees stay in its pool, so the first figure
-// is what its budgets can count on, and no driver query runs per pipeline).
+// Device memory this library can still count on: the free memory it first
+// saw on the current device (plus what it held then) minus the blocks it
+// holds now.  Freed blocks stay in its pool, so they count as available; no
+// driver query runs after the first call.
 size_t device_free_bytes();
 
 // Streams and events recycled across pipelines (creating them per cloud

@@ -547,7 +547,7 @@ int Pipeline::iterate_grid() {
     qg.res[2] = gnz;
     qg.zoff = gz0;
     qg.spacing = gh;
-    if (prm.grid_lists)
+    if (prm.grid_lists && !grid_batched)
         return gwn_eval_listed(t2, qg, gwn_params(), glist, field.ptr, terms_cur.ptr, s, cur_sigma.ptr, glist_budget,
                                weight_slots());
     return gwn_eval(t2, qg, gwn_params(), field.ptr, terms_cur.ptr, nullptr, s, cur_sigma.ptr);

@@ -40,6 +40,7 @@ struct Pipeline {
     DevBuf<float> field, wleaf;
     GwnList glist;               // interaction lists of the iteration grid (fixed leaves, fixed grid)
     GwnList llist;               // interaction lists of the sums at the leaves (fixed leaves)
+    bool grid_batched = false;   // a batch sums the grid after the first iteration: no grid lists
     int weight_slots() const;    // sigmas of the schedule whose screening weights are kept
     size_t glist_budget = 0;     // largest list kept, bytes
     long long cap = 0;
