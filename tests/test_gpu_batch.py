@@ -44,14 +44,17 @@ def results(lib, h):
             "field": get("field", (size("grid"),), np.float32), "tris": get("tris", (T, 9), np.float32)}
 
 
-@pytest.mark.parametrize("tile", [0, 3])
-def test_batch_equals_single_clouds(dwg_lib, tile):
+@pytest.mark.parametrize("tile,lists", [(0, 2), (3, 2), (0, 0), (3, 0)])
+def test_batch_equals_single_clouds(dwg_lib, tile, lists):
+    # the batch's persistent launch sums every cloud's grid; with lists 2 the
+    # sums at the leaves replay each cloud's lists and kept weights
     lib = dwg_lib
     P = clouds()
     grids = [48, 64, 56]
     iters = 6
     dev = [torch.from_numpy(p).cuda() for p in P]
-    prms = [capi.default_params(grid_reso=g, final_reso=g, total_iter=iters, tile=tile) for g in grids]
+    prms = [capi.default_params(grid_reso=g, final_reso=g, total_iter=iters, tile=tile, grid_lists=lists)
+            for g in grids]
     # one by one
     single = []
     for d, prm in zip(dev, prms):
