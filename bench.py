@@ -13,8 +13,11 @@ value       Mpts/s = points / step time (sum over ranks for --gpus N; every
             cross-GPU exchange)
 e2e         the same through dwg_reconstruct_host: pinned host points in,
             mesh + point normals out, copies inside the timed region
-roofline    the screened GWN grid kernel (dominant), FP32 pipe: 20 flops per
-            pair term (algorithmic), timed live with CUDA events
+roofline    the kernel that sums the iteration grid in 28 of 30 iterations
+            (k_gwn_wread, kept screening weights), HBM-bound: 272 algorithmic
+            bytes per interaction-list entry + 4 per sample, timed live with
+            CUDA events against the measured copy bandwidth; the evaluating
+            replay and the traversal (20 FP32 flops per pair term) beside it
 cpu_baseline  the FP64 CPU oracle's Barnes-Hut GWN on a bounded sample of the
             same workload, all host cores, scaled to a full reconstruction
 
