@@ -105,6 +105,45 @@ void event_release(cudaEvent_t e) {
     else cudaEventDestroy(e);
 }
 
+namespace {
+std::vector<std::pair<int, cudaGraphExec_t>> g_execs;  // guarded by g_recycle_mu
+}  // namespace
+
+int graph_exec_acquire(cudaGraph_t g, cudaGraphExec_t* out) {
+    int dev = 0;
+    DWG_CHECK_CUDA(cudaGetDevice(&dev));
+    cudaGraphExec_t e = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_recycle_mu);
+        for (size_t i = 0; i < g_execs.size(); ++i)
+            if (g_execs[i].first == dev) {
+                e = g_execs[i].second;
+                g_execs.erase(g_execs.begin() + (long)i);
+                break;
+            }
+    }
+    if (e) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(e, g, &info) == cudaSuccess) {
+            *out = e;
+            return DWG_OK;
+        }
+        cudaGetLastError();  // another shape: that executable is not reused
+        cudaGraphExecDestroy(e);
+    }
+    DWG_CHECK_CUDA(cudaGraphInstantiate(out, g, 0));
+    return DWG_OK;
+}
+
+void graph_exec_release(cudaGraphExec_t e) {
+    if (!e) return;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(g_recycle_mu);
+    if (g_execs.size() < 8) g_execs.emplace_back(dev, e);
+    else cudaGraphExecDestroy(e);
+}
+
 int pool_alloc(void** p, size_t bytes) {
     static std::mutex mu;
     static bool configured[64] = {false};

@@ -67,6 +67,13 @@ void stream_release(cudaStream_t s);
 cudaEvent_t event_acquire();
 void event_release(cudaEvent_t e);
 
+// An executable graph for g: a released executable of the same topology is
+// updated in place (cudaGraphExecUpdate: new buffers and arguments, no new
+// instantiation), otherwise g is instantiated.  release() keeps it for the
+// next pipeline of the same shape; it must be idle.
+int graph_exec_acquire(cudaGraph_t g, cudaGraphExec_t* out);
+void graph_exec_release(cudaGraphExec_t e);
+
 // Grow-only device buffer; owner frees.
 template <typename T>
 struct DevBuf {

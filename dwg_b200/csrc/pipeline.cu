@@ -225,7 +225,7 @@ void slab_range(int samples, int rank, int world, int* z0, int* nz) {
 // ------------------------------------------------------------------ setup --
 Pipeline::~Pipeline() {
     if (s) cudaStreamSynchronize(s);
-    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    graph_exec_release(graph_exec);  // idle: the stream was drained
     if (graph) cudaGraphDestroy(graph);
     event_release(ev);
     stream_release(s);
@@ -629,7 +629,7 @@ int Pipeline::iterate(int n_iters) {
                 }
                 DWG_CHECK_CUDA(e);
                 graph = gr;
-                DWG_CHECK_CUDA(cudaGraphInstantiate(&graph_exec, graph, 0));
+                DWG_TRY(graph_exec_acquire(graph, &graph_exec));
             }
             DWG_CHECK_CUDA(cudaGraphLaunch(graph_exec, s));
         } else {
