@@ -69,6 +69,24 @@ def test_default_params_match_dwg_cuda_flags(dwg_lib):
     assert abs(p.offset_1 - 0.05) < 1e-7 and abs(p.offset_2 - 0.01) < 1e-7
     assert abs(p.beta - 2.3) < 1e-6 and abs(p.area - 2e-6) < 1e-12 and abs(p.screen - 0.0015) < 1e-9
     assert (p.knn_tri, p.knn_zero) == (15, 10)
+    # this library's own switches: CUDA graphs on, FP32 terms summed in FP64,
+    # interaction lists with kept screening weights
+    assert (p.use_graph, p.precision, p.grid_lists, p.com_as) == (1, 1, 2, 0)
+
+
+def test_ctypes_structs_match_the_header():
+    # field names and order of the ctypes mirrors follow include/dwg_b200.h
+    import re
+    hdr = open(os.path.join(ROOT, "include", "dwg_b200.h")).read()
+
+    def fields(struct):
+        body = re.search(r"typedef struct\s*\{([^{}]*)\}\s*" + struct + r"\s*;", hdr).group(1)
+        body = re.sub(r"/\*.*?\*/", "", body, flags=re.S)
+        decls = re.findall(r"\b(?:int|float|double|long long)\s+([\w\s,]+);", body)
+        return [n.strip() for d in decls for n in d.split(",")]
+
+    assert [f for f, _ in capi.GwnParams._fields_] == fields("dwg_gwn_params")
+    assert [f.rstrip("_") for f, _ in capi.Params._fields_] == fields("dwg_params")
 
 
 def test_read_xyz_normalises_like_the_reference(dwg_lib, tmp_path):
