@@ -19,8 +19,10 @@ struct McWorkspace {
     DevBuf<unsigned char> scratch;
 };
 
-// generated tables (host copies)
-void mc_tables_host(int* edge_table, signed char* tri_table);
+// host copies of the case tables: edge masks from the cube geometry, the
+// reference's triangles per case; false if the triangles of a case do not
+// close into the polygons the geometry gives
+bool mc_tables_host(int* edge_table, signed char* tri_table);
 int mc_upload_tables();
 
 // count -> scan -> emit.  *num_tris_dev receives the full count (may exceed cap).

@@ -11,6 +11,7 @@
 #include <math.h>
 #include <pthread.h>
 #include <stdint.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -261,6 +262,45 @@ static inline double term_plain(double dx, double dy, double dz, double dot_an) 
     return dot_an / (4.0 * PI_D * r * r * r + 1e-8);
 }
 
+/* Gradients with respect to the query q of the two terms above (the
+ * reference has none; they are the analytic derivatives).  With
+ * (dx,dy,dz) = p - q, ne the term's weighted normal (A n, or sum A n of a
+ * node) and dot = ne.(p - q):
+ *   screened  v = G(rho) dot, G = (sigma rho + 1) / (e^{sigma rho} 4 pi rho^3 + 1e-7),
+ *             grad v = -G ne + dot G'(rho) grad rho, grad rho = -(p - q)/r when
+ *             r > s and 0 when the screen radius s takes over;
+ *   plain     v = dot / (4 pi r^3 + 1e-8),
+ *             grad v = -ne / den + dot 12 pi r (p - q) / den^2.
+ * Terms the value skips (r <= 1e-10 screened, r == 0 plain) add nothing. */
+static inline void grad_screened(double dx, double dy, double dz, const double ne[3], double s, double sigma,
+                                 double g[3]) {
+    const double r = sqrt(dx * dx + dy * dy + dz * dz);
+    if (!(r > 1e-10)) return;
+    const double rho = (s > r) ? s : r;
+    const double e = exp(rho * sigma);
+    const double den = e * (4.0 * PI_D * rho * rho * rho) + 1e-7;
+    const double up = rho * sigma + 1.0;
+    const double G = up / den;
+    const double dot = dx * ne[0] + dy * ne[1] + dz * ne[2];
+    const double dden = e * (sigma * 4.0 * PI_D * rho * rho * rho + 12.0 * PI_D * rho * rho);
+    const double Gp = (sigma * den - up * dden) / (den * den);
+    const double k = (s > r) ? 0.0 : -dot * Gp / r; /* dot G' grad rho = k (p - q) */
+    g[0] += -G * ne[0] + k * dx;
+    g[1] += -G * ne[1] + k * dy;
+    g[2] += -G * ne[2] + k * dz;
+}
+
+static inline void grad_plain(double dx, double dy, double dz, const double ne[3], double g[3]) {
+    const double r = sqrt(dx * dx + dy * dy + dz * dz);
+    if (r == 0.0) return;
+    const double den = 4.0 * PI_D * r * r * r + 1e-8;
+    const double dot = dx * ne[0] + dy * ne[1] + dz * ne[2];
+    const double k = dot * 12.0 * PI_D * r / (den * den);
+    g[0] += -ne[0] / den + k * dx;
+    g[1] += -ne[1] / den + k * dy;
+    g[2] += -ne[2] / den + k * dz;
+}
+
 /* higher-order far-field terms of igl::fast_winding_number's expansion_eval
  * (deps/libigl/include/igl/fast_winding_number.cpp:187-241), loc = CM - q:
  * order 1 adds sum_uv SecondDerivative(u,v) m1[u + 3v] with
@@ -310,13 +350,14 @@ typedef struct {
     float beta, sigma, screen;
     int screened, use_radii;
     double* out;
+    double* gout; /* nq x 3 gradients, or NULL */
     long long* terms;
     long long next;
     pthread_mutex_t mu;
 } bh_ctx;
 
 static inline void add_points(const bh_ctx* c, int node, double qx, double qy, double qz,
-                              double* acc, long long* nt) {
+                              double* acc, double* g, long long* nt) {
     const dwgo_octree* t = c->t;
     for (long long j = t->list_off[node]; j < t->list_off[node + 1]; j++) {
         int i = t->flat[j];
@@ -324,15 +365,20 @@ static inline void add_points(const bh_ctx* c, int node, double qx, double qy, d
                dz = (double)c->P[(size_t)i * 3 + 2] - qz;
         double dot = (double)c->A[i] *
                      (dx * c->N[(size_t)i * 3] + dy * c->N[(size_t)i * 3 + 1] + dz * c->N[(size_t)i * 3 + 2]);
+        double ne[3] = {0, 0, 0};
+        if (g)
+            for (int d = 0; d < 3; d++) ne[d] = (double)c->A[i] * (double)c->N[(size_t)i * 3 + d];
         if (c->screened) {
             double s = c->use_radii ? (double)c->radii[i] : (double)c->screen, v;
             if (term_screened(dx, dy, dz, dot, s, c->sigma, &v)) {
                 *acc += v;
                 (*nt)++;
+                if (g) grad_screened(dx, dy, dz, ne, s, c->sigma, g);
             }
         } else {
             *acc += term_plain(dx, dy, dz, dot);
             (*nt)++;
+            if (g) grad_plain(dx, dy, dz, ne, g);
         }
     }
 }
@@ -351,12 +397,12 @@ static inline int is_far(const bh_ctx* c, int node, float qx, float qy, float qz
     return dist > lim;
 }
 
-static void bh_visit(const bh_ctx* c, int node, float qxf, float qyf, float qzf, double* acc,
+static void bh_visit(const bh_ctx* c, int node, float qxf, float qyf, float qzf, double* acc, double* g,
                      long long* nt) {
     const dwgo_octree* t = c->t;
     double qx = qxf, qy = qyf, qz = qzf;
     if (t->children[(size_t)node * 8] == -1) {
-        add_points(c, node, qx, qy, qz, acc, nt);
+        add_points(c, node, qx, qy, qz, acc, g, nt);
         return;
     }
     for (int k = 0; k < 8; k++) {
@@ -364,26 +410,28 @@ static void bh_visit(const bh_ctx* c, int node, float qxf, float qyf, float qzf,
         if (t->lcount[ch] <= 0) continue;
         if (is_far(c, ch, qxf, qyf, qzf)) {
             if (t->children[(size_t)ch * 8] == -1) {
-                add_points(c, ch, qx, qy, qz, acc, nt);
+                add_points(c, ch, qx, qy, qz, acc, g, nt);
             } else {
                 double dx = c->CM[(size_t)ch * 3] - qx, dy = c->CM[(size_t)ch * 3 + 1] - qy,
                        dz = c->CM[(size_t)ch * 3 + 2] - qz;
-                double dot = dx * c->EC[(size_t)ch * 3] + dy * c->EC[(size_t)ch * 3 + 1] +
-                             dz * c->EC[(size_t)ch * 3 + 2];
+                const double* ne = c->EC + (size_t)ch * 3;
+                double dot = dx * ne[0] + dy * ne[1] + dz * ne[2];
                 if (c->screened) {
                     double v;
                     if (term_screened(dx, dy, dz, dot, (double)c->screen, c->sigma, &v)) {
                         *acc += v;
                         (*nt)++;
+                        if (g) grad_screened(dx, dy, dz, ne, (double)c->screen, c->sigma, g);
                     }
                 } else {
                     *acc += term_plain(dx, dy, dz, dot) +
                             (c->order > 0 ? expansion_terms(dx, dy, dz, c->HO + (size_t)ch * 36, c->order) : 0.0);
                     (*nt)++;
+                    if (g) grad_plain(dx, dy, dz, ne, g);
                 }
             }
         } else {
-            bh_visit(c, ch, qxf, qyf, qzf, acc, nt);
+            bh_visit(c, ch, qxf, qyf, qzf, acc, g, nt);
         }
     }
 }
@@ -399,11 +447,13 @@ static void* bh_worker(void* arg) {
         if (s >= c->nq) break;
         long long e = s + chunk < c->nq ? s + chunk : c->nq;
         for (long long q = s; q < e; q++) {
-            double acc = 0;
+            double acc = 0, g[3] = {0, 0, 0};
             long long nt = 0;
             if (c->t->lcount[0] > 0)
-                bh_visit(c, 0, c->Q[q * 3], c->Q[q * 3 + 1], c->Q[q * 3 + 2], &acc, &nt);
+                bh_visit(c, 0, c->Q[q * 3], c->Q[q * 3 + 1], c->Q[q * 3 + 2], &acc, c->gout ? g : NULL, &nt);
             c->out[q] = acc;
+            if (c->gout)
+                for (int d = 0; d < 3; d++) c->gout[q * 3 + d] = g[d];
             if (c->terms) c->terms[q] = nt;
         }
     }
@@ -425,9 +475,11 @@ static void gwn_bh_impl(const dwgo_octree* t, const float* P, const float* N,
                         const float* A, const float* radii, const double* CM,
                         const double* R, const double* EC, const double* HO, int order,
                         const float* Q, long long nq, float beta, float sigma, int screened,
-                        int use_radii, float screen, int nthreads, double* out, long long* terms) {
+                        int use_radii, float screen, int nthreads, double* out, double* gout,
+                        long long* terms) {
     bh_ctx c;
     memset(&c, 0, sizeof(c));
+    c.gout = gout;
     c.HO = HO;
     c.order = order;
     c.t = t;
@@ -463,13 +515,22 @@ void dwgo_gwn_bh(const dwgo_octree* t, const float* P, const float* N,
                  float beta, float sigma, int screened, int use_radii,
                  float screen, int nthreads, double* out, long long* terms) {
     gwn_bh_impl(t, P, N, A, radii, CM, R, EC, NULL, 0, Q, nq, beta, sigma, screened, use_radii, screen,
-                nthreads, out, terms);
+                nthreads, out, NULL, terms);
+}
+
+void dwgo_gwn_bh_grad(const dwgo_octree* t, const float* P, const float* N,
+                      const float* A, const float* radii, const double* CM,
+                      const double* R, const double* EC, const float* Q, long long nq,
+                      float beta, float sigma, int screened, int use_radii,
+                      float screen, int nthreads, double* out, double* grad_out) {
+    gwn_bh_impl(t, P, N, A, radii, CM, R, EC, NULL, 0, Q, nq, beta, sigma, screened, use_radii, screen,
+                nthreads, out, grad_out, NULL);
 }
 
 void dwgo_fwn(const dwgo_octree* t, const float* P, const float* N, const float* A,
               const double* CM, const double* R, const double* EC, const double* HO, int order,
               const float* Q, long long nq, float beta, int nthreads, double* out, long long* terms) {
-    gwn_bh_impl(t, P, N, A, NULL, CM, R, EC, HO, order, Q, nq, beta, 0.f, 0, 0, 0.f, nthreads, out, terms);
+    gwn_bh_impl(t, P, N, A, NULL, CM, R, EC, HO, order, Q, nq, beta, 0.f, 0, 0, 0.f, nthreads, out, NULL, terms);
 }
 
 void dwgo_expansion(const dwgo_octree* t, const float* P, const float* N, const float* A,
@@ -627,15 +688,27 @@ void dwgo_grid_points(const int res[3], const float origin[3], float spacing, fl
 }
 
 /* ------------------------------------------------------------------------ */
-/* marching cubes tables, generated (not transcribed)                        */
+/* marching cubes tables                                                     */
 /* Corner c sits at (x + (b0 != b1), y + b1, z + !b2) (src/TurboMC.cu:408-413)*/
 /* edge e joins (e & 7, e<4 ? (e+1)&3 : e<8 ? 4+((e-3)&3) : e-4) (:433-434). */
-/* Polygons: on every face, crossing edges pair up; an ambiguous face cuts   */
-/* off the corners above the iso value.  Loops are oriented so that, seen    */
-/* from outside the cube with the face corners counter-clockwise, each face  */
-/* segment runs from the crossing entered from a corner below the iso value. */
-/* Each loop is fanned from its lowest edge index.                           */
+/* Edge masks follow from the corners.  The triangles of each case are the   */
+/* reference's (src/TurboMC.cu:57-314), handed in by dwgo_mc_set_triangles   */
+/* from the fixture tests/golden/mc_reference_loops.json (the front end does */
+/* this when it loads the library).  dwgo_mc_polygons gives the polygons the */
+/* cube geometry implies, fanned from their lowest edge, for the tests that  */
+/* check the triangles against them: on every face, crossing edges pair up;  */
+/* an ambiguous face cuts off the corners above the iso value; loops are     */
+/* oriented so that, seen from outside the cube with the face corners        */
+/* counter-clockwise, each face segment runs from the crossing entered from  */
+/* a corner below the iso value.                                             */
 /* ------------------------------------------------------------------------ */
+static signed char mc_ref_tris[256 * 16];
+static int mc_ref_tris_set = 0;
+
+void dwgo_mc_set_triangles(const signed char* tri_table) {
+    memcpy(mc_ref_tris, tri_table, sizeof(mc_ref_tris));
+    mc_ref_tris_set = 1;
+}
 static const int MC_CORNER[8][3] = {{0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1},
                                     {0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}};
 static int mc_edge_a(int e) { return e & 7; }
@@ -646,7 +719,7 @@ static int mc_edge_of(int a, int b) {
     return -1;
 }
 
-void dwgo_mc_tables(int* edge_table, signed char* tri_table) {
+void dwgo_mc_polygons(int* edge_table, signed char* tri_table) {
     /* faces: the 4 corners of each face in counter-clockwise order seen from
      * outside */
     int faces[6][4];
@@ -755,6 +828,15 @@ void dwgo_mc_tables(int* edge_table, signed char* tri_table) {
         if (row)
             for (; w < 16; w++) row[w] = -1;
     }
+}
+
+void dwgo_mc_tables(int* edge_table, signed char* tri_table) {
+    if (!mc_ref_tris_set) {
+        fprintf(stderr, "dwg oracle: marching-cubes triangles not set (dwgo_mc_set_triangles)\n");
+        abort();
+    }
+    dwgo_mc_polygons(edge_table, NULL);
+    if (tri_table) memcpy(tri_table, mc_ref_tris, sizeof(mc_ref_tris));
 }
 
 long long dwgo_marching_cubes(const float* field, const int res[3],

@@ -52,6 +52,13 @@ void dwgo_gwn_bh(const dwgo_octree* t, const float* P, const float* N,
                  const double* R, const double* EC, const float* Q, long long nq,
                  float beta, float sigma, int screened, int use_radii,
                  float screen, int nthreads, double* out, long long* terms);
+/* the same sums and their analytic gradients with respect to the query
+ * (grad_out: nq x 3), same decisions; order-0 far field */
+void dwgo_gwn_bh_grad(const dwgo_octree* t, const float* P, const float* N,
+                      const float* A, const float* radii, const double* CM,
+                      const double* R, const double* EC, const float* Q, long long nq,
+                      float beta, float sigma, int screened, int use_radii,
+                      float screen, int nthreads, double* out, double* grad_out);
 /* igl::fast_winding_number's expansion coefficients of orders 1 and 2
  * (deps/libigl/include/igl/fast_winding_number.cpp:87-105), 36 per node:
  * m1[u + 3v] = sum A a_u n_v, m2[9i + u + 3v] = sum 0.5 a_i A a_u n_v with
@@ -77,7 +84,14 @@ void dwgo_grid_points(const int res[3], const float origin[3], float spacing,
                       float* out);
 
 /* ---- marching cubes (src/TurboMC.cu:373-478) ---- */
+/* the reference's triangles per case (256 x 16 edge indices, -1 padded); must
+ * be set before any marching-cubes call */
+void dwgo_mc_set_triangles(const signed char* tri_table);
+/* edge masks and the set triangles */
 void dwgo_mc_tables(int* edge_table, signed char* tri_table);
+/* edge masks and the polygons of the cube geometry, fanned from their lowest
+ * edge (tri_table may be NULL) */
+void dwgo_mc_polygons(int* edge_table, signed char* tri_table);
 long long dwgo_marching_cubes(const float* field, const int res[3],
                               const float origin[3], float spacing, float iso,
                               float* tris, float* centroids, float* normals,

@@ -44,6 +44,23 @@ class Params(C.Structure):
     ]
 
 
+_FIXTURE = os.path.join(os.path.dirname(_HERE), "tests", "golden", "mc_reference_loops.json")
+
+
+def _reference_triangles():
+    """The reference's triangles per case (src/TurboMC.cu:57-314) from the
+    committed fixture (tests/golden/make_mc_fixture.py), as 256 x 16 int8."""
+    import json
+
+    with open(_FIXTURE) as f:
+        cases = json.load(f)["cases"]
+    tt = np.full((256, 16), -1, np.int8)
+    for c in cases:
+        flat = [e for t in c["tris"] for e in t]
+        tt[c["case"], : len(flat)] = flat
+    return tt.reshape(-1)
+
+
 def lib():
     global _lib
     if _lib is not None:
@@ -64,12 +81,18 @@ def lib():
     L.dwgo_gwn_bh.argtypes = [vp, _f32p, _f32p, _f32p, _f32p, _f64p, _f64p, _f64p, _f32p,
                               C.c_longlong, C.c_float, C.c_float, C.c_int, C.c_int, C.c_float,
                               C.c_int, _f64p, _i64p]
+    L.dwgo_gwn_bh_grad.argtypes = [vp, _f32p, _f32p, _f32p, _f32p, _f64p, _f64p, _f64p, _f32p,
+                                   C.c_longlong, C.c_float, C.c_float, C.c_int, C.c_int, C.c_float,
+                                   C.c_int, _f64p, _f64p]
     L.dwgo_gwn_exact.argtypes = [_f32p, _f32p, _f32p, _f32p, C.c_int, _f32p, C.c_longlong,
                                  C.c_float, C.c_int, C.c_int, C.c_float, C.c_int, _f64p]
     L.dwgo_voxel_grid.argtypes = [_f32p, C.c_int, C.c_float, C.c_int, _i32p, _f32p,
                                   C.POINTER(C.c_float)]
     L.dwgo_grid_points.argtypes = [_i32p, _f32p, C.c_float, _f32p]
     L.dwgo_mc_tables.argtypes = [_i32p, _i8p]
+    L.dwgo_mc_polygons.argtypes = [_i32p, _i8p]
+    L.dwgo_mc_set_triangles.argtypes = [_i8p]
+    L.dwgo_mc_set_triangles(_reference_triangles())
     L.dwgo_marching_cubes.restype = C.c_longlong
     L.dwgo_marching_cubes.argtypes = [_f32p, _i32p, _f32p, C.c_float, C.c_float, vp, vp, vp,
                                       C.c_longlong, vp]
@@ -200,6 +223,24 @@ class Octree:
                           int(radii is not None), screen, nthreads or NTHREADS, out, terms)
         return out[:nq], terms[:nq]
 
+    def gwn_grad(self, P, N, A, Q, beta=2.3, sigma=0.0, screened=True, radii=None, screen=0.0015,
+                 moments=None, nthreads=None):
+        """The sums of :meth:`gwn` and their analytic gradients with respect to
+        the query (same decisions, FP64).  Returns (w, grad (nq x 3))."""
+        P = _f32(P).reshape(-1)
+        N = _f32(N).reshape(-1)
+        A = _f32(A)
+        Q = _f32(Q).reshape(-1)
+        nq = len(Q) // 3
+        rad = _f32(radii) if radii is not None else np.zeros(1, np.float32)
+        CM, R, EC = moments if moments is not None else self.moments(P.reshape(-1, 3), N.reshape(-1, 3), A)
+        out = np.empty(max(nq, 1), np.float64)
+        g = np.empty(max(nq, 1) * 3, np.float64)
+        lib().dwgo_gwn_bh_grad(self._h, P, N, A, rad, np.ascontiguousarray(CM), np.ascontiguousarray(R),
+                               np.ascontiguousarray(EC), Q, nq, beta, sigma, int(screened),
+                               int(radii is not None), screen, nthreads or NTHREADS, out, g)
+        return out[:nq], g[: nq * 3].reshape(nq, 3)
+
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:
             _lib.dwgo_octree_free(self._h)
@@ -236,9 +277,21 @@ def grid_points(res, origin, spacing):
 
 
 def mc_tables():
+    """Edge masks and the reference's triangles per case (what the oracle's
+    marching cubes uses)."""
     et = np.empty(256, np.int32)
     tt = np.empty(256 * 16, np.int8)
     lib().dwgo_mc_tables(et, tt)
+    return et, tt.reshape(256, 16)
+
+
+def mc_polygons():
+    """Edge masks and the polygons the cube geometry implies, each fanned from
+    its lowest edge (the oracle's own derivation, checked against the
+    reference's triangles by the tests)."""
+    et = np.empty(256, np.int32)
+    tt = np.empty(256 * 16, np.int8)
+    lib().dwgo_mc_polygons(et, tt)
     return et, tt.reshape(256, 16)
 
 

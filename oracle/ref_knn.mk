@@ -2,8 +2,8 @@
 # src/KNN_GWN.cu) from the reference sources in place, plus the C shim of this
 # directory, into _ref/libref_knn.so.  Test infrastructure only (a comparator).
 # Needs the reference checkout; the output is git-ignored and travels with the
-# repository snapshot.  Usage: make -f ref_knn.mk [REF=/root/reference]
-REF ?= /root/reference
+# repository snapshot.  Usage: make -f ref_knn.mk REF=<reference checkout> (default: $DWG_REFERENCE)
+REF ?= $(DWG_REFERENCE)
 NVCC ?= /usr/local/cuda/bin/nvcc
 HERE := $(dir $(abspath $(lastword $(MAKEFILE_LIST))))
 OUT := $(HERE)_ref/libref_knn.so

@@ -32,13 +32,17 @@ def test_library_exports_every_declared_symbol(dwg_lib):
     assert dwg_lib.dwg_version().startswith(b"dwg_b200")
 
 
-def test_generated_table_matches_reference_fixture_and_oracle(dwg_lib, oracle_lib):
-    from tests.test_oracle import check_table_against_fixture
+def test_mc_table_matches_reference_fixture_and_oracle(dwg_lib, oracle_lib):
+    """Edge masks from the cube geometry; triangles per case equal to the
+    reference's (the fixture read from src/TurboMC.cu), which the library
+    checks against the polygons the geometry gives."""
+    from tests.test_oracle import check_table_against_fixture, reference_triangles
     et = np.zeros(256, np.int32)
     tt = np.zeros(256 * 16, np.int8)
     assert dwg_lib.dwg_mc_tables(et.ctypes.data, tt.ctypes.data) == 0
     tt = tt.reshape(256, 16)
     check_table_against_fixture(et, tt)
+    assert np.array_equal(tt, reference_triangles())
     oet, ott = oracle_lib.mc_tables()
     assert np.array_equal(et, oet) and np.array_equal(tt, ott)
 

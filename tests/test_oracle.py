@@ -52,9 +52,24 @@ def check_table_against_fixture(et, tt):
         assert et[ci] == mask
 
 
+def reference_triangles():
+    g = json.load(open(GOLDEN))
+    tt = np.full((256, 16), -1, np.int8)
+    for c in g["cases"]:
+        flat = [e for t in c["tris"] for e in t]
+        tt[c["case"], : len(flat)] = flat
+    return tt
+
+
 def test_oracle_mc_table_matches_reference_fixture(oracle_lib):
-    et, tt = oracle_lib.mc_tables()
-    check_table_against_fixture(et, tt)
+    # the oracle's own polygons from the cube geometry are the reference's ...
+    et, tp = oracle_lib.mc_polygons()
+    check_table_against_fixture(et, tp)
+    # ... and it triangulates them with the reference's triangles
+    et2, tt = oracle_lib.mc_tables()
+    assert np.array_equal(et, et2)
+    assert np.array_equal(tt, reference_triangles())
+    check_table_against_fixture(et2, tt)
 
 
 def test_oracle_sphere_gwn_known_answer(oracle_lib):
@@ -287,3 +302,28 @@ def test_oracle_fwn_sphere_order2_beats_order0(oracle_lib):
     rms0 = np.sqrt(np.mean((w0 - exact) ** 2))
     rms2 = np.sqrt(np.mean((w2 - exact) ** 2))
     assert rms2 < rms0 / 3
+
+
+@pytest.mark.parametrize("screened,sigma", [(True, 20.0), (False, 0.0)])
+def test_oracle_gradient_matches_central_differences(oracle_lib, screened, sigma):
+    """The oracle's analytic gradient of the exact sum (beta = 1e30 opens every
+    node, so no decision moves under the perturbation) against central
+    differences of its value, at h = 1e-5 (the error falls as h^2)."""
+    P, N = D.torus(3000, seed=3)
+    Pn, _, _ = D.normalize(P)
+    A = np.full(len(Pn), 2e-6, np.float32)
+    rng = np.random.default_rng(1)
+    Q = (Pn[:50] + rng.normal(0, 0.02, (50, 3))).astype(np.float64)
+    t = oracle_lib.Octree(Pn, 8)
+    w, g = t.gwn_grad(Pn, N, A, Q.astype(np.float32), beta=1e30, sigma=sigma, screened=screened)
+    w0, _ = t.gwn(Pn, N, A, Q.astype(np.float32), beta=1e30, sigma=sigma, screened=screened)
+    assert np.array_equal(w, w0)
+    fd = np.zeros_like(g)
+    for d in range(3):
+        e = np.zeros(3)
+        e[d] = 1e-5
+        qp, qm = (Q + e).astype(np.float32), (Q - e).astype(np.float32)
+        wp, _ = t.gwn(Pn, N, A, qp, beta=1e30, sigma=sigma, screened=screened)
+        wm, _ = t.gwn(Pn, N, A, qm, beta=1e30, sigma=sigma, screened=screened)
+        fd[:, d] = (wp - wm) / (qp[:, d].astype(np.float64) - qm[:, d])
+    assert np.abs(fd - g).max() <= 2e-5 * np.abs(g).max()
