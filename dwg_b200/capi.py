@@ -70,6 +70,10 @@ _SIGS = {
     "dwg_gwn_points": (_i, [_vp, _vp, _vp, _vp, _vp, _ll, C.POINTER(GwnParams), _vp, _vp, _vp]),
     "dwg_gwn_points_counted": (_i, [_vp, _vp, _vp, _vp, _vp, _ll, C.POINTER(GwnParams), _vp, _vp, _vp]),
     "dwg_gwn_grid": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _f, C.POINTER(GwnParams), _vp, _vp, _vp]),
+    "dwg_gwn_points_grad": (_i, [_vp, _vp, _vp, _vp, _vp, _ll, C.POINTER(GwnParams), _vp, _vp, _vp]),
+    "dwg_gwn_grid_grad": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _f, C.POINTER(GwnParams), _vp, _vp, _vp]),
+    "dwg_gwn_points_fp64": (_i, [_vp, _vp, _vp, _vp, _vp, _ll, C.POINTER(GwnParams), _vp, _vp, _vp]),
+    "dwg_gwn_grid_fp64": (_i, [_vp, _vp, _vp, _vp, _vp, _vp, _f, C.POINTER(GwnParams), _vp, _vp, _vp]),
     "dwg_voxel_grid": (_i, [_vp, _i, _f, _i, _vp, _vp, _vp, _vp]),
     "dwg_marching_cubes": (_i, [_vp, _vp, _vp, _vp, _f, _f, _vp, _vp, _vp, _ll, _vp, _vp, _vp]),
     "dwg_mc_tables": (_i, [_vp, _vp]),

@@ -392,11 +392,79 @@ int dwg_gwn_grid(dwg_octree* tree, const float* normals_dev, const float* areas_
         if (params && params->lists && params->screened && params->order == 0) {
             DWG_REQUIRE(tree && out_dev, "gwn_grid: null argument");
             DWG_TRY(octree_set_point_data(tree->t, normals_dev, areas_dev, radii_dev, S(stream)));
+            // kept screening weights use the points' radii (use_radii): new
+            // radii make them stale
+            if (radii_dev) DWG_TRY(gwn_list_drop_weights(tree->list, S(stream)));
             if (normals_dev || areas_dev) DWG_TRY(octree_update_normals(tree->t, S(stream)));
             return gwn_eval_listed(tree->t, q, *params, tree->list, out_dev, terms_dev, S(stream), nullptr, 0,
                                    params->lists >= 2 ? 2 : 0);
         }
         return gwn_common(tree, normals_dev, areas_dev, radii_dev, q, params, out_dev, terms_dev, nullptr, stream);
+    })
+}
+
+static int gwn_thread_common(dwg_octree* tree, const float* normals_dev, const float* areas_dev,
+                             const float* radii_dev, const GwnQuery& q, const dwg_gwn_params* params, bool fp64,
+                             void* out_w, void* out_g, void* stream) {
+    DWG_REQUIRE(tree && params && (out_w || out_g), "gwn: null argument");
+    DWG_TRY(octree_set_point_data(tree->t, normals_dev, areas_dev, radii_dev, S(stream)));
+    if (normals_dev || areas_dev) DWG_TRY(octree_update_normals(tree->t, S(stream)));
+    return gwn_eval_thread(tree->t, q, *params, fp64, out_w, out_g, S(stream));
+}
+
+int dwg_gwn_points_grad(dwg_octree* tree, const float* normals_dev, const float* areas_dev, const float* radii_dev,
+                        const float* queries_dev, long long num_queries, const dwg_gwn_params* params,
+                        float* out_dev, float* grad_dev, void* stream) {
+    API_GUARD({
+        DWG_REQUIRE(num_queries >= 0 && (queries_dev || num_queries == 0), "gwn_points_grad: bad queries");
+        if (num_queries == 0) return DWG_OK;
+        GwnQuery q;
+        q.q = queries_dev;
+        q.nq = num_queries;
+        return gwn_thread_common(tree, normals_dev, areas_dev, radii_dev, q, params, false, out_dev, grad_dev, stream);
+    })
+}
+
+int dwg_gwn_points_fp64(dwg_octree* tree, const float* normals_dev, const float* areas_dev, const float* radii_dev,
+                        const float* queries_dev, long long num_queries, const dwg_gwn_params* params,
+                        double* out_dev, double* grad_dev, void* stream) {
+    API_GUARD({
+        DWG_REQUIRE(num_queries >= 0 && (queries_dev || num_queries == 0), "gwn_points_fp64: bad queries");
+        if (num_queries == 0) return DWG_OK;
+        GwnQuery q;
+        q.q = queries_dev;
+        q.nq = num_queries;
+        return gwn_thread_common(tree, normals_dev, areas_dev, radii_dev, q, params, true, out_dev, grad_dev, stream);
+    })
+}
+
+static int grid_query(const int res[3], const float origin[3], float spacing, GwnQuery& q) {
+    DWG_REQUIRE(res && origin, "gwn_grid: null grid");
+    for (int d = 0; d < 3; ++d) {
+        q.res[d] = res[d];
+        q.origin[d] = origin[d];
+    }
+    q.spacing = spacing;
+    return DWG_OK;
+}
+
+int dwg_gwn_grid_grad(dwg_octree* tree, const float* normals_dev, const float* areas_dev, const float* radii_dev,
+                      const int res[3], const float origin[3], float spacing, const dwg_gwn_params* params,
+                      float* out_dev, float* grad_dev, void* stream) {
+    API_GUARD({
+        GwnQuery q;
+        DWG_TRY(grid_query(res, origin, spacing, q));
+        return gwn_thread_common(tree, normals_dev, areas_dev, radii_dev, q, params, false, out_dev, grad_dev, stream);
+    })
+}
+
+int dwg_gwn_grid_fp64(dwg_octree* tree, const float* normals_dev, const float* areas_dev, const float* radii_dev,
+                      const int res[3], const float origin[3], float spacing, const dwg_gwn_params* params,
+                      double* out_dev, double* grad_dev, void* stream) {
+    API_GUARD({
+        GwnQuery q;
+        DWG_TRY(grid_query(res, origin, spacing, q));
+        return gwn_thread_common(tree, normals_dev, areas_dev, radii_dev, q, params, true, out_dev, grad_dev, stream);
     })
 }
 
@@ -446,7 +514,7 @@ int dwg_marching_cubes(const float* field_dev, const int res[3], const float* po
 
 int dwg_mc_tables(int* edge_table_host, signed char* tri_table_host) {
     DWG_REQUIRE(edge_table_host && tri_table_host, "mc_tables: null output");
-    mc_tables_host(edge_table_host, tri_table_host);
+    DWG_REQUIRE(mc_tables_host(edge_table_host, tri_table_host), "mc_tables: a case's triangles do not match its polygons");
     return DWG_OK;
 }
 

@@ -8,7 +8,8 @@
 // exactly the reference's per-query decisions -- a child is a dipole term
 // when |CM - q| > beta R, otherwise it is opened, and leaves are summed point
 // by point -- while node and point loads are warp-broadcast.  Terms are
-// FP32; each query's sum is FP32 (precision 0) or FP64 (precision >= 1).
+// FP32; each query's sum is FP32 (precision 0), FP64 (precision 1 and 2) or
+// compensated FP32 (precision 3, Neumaier).
 #include "gwn.cuh"
 
 #include <cub/cub.cuh>
@@ -43,31 +44,31 @@ __device__ __forceinline__ float rcp_ftz(float x) {
 // Screened (src/TurboLibiGWN.cu:530-584): rho = max(|p-q|, s),
 // v = (sigma rho + 1) d / (e^{sigma rho} 4 pi rho^3 + 1e-7) with the sign of d,
 // skipped when |p-q| <= 1e-10.  Plain (:351-360): v = d / (4 pi |p-q|^3 + 1e-8).
-// PREC < 2 uses the MUFU approximations (sigma_l2e = sigma log2 e);
+// PREC != 2 uses the MUFU approximations (sigma_l2e = sigma log2 e);
 // PREC 2 uses correctly rounded sqrt / division and expf.
 template <bool SCREENED, int PREC>
 __device__ __forceinline__ bool gwn_term_r2(float r2, float d, float s, float sigma, float sigma_l2e, float& v) {
     if (SCREENED) {
         if (!(r2 > 1e-20f)) return false;  // |p - q| <= 1e-10
-        const float r = (PREC >= 2) ? sqrtf(r2) : r2 * rsqrt_ftz(r2);
+        const float r = (PREC == 2) ? sqrtf(r2) : r2 * rsqrt_ftz(r2);
         const float rho = fmaxf(r, s);
-        const float e = (PREC >= 2) ? expf(sigma * rho) : ex2_ftz(rho * sigma_l2e);
+        const float e = (PREC == 2) ? expf(sigma * rho) : ex2_ftz(rho * sigma_l2e);
         const float r3 = rho * rho * rho;
         const float den = fmaf(e, kFourPi * r3, 1e-7f);
         // the reference forces the sign of d onto the term
         // (src/TurboLibiGWN.cu:550-584); den > 0, so |sigma rho + 1| d does
         // that (an operand modifier, no extra instruction)
         const float num = fabsf(fmaf(sigma, rho, 1.0f)) * d;
-        v = (PREC >= 2) ? __fdiv_rn(num, den) : num * rcp_ftz(den);
+        v = (PREC == 2) ? __fdiv_rn(num, den) : num * rcp_ftz(den);
         return true;
     } else {
         if (r2 == 0.0f) {
             v = 0.0f;
             return true;
         }
-        const float r = (PREC >= 2) ? sqrtf(r2) : r2 * rsqrt_ftz(r2);
+        const float r = (PREC == 2) ? sqrtf(r2) : r2 * rsqrt_ftz(r2);
         const float den = fmaf(kFourPi * r, r2, 1e-8f);
-        v = (PREC >= 2) ? __fdiv_rn(d, den) : d * rcp_ftz(den);
+        v = (PREC == 2) ? __fdiv_rn(d, den) : d * rcp_ftz(den);
         return true;
     }
 }
@@ -78,8 +79,34 @@ __device__ __forceinline__ bool gwn_term(float dx, float dy, float dz, float d, 
     return gwn_term_r2<SCREENED, PREC>(fmaf(dx, dx, fmaf(dy, dy, dz * dz)), d, s, sigma, sigma_l2e, v);
 }
 
-// per-query accumulator: FP32 (PREC 0) or FP64 (PREC >= 1: each FP32 term
-// converted exactly and added in double, one conversion and one add per term)
+// A sum of FP32 terms kept in FP32 with Neumaier's compensation (the
+// improved Kahan-Babuska summation, Neumaier 1974): s is the rounded running
+// sum and c collects the rounding error of every addition, taken exactly
+// from the larger and the smaller operand; the sum is s + c, rounded once.
+// Its error is about that of summing in twice the precision, independent of
+// the number of terms up to ~1/eps of them.
+struct CompSum {
+    float s, c;
+    CompSum() = default;
+    __device__ CompSum(float v) : s(v), c(0.f) {}
+    __device__ __forceinline__ void add(float v) {
+        const float t = __fadd_rn(s, v);
+        const bool sbig = fabsf(s) >= fabsf(v);
+        const float big = sbig ? s : v, small = sbig ? v : s;
+        c = __fadd_rn(c, __fadd_rn(__fsub_rn(big, t), small));
+        s = t;
+    }
+    __device__ __forceinline__ CompSum& operator+=(const CompSum& o) {
+        add(o.s);
+        c = __fadd_rn(c, o.c);
+        return *this;
+    }
+    __device__ __forceinline__ explicit operator float() const { return __fadd_rn(s, c); }
+};
+
+// per-query accumulator: FP32 (PREC 0); FP64 (PREC 1 and 2: each FP32 term
+// converted exactly and added in double, one conversion and one add per
+// term); compensated FP32 (PREC 3)
 template <int PREC>
 struct AccType {
     using T = double;
@@ -87,6 +114,10 @@ struct AccType {
 template <>
 struct AccType<0> {
     using T = float;
+};
+template <>
+struct AccType<3> {
+    using T = CompSum;
 };
 
 // brick shapes of 32 grid samples (x, y, z extents) a warp evaluates together
@@ -173,7 +204,7 @@ __device__ __forceinline__ float gwn_term_masked(bool take, float r2, float d, f
                                                  float sigma_l2e, bool& counted) {
     float v = 0.f;
     counted = false;
-    if (SCREENED && PREC < 2) {
+    if (SCREENED && PREC != 2) {
         v = __fmul_rn(screen_weight_masked(take, r2, s, sigma, sigma_l2e, counted), d);
     } else if (SCREENED) {
         const bool ok = take && r2 > 1e-20f;  // |p - q| <= 1e-10 is skipped
@@ -189,9 +220,9 @@ __device__ __forceinline__ float gwn_term_masked(bool take, float r2, float d, f
     } else {
         const bool zero = r2 == 0.0f;  // a zero distance is a term of value 0
         const float r2s = (take && !zero) ? r2 : 1.0f;
-        const float r = (PREC >= 2) ? sqrtf(r2s) : r2s * rsqrt_ftz(r2s);
+        const float r = (PREC == 2) ? sqrtf(r2s) : r2s * rsqrt_ftz(r2s);
         const float den = fmaf(kFourPi * r, r2s, 1e-8f);
-        const float t = (PREC >= 2) ? __fdiv_rn(d, den) : d * rcp_ftz(den);
+        const float t = (PREC == 2) ? __fdiv_rn(d, den) : d * rcp_ftz(den);
         v = (take && !zero) ? t : 0.f;
         counted = take;
     }
@@ -210,11 +241,11 @@ __device__ __forceinline__ float gwn_term_masked(bool take, float r2, float d, f
 // order-0 dipole is the usual term.
 template <int ORDER, int PREC>
 __device__ __forceinline__ float fwn_correction(float lx, float ly, float lz, float r2, const float4* __restrict__ H) {
-    const float r = (PREC >= 2) ? sqrtf(r2) : r2 * rsqrt_ftz(r2);
+    const float r = (PREC == 2) ? sqrtf(r2) : r2 * rsqrt_ftz(r2);
     const float p3 = kFourPi * r * r * r;
     const float p5 = p3 * r * r;
-    const float d = (PREC >= 2) ? __fdiv_rn(1.0f, p3) : rcp_ftz(p3);
-    const float c5 = (PREC >= 2) ? __fdiv_rn(-3.0f, p5) : -3.0f * rcp_ftz(p5);
+    const float d = (PREC == 2) ? __fdiv_rn(1.0f, p3) : rcp_ftz(p3);
+    const float c5 = (PREC == 2) ? __fdiv_rn(-3.0f, p5) : -3.0f * rcp_ftz(p5);
     float h[32];
 #pragma unroll
     for (int t = 0; t < (ORDER >= 2 ? 8 : 3); ++t) {
@@ -232,7 +263,7 @@ __device__ __forceinline__ float fwn_correction(float lx, float ly, float lz, fl
     float w = fmaf(d, h[9], c5 * q1);
     if (ORDER >= 2) {
         const float p7 = p5 * r * r;
-        const float i15 = (PREC >= 2) ? __fdiv_rn(15.0f, p7) : 15.0f * rcp_ftz(p7);
+        const float i15 = (PREC == 2) ? __fdiv_rn(15.0f, p7) : 15.0f * rcp_ftz(p7);
         const float l00 = lx * lx, l01 = lx * ly, l02 = lx * lz, l11 = ly * ly, l12 = ly * lz, l22 = lz * lz;
         float cub = 0.f;
         const float lv[3] = {lx, ly, lz};
@@ -355,7 +386,7 @@ __device__ __forceinline__ float node_dot(const float4& nb, float dx, float dy, 
 
 // one far-node term, masked to the lanes that take it (shared by the
 // traversal and the replay of its interaction list, so both give the same bits)
-// (returns the screening weight g of the term for PREC < 2, 0 otherwise)
+// (returns the screening weight g of the term for PREC != 2, 0 otherwise)
 template <bool SCREENED, int PREC, typename Acc>
 __device__ __forceinline__ float node_term(const GwnArgs& a, const float4& na, const float4& nb, float dx, float dy,
                                            float dz, float d2, bool take, float sigma, float sigma_l2e, Acc& sum,
@@ -364,7 +395,7 @@ __device__ __forceinline__ float node_term(const GwnArgs& a, const float4& na, c
     const float dd = node_dot(nb, dx, dy, dz);
     bool k;
     float v, g = 0.f;
-    if (SCREENED && PREC < 2) {
+    if (SCREENED && PREC != 2) {
         g = screen_weight_masked(take, d2, a.screen, sigma, sigma_l2e, k);
         v = __fmul_rn(g, dd);  // never contracted into the sum: a kept g gives the same bits
     } else {
@@ -616,7 +647,7 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_replay(GwnArgs a) {
     const float sigma_l2e = sigma * 1.4426950408889634f;
     int wmode = 0;
     W* wp = nullptr;
-    if (SCREENED && PREC < 2 && a.wsel) {
+    if (SCREENED && PREC != 2 && a.wsel) {
         wmode = a.wsel->mode;
         if (wmode == 2) return;  // k_gwn_wread reads the kept weights
         wp = reinterpret_cast<W*>(a.wbuf) + (size_t)a.wsel->slot * a.wstride;
@@ -927,6 +958,13 @@ __global__ void k_weight_reset(GwnWeightState* __restrict__ w, int nslots) {
     }
 }
 
+int gwn_list_drop_weights(GwnList& L, cudaStream_t s) {
+    if (!L.valid || L.nslots <= 0) return DWG_OK;
+    k_weight_reset<<<1, 1, 0, s>>>(L.wstate.ptr, L.nslots);
+    DWG_CHECK_LAUNCH();
+    return DWG_OK;
+}
+
 // Grid sums of many clouds in one persistent launch: the groups of all
 // clouds form one work list (prefix[c] = first group of cloud c), taken in
 // order by the warps of the grid, so that small clouds do not idle the GPU.
@@ -1001,14 +1039,16 @@ static int launch_plain(const GwnArgs& a, const dwg_gwn_params& p, cudaStream_t 
 
 template <bool GRID>
 static int dispatch(const GwnArgs& a, const dwg_gwn_params& p, cudaStream_t s) {
-    const int prec = p.precision < 0 ? 0 : (p.precision > 2 ? 2 : p.precision);
+    const int prec = p.precision < 0 ? 0 : (p.precision > 3 ? 3 : p.precision);
     if (p.screened) {
         if (prec == 0) return launch_shape<GRID, true, 0, 0>(a, p.tile, s);
         if (prec == 1) return launch_shape<GRID, true, 1, 0>(a, p.tile, s);
+        if (prec == 3) return launch_shape<GRID, true, 3, 0>(a, p.tile, s);
         return launch_shape<GRID, true, 2, 0>(a, p.tile, s);
     }
     if (prec == 0) return launch_plain<GRID, 0>(a, p, s);
     if (prec == 1) return launch_plain<GRID, 1>(a, p, s);
+    if (prec == 3) return launch_plain<GRID, 3>(a, p, s);
     return launch_plain<GRID, 2>(a, p, s);
 }
 
@@ -1155,7 +1195,7 @@ static int listed_shape(GwnArgs& a, GwnList& L, const Octree& t, cudaStream_t s,
         // weight slots: 8 bytes per entry and lane each, together at most a
         // third of the free memory and 64 GB
         L.nslots = 0;
-        if (SCREENED && PREC < 2 && L.wslots > 0 && total > 0) {
+        if (SCREENED && PREC != 2 && L.wslots > 0 && total > 0) {
             const size_t fr = device_free_bytes();
             const unsigned long long per = total * 32ull * sizeof(W);
             const unsigned long long cap = std::min<unsigned long long>(fr / 3, 64ull << 30);
@@ -1217,10 +1257,11 @@ static int listed_prec(GwnArgs& a, GwnList& L, const Octree& t, int tile, cudaSt
 template <bool GRID>
 static int listed_dispatch(GwnArgs& a, GwnList& L, const Octree& t, const dwg_gwn_params& p, cudaStream_t s,
                            size_t max_bytes) {
-    const int prec = p.precision < 0 ? 0 : (p.precision > 2 ? 2 : p.precision);
+    const int prec = p.precision < 0 ? 0 : (p.precision > 3 ? 3 : p.precision);
     bool fallback = false;
     if (prec == 0) DWG_TRY(listed_prec<GRID, 0>(a, L, t, p.tile, s, max_bytes, &fallback));
     else if (prec == 1) DWG_TRY(listed_prec<GRID, 1>(a, L, t, p.tile, s, max_bytes, &fallback));
+    else if (prec == 3) DWG_TRY(listed_prec<GRID, 3>(a, L, t, p.tile, s, max_bytes, &fallback));
     else DWG_TRY(listed_prec<GRID, 2>(a, L, t, p.tile, s, max_bytes, &fallback));
     if (fallback) {
         DWG_CHECK_CUDA(cudaMemsetAsync(t.work.ptr, 0, sizeof(unsigned int), s));
@@ -1373,9 +1414,10 @@ int gwn_batch_launch(GwnBatch& b, cudaStream_t s) {
     DWG_REQUIRE(b.impl && b.impl->n > 0, "gwn batch: not prepared");
     GwnBatchImpl& B = *b.impl;
     DWG_CHECK_CUDA(cudaMemsetAsync(B.work.ptr, 0, sizeof(unsigned long long), s));
-    const int prec = B.p.precision < 0 ? 0 : (B.p.precision > 2 ? 2 : B.p.precision);
+    const int prec = B.p.precision < 0 ? 0 : (B.p.precision > 3 ? 3 : B.p.precision);
     if (prec == 0) return launch_batch_shape<0>(B, b.groups, s);
     if (prec == 1) return launch_batch_shape<1>(B, b.groups, s);
+    if (prec == 3) return launch_batch_shape<3>(B, b.groups, s);
     return launch_batch_shape<2>(B, b.groups, s);
 }
 

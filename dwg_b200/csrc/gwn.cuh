@@ -89,6 +89,18 @@ int gwn_eval_listed(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p,
                     unsigned long long* terms_total, cudaStream_t s, const float* sigma_dev, size_t max_bytes,
                     int wslots = 0);
 
+// Values and/or gradients (out_g: 3 per query) of the sums, one thread per
+// query with the decisions of gwn_eval; fp64: terms and sums in double from
+// the FP64 moments (outputs double), else FP32 terms summed in double
+// (outputs float).  Order-0 far field only.
+int gwn_eval_thread(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p, bool fp64, void* out_w,
+                    void* out_g, cudaStream_t s);
+
+// Frees every weight slot of L (the list itself stays): the kept weights
+// depend on the points' screening radii when use_radii is set, so new radii
+// make them stale.  Stream-ordered, no host synchronisation.
+int gwn_list_drop_weights(GwnList& L, cudaStream_t s);
+
 // Grid sums of many clouds in one persistent launch (screened).  prepare()
 // records the clouds' octrees, grids and outputs once (host work, not
 // capturable); launch() is two stream operations and can be captured in a

@@ -114,20 +114,53 @@ class TurboLibiGWN:
         return self._launch(query_points, i_Normals, i_As, i_radii if use_radii else None, p, out_gwn)
 
     def grid(self, res, origin, spacing, i_Normals=None, i_As=None, beta=2.3, sigma=10.0, screened=True,
-             precision=1, out=None, terms=None, screen=0.0015, tile=0, order=0, lists=0):
+             precision=1, out=None, terms=None, screen=0.0015, tile=0, order=0, lists=0, i_radii=None):
         """GWN at the closed-form grid origin + index * spacing (x fastest);
-        ``tile`` picks the brick of samples a warp evaluates together."""
+        ``tile`` picks the brick of samples a warp evaluates together;
+        ``i_radii`` (per point) switches the screening radius to the points'
+        radii (use_radii)."""
         res = np.ascontiguousarray(res, np.int32)
         org = np.ascontiguousarray(origin, np.float32)
         n = int(np.prod(res.astype(np.int64)))
         if out is None:
             out = torch.empty(n, dtype=torch.float32, device="cuda")
         p = capi.gwn_params(beta=beta, sigma=sigma, screen=screen, screened=screened, precision=precision,
-                            tile=tile, order=order, lists=lists)
-        capi.check(capi.load().dwg_gwn_grid(self._h, capi.ptr(i_Normals), capi.ptr(i_As), None, res.ctypes.data,
+                            tile=tile, order=order, lists=lists, use_radii=i_radii is not None)
+        capi.check(capi.load().dwg_gwn_grid(self._h, capi.ptr(i_Normals), capi.ptr(i_As), capi.ptr(i_radii),
+                                            res.ctypes.data,
                                             org.ctypes.data, float(spacing), C.byref(p), capi.ptr(out),
                                             capi.ptr(terms), capi.stream_ptr()))
         return out
+
+    def value_and_gradient(self, query_points=None, i_Normals=None, i_As=None, i_radii=None, beta=2.3, sigma=10.0,
+                           screened=True, screen=0.0015, fp64=False, grid=None):
+        """Sums and their gradients with respect to the query at points
+        (``query_points``, (n, 3) float32 on the GPU) or at a grid
+        (``grid`` = (res, origin, spacing)): (w, grad) tensors, float32 (FP32
+        terms summed in FP64) or float64 (``fp64``: terms and sums in double).
+        The reference has no gradient; see dwg_gwn_points_grad."""
+        p = capi.gwn_params(beta=beta, sigma=sigma, screen=screen, screened=screened,
+                            use_radii=i_radii is not None)
+        dt = torch.float64 if fp64 else torch.float32
+        L = capi.load()
+        if grid is None:
+            _req_cuda_f32(query_points, "query_points", 3)
+            nq = query_points.shape[0]
+        else:
+            res = np.ascontiguousarray(grid[0], np.int32)
+            org = np.ascontiguousarray(grid[1], np.float32)
+            nq = int(np.prod(res.astype(np.int64)))
+        w = torch.empty(nq, dtype=dt, device="cuda")
+        g = torch.empty((nq, 3), dtype=dt, device="cuda")
+        args = (self._h, capi.ptr(i_Normals), capi.ptr(i_As), capi.ptr(i_radii))
+        if grid is None:
+            fn = L.dwg_gwn_points_fp64 if fp64 else L.dwg_gwn_points_grad
+            capi.check(fn(*args, capi.ptr(query_points), nq, C.byref(p), capi.ptr(w), capi.ptr(g), capi.stream_ptr()))
+        else:
+            fn = L.dwg_gwn_grid_fp64 if fp64 else L.dwg_gwn_grid_grad
+            capi.check(fn(*args, res.ctypes.data, org.ctypes.data, float(grid[2]), C.byref(p), capi.ptr(w),
+                          capi.ptr(g), capi.stream_ptr()))
+        return w, g
 
     def list_size(self):
         """(entries, weight slots) of the kept interaction list of grid()."""

@@ -104,7 +104,11 @@ typedef struct {
     int use_radii;   /* 1: s = radii[i] for point terms (far field keeps `screen`) */
     int precision;   /* terms in FP32; 0 FP32 accumulation, 1 FP64 accumulation
                         (default), 2 FP64 accumulation with correctly rounded
-                        sqrt / exp / division in the terms */
+                        sqrt / exp / division in the terms, 3 FP32
+                        accumulation compensated per query (Neumaier: every
+                        addition's rounding error kept in a second FP32
+                        word); 0, 1 and 3 use the MUFU approximations of
+                        rsqrt / exp2 / rcp in the terms */
     int tile;        /* grid samples per warp: 0 4x4x2 (default), 1 8x4x1,
                         2 2x4x4, 3 8x2x2 (point queries ignore it) */
     int order;       /* far-field expansion order of the plain sum: 0 (the DWG
@@ -118,8 +122,8 @@ typedef struct {
                         with the same grid, beta and tile until the centres
                         change (dwg_octree_update_info): bit-identical values,
                         no traversal; 2 also keeps the terms' screening
-                        weights for two (sigma, screen) values (precision 0
-                        and 1): later calls with one of them read the weights
+                        weights for two (sigma, screen) values (precision 0,
+                        1 and 3): later calls with one of them read the weights
                         instead of evaluating them, same bits (the calls of
                         one octree must then follow each other on one
                         stream); 0 traverses every call */
@@ -154,6 +158,32 @@ int dwg_gwn_grid(dwg_octree* tree, const float* normals_dev, const float* areas_
                  const dwg_gwn_params* params, float* out_dev, unsigned long long* terms_dev,
                  void* stream);
 
+/* Values and gradients of the same sums.  The reference has no gradient
+ * (its sums are ScreenedGWNLibiPStoQ / GWNLibiPStoQ, src/TurboLibiGWN.cu:
+ * 328-812); grad_dev (3 floats per query, nullable) receives the analytic
+ * derivative of each term with respect to the query -- of the point terms
+ * and of the far nodes' order-0 dipoles, with the opening decisions of
+ * dwg_gwn_points -- and out_dev (nullable) the values.  FP32 terms summed in
+ * FP64, one thread per query (slower than dwg_gwn_points, which the DWG loop
+ * uses); params->order must be 0; lists, tile and precision are ignored. */
+int dwg_gwn_points_grad(dwg_octree* tree, const float* normals_dev, const float* areas_dev,
+                        const float* radii_dev, const float* queries_dev, long long num_queries,
+                        const dwg_gwn_params* params, float* out_dev, float* grad_dev, void* stream);
+int dwg_gwn_grid_grad(dwg_octree* tree, const float* normals_dev, const float* areas_dev,
+                      const float* radii_dev, const int res[3], const float origin[3], float spacing,
+                      const dwg_gwn_params* params, float* out_dev, float* grad_dev, void* stream);
+
+/* The same sums (and, with grad_dev, gradients) in FP64: terms and sums in
+ * double from the tree's FP64 moments, with the opening decisions of the
+ * FP32 kernels -- the yardstick for checking FP32 fields on the GPU (as the
+ * FP64 CPU restatement does on the host).  No counterpart in the reference. */
+int dwg_gwn_points_fp64(dwg_octree* tree, const float* normals_dev, const float* areas_dev,
+                        const float* radii_dev, const float* queries_dev, long long num_queries,
+                        const dwg_gwn_params* params, double* out_dev, double* grad_dev, void* stream);
+int dwg_gwn_grid_fp64(dwg_octree* tree, const float* normals_dev, const float* areas_dev,
+                      const float* radii_dev, const int res[3], const float origin[3], float spacing,
+                      const dwg_gwn_params* params, double* out_dev, double* grad_dev, void* stream);
+
 /* Closed-form igl::voxel_grid(V, offset, s, 1) (deps/libigl/include/igl/voxel_grid.cpp:11-87):
  * resolution, origin and spacing of the padded grid around points_dev.
  * Synchronises `stream` (the bounding box is read back). */
@@ -179,19 +209,25 @@ int dwg_marching_cubes(const float* field_dev, const int res[3], const float* po
 int dwg_mc_tables(int* edge_table_host, signed char* tri_table_host);
 
 /* Marching cubes that allocates no device memory.  No counterpart in the
- * reference: it is for callers that cannot allocate while they mesh -- a host
- * recording a CUDA graph in global capture mode (cudaMalloc is not allowed
- * during such a capture), a real-time loop that must not allocate after
- * start-up, or an application whose device memory all comes from its own pool.
- * Same arguments, kernels and output as dwg_marching_cubes (the count is
- * returned in *num_tris_host, required; the call synchronises `stream`).
+ * reference.  It is for callers that cannot call cudaMalloc while they mesh:
+ * a real-time loop that must not allocate after start-up (cudaMalloc and
+ * cudaFree can wait for the whole device and take unbounded time), and an
+ * application whose device memory is a fixed budget handed out by its own
+ * pool, where a library allocation could fail or take memory the pool
+ * counts on.  Same arguments, kernels and output as dwg_marching_cubes; the
+ * count is returned in *num_tris_host (required), and the call synchronises
+ * `stream` to read it.  With T > capacity it writes the first `capacity`
+ * triangles, sets *num_tris_host = T and returns DWG_ERR_OVERFLOW.
  * Its scratch is a static device array of the library (about 4 MB, held by
  * every GPU that loads the library until the process exits), which limits the
  * grid to 134,217,728 cells (e.g. 512^3); larger grids are rejected with
  * DWG_ERR_INVALID before any GPU work.  The first call on a device looks up
- * the array's device address (cudaGetSymbolAddress); make that first call
- * before any stream capture.  All calls share the array, so calls that
- * overlap on the GPU (different streams or threads at once) race. */
+ * the array's device address (cudaGetSymbolAddress) and uploads the case
+ * tables; make that first call before any stream capture.  Every call reuses
+ * the array (the scan rewrites each slot it reads), so calls that overlap on
+ * the GPU (different streams or threads at once) race.  The looked-up
+ * address and the tables are cached per device ordinal and do not survive a
+ * cudaDeviceReset. */
 int dwg_marching_cubes_noalloc(const float* field_dev, const int res[3], const float* positions_dev,
                                const float origin[3], float spacing, float iso, float* tris_dev,
                                float* centroids_dev, float* normals_dev, long long capacity,

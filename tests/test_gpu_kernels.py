@@ -84,7 +84,7 @@ def _oracle_gwn_with_gpu_moments(ot, g, idx, P, N, A, Q, **kw):
 
 
 @pytest.mark.parametrize("screened,sigma", [(True, 20.0), (True, 10.0), (False, 0.0)])
-@pytest.mark.parametrize("precision", [0, 1, 2])
+@pytest.mark.parametrize("precision", [0, 1, 2, 3])
 def test_gwn_points_same_sums_as_oracle(torus_tree, screened, sigma, precision, dwg_lib):
     import ctypes as C
     P, N, A, gt, ot = torus_tree
@@ -432,3 +432,48 @@ def test_gwn_grid_lists_bit_identical(tile):
                 assert t0 > 0
                 assert np.array_equal(w0, w), (tuple(res), lists, step)
                 assert t == t0, (tuple(res), lists, step)
+
+
+def test_gwn_grid_kept_weights_follow_new_radii():
+    # With use_radii the screening weights depend on the points' radii:
+    # dwg_gwn_grid drops the kept weights whenever radii are passed, so a call
+    # with new radii and the same sigma sums with the new radii (lists 2 equal
+    # to the traversal, bit for bit)
+    P, N = cloud(20000, seed=9)
+    A = np.full(len(P), 2e-6, np.float32)
+    rng = np.random.default_rng(12)
+    R1 = rng.uniform(0.001, 0.004, len(P)).astype(np.float32)
+    R2 = (R1 * 1.7).astype(np.float32)
+    res, org, h = np.array([40, 36, 30], np.int32), np.array([-0.55, -0.5, -0.2], np.float32), 0.03
+    runs = {}
+    for lists in (0, 2):
+        gt = turbo.TurboLibiGWN(cu(P), max_depth=8, areas=cu(A))
+        gt.UpdateMassNormals(cu(N), cu(A))
+        runs[lists] = [gt.grid(res, org, h, sigma=20.0, lists=lists, i_radii=cu(R)).cpu().numpy()
+                       for R in (R1, R1, R2, R2)]
+        assert gt.status() == 0
+    assert not np.array_equal(runs[0][0], runs[0][2])  # the radii matter
+    for step, (w0, w2) in enumerate(zip(runs[0], runs[2])):
+        assert np.array_equal(w0, w2), step
+
+
+def test_compensated_fp32_sums_are_as_close_to_fp64_as_fp64_sums(torus_tree):
+    # precision 3 keeps each query's sum in FP32 with Neumaier compensation:
+    # its error against the FP64 oracle (same terms) is that of precision 1
+    # (FP32 terms summed in FP64), below that of plain FP32 sums
+    P, N, A, gt, ot = torus_tree
+    g = gt.export()
+    idx = match_nodes(g, ot)
+    rng = np.random.default_rng(17)
+    Q = np.concatenate([P[rng.choice(len(P), 4000, replace=False)],
+                        rng.uniform(-0.6, 0.6, (4000, 3)).astype(np.float32)])
+    w_ref, _ = _oracle_gwn_with_gpu_moments(ot, g, idx, P, N, A, Q, beta=2.3, sigma=20.0, screened=True)
+    err = {}
+    for prec in (0, 1, 3):
+        w = gt.TurboLibiScreenedGWNLaunch(cu(Q), None, len(Q), None, None, None, 2.3, 20.0,
+                                          precision=prec).cpu().numpy().astype(np.float64)
+        err[prec] = float(np.sqrt(np.mean((w - w_ref) ** 2)))
+    print("RMS error vs FP64 (same terms): fp32 sum %.3g, fp64 sum %.3g, compensated fp32 sum %.3g"
+          % (err[0], err[1], err[3]))
+    assert err[3] <= 1.1 * err[1] + 1e-12, err
+    assert err[3] <= 1.02 * err[0], err
