@@ -162,6 +162,18 @@ class TurboLibiGWN:
                           capi.ptr(g), capi.stream_ptr()))
         return w, g
 
+    def values_fp64(self, query_points, i_Normals=None, i_As=None, i_radii=None, beta=2.3, sigma=10.0,
+                    screened=True, screen=0.0015):
+        """FP64 sums (terms and sums in double, the FP32 kernels' decisions)
+        at points: a float64 tensor (dwg_gwn_points_fp64)."""
+        _req_cuda_f32(query_points, "query_points", 3)
+        p = capi.gwn_params(beta=beta, sigma=sigma, screen=screen, screened=screened, use_radii=i_radii is not None)
+        w = torch.empty(query_points.shape[0], dtype=torch.float64, device=query_points.device)
+        capi.check(capi.load().dwg_gwn_points_fp64(self._h, capi.ptr(i_Normals), capi.ptr(i_As), capi.ptr(i_radii),
+                                                   capi.ptr(query_points), query_points.shape[0], C.byref(p),
+                                                   capi.ptr(w), None, capi.stream_ptr()))
+        return w
+
     def list_size(self):
         """(entries, weight slots) of the kept interaction list of grid()."""
         e = C.c_longlong()

@@ -209,8 +209,13 @@ def reconstruct(P, workdir=None, **kw):
     L = len(Lk)
     An = np.full(L, prm["area"], np.float32)
     t2 = IglTree(Lk, prm["max_depth"], A=An)
+    # GetRadiiandAs (include/DWGProcess.h:283-381): the radii only enter the
+    # sums with use_radii (the oracle's kNN is brute force, so skip it otherwise)
     kw_ = min(prm["kw"], L)
-    radii = O.radii(Lk, O.knn(Lk, Lk, kw_)) if kw_ > 0 else np.zeros(L, np.float32)
+    if prm["use_radii"] and kw_ > 0:
+        radii = O.radii(Lk, O.knn(Lk, Lk, kw_))
+    else:
+        radii = np.full(L, prm["screen"], np.float32)
     res1, org1, h1 = O.voxel_grid(Pk, prm["offset_1"], prm["grid_reso"])
     G1 = O.grid_points(res1, org1, h1)
     res2, org2, h2 = O.voxel_grid(Pk, prm["offset_2"], prm["final_reso"])
