@@ -430,7 +430,7 @@ __device__ __forceinline__ void knn_pyramid(const KnnArgs& a, float qx, float qy
 // (replace-the-maximum on insertion, one sort at the end).  The search stops
 // when the k-th key is closer than the boundary of the visited block.
 template <int KMAX>
-__global__ void __launch_bounds__(128) k_knn_thread(KnnArgs a) {
+__global__ void __launch_bounds__(128, KMAX <= 10 ? 4 : 1) k_knn_thread(KnnArgs a) {
     if (a.gate_count && *a.gate_count <= a.gate_min) return;
     const long long nq = knn_count(a);
     const unsigned long long NONE = ~0ull;
@@ -1102,9 +1102,12 @@ static int knn_query_cells(const KnnIndex& ix, const KnnArgs& a0, long long nq, 
     }
     k_cq_scatter<<<(unsigned)blocks, 256, 0, s>>>(a, ix.q_key.ptr, ix.c_fill.ptr, ix.q_order.ptr);
     DWG_CHECK_LAUNCH();
-    // k = 15 (the triangle and zero-repair queries) keeps 15 slots per lane
-    // instead of 16: every maximum search and the final sort are shorter
-    return a.k == 15 ? cells_launch<15>(ix, a, nq, s) : cells_launch<16>(ix, a, nq, s);
+    // k = 15 (the triangle queries) keeps 15 slots per lane instead of 16 and
+    // k <= 10 (the zero repair) 10: every maximum search and the final sort
+    // are shorter, and the lanes hold fewer registers
+    if (a.k == 15) return cells_launch<15>(ix, a, nq, s);
+    if (a.k <= 10) return cells_launch<10>(ix, a, nq, s);
+    return cells_launch<16>(ix, a, nq, s);
 }
 
 // ------------------------------------------------------------- subsets --
@@ -1233,6 +1236,7 @@ int knn_query(const KnnIndex& ix, const KnnQuery& q, int k, int* out, cudaStream
     k_knn_qscatter<<<(unsigned)blocks, 256, 0, s>>>(a, ix.q_fill.ptr, ix.q_order.ptr);
     DWG_CHECK_LAUNCH();
     a.order = ix.q_order.ptr;
+    if (k <= 10) return knn_launch<10>(a, q.nq, s);
     if (k <= 16) return knn_launch<16>(a, q.nq, s);
     if (k <= 32) return knn_launch<32>(a, q.nq, s);
     return knn_launch<64>(a, q.nq, s);

@@ -1,14 +1,20 @@
-"""Small, self-contained workloads for profiler captures of the hot kernels,
-and a summariser of a profiler launch list.
+"""The profiling recipe of this repository: small, self-contained workloads
+for profiler captures of the hot kernels, and a summariser of a profiler
+launch list (the ncu summaries under profiles/ name the command that made
+them).
 
-    python -m dwg_b200.profile_cases step     [--points N --grid R --iters T --reps K --shape torus|sq_union]
-    python -m dwg_b200.profile_cases gwn_grid [--points N --grid R --launches K --lists [1|2]]
-    python -m dwg_b200.profile_cases knn_tri  [--points N --grid R --launches K]
-    python -m dwg_b200.profile_cases mc       [--points N --grid R --launches K]
-    python -m dwg_b200.profile_cases summarize launches.csv
+    python profile_cases.py step     [--points N --grid R --iters T --reps K --shape torus|sq_union
+                                      --grid-lists 0|1|2]
+    python profile_cases.py gwn_grid [--points N --grid R --launches K --lists [1|2]]
+    python profile_cases.py knn_tri  [--points N --grid R --launches K --shape torus|sq_union]
+    python profile_cases.py mc       [--points N --grid R --launches K]
+    python profile_cases.py summarize launches.csv
 
 ``step`` runs whole reconstructions (create, iterate, finalize) of the seeded
-non-uniform torus and prints per-phase host timings.  The single-kernel cases
+non-uniform torus (or the superquadric union) and prints per-phase host
+timings; ``--grid-lists 0`` turns off the kept interaction lists and
+screening weights (the same results bit for bit, a small fraction of the
+device memory, for captures that save and restore it).  The single-kernel cases
 first run one plain DWG iteration to obtain a realistic state (leaf normals,
 iteration-0 field and triangles), then launch only the named kernel
 ``--launches`` times, so that a capture filtered by kernel name and launch
@@ -30,14 +36,17 @@ import re
 import sys
 import time
 
+import os
+
 import numpy as np
 
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 
 _SHAPE = "torus"
 
 
 def _cloud(n, seed=1000):
-    from . import datasets as D
+    from dwg_b200 import datasets as D
     if _SHAPE == "sq_union":  # 12 superquadrics + 1 % outliers
         P, _ = D.superquadric_union(int(round(n / 1.01)), seed=seed)
     else:
@@ -48,11 +57,11 @@ def _cloud(n, seed=1000):
 
 def case_step(a):
     import torch
-    from . import capi
+    from dwg_b200 import capi
     lib = capi.load()
     P = _cloud(a.points)
     Pd = torch.from_numpy(P).cuda()
-    prm = capi.default_params(grid_reso=a.grid, final_reso=a.grid, total_iter=a.iters)
+    prm = capi.default_params(grid_reso=a.grid, final_reso=a.grid, total_iter=a.iters, grid_lists=a.grid_lists)
     n = len(P)
     for rep in range(a.reps):
         h = C.c_void_p()
@@ -78,7 +87,7 @@ def case_step(a):
 def _iteration0_state(a):
     """Leaves, leaf normals, grid and the iteration-0 field / triangles."""
     import torch
-    from . import turbo
+    from dwg_b200 import turbo
     Pd = torch.from_numpy(_cloud(a.points)).cuda()
     d = turbo.TurboDWG(Pd, None, grid_reso=a.grid, final_reso=a.grid, total_iter=1, use_graph=0)
     st = {"leaf_pos": d.get("leaf_pos"), "leaf_nrm": d.get("leaf_nrm"), "res": d.get("grid_res"),
@@ -93,7 +102,7 @@ def _iteration0_state(a):
 
 def case_gwn_grid(a):
     import torch
-    from . import turbo
+    from dwg_b200 import turbo
     st = _iteration0_state(a)
     L = len(st["leaf_pos"])
     lp = torch.from_numpy(st["leaf_pos"]).cuda()
@@ -118,7 +127,7 @@ def _mc_buffers(res):
 
 def case_mc(a):
     import torch
-    from . import turbo
+    from dwg_b200 import turbo
     st = _iteration0_state(a)
     res, org = st["res"], st["org"]
     tris, cent, nrm, cap = _mc_buffers(res)
@@ -134,7 +143,7 @@ def case_mc(a):
 
 def case_knn_tri(a):
     import torch
-    from . import turbo
+    from dwg_b200 import turbo
     st = _iteration0_state(a)
     res, org = st["res"], st["org"]
     tris, cent, nrm, cap = _mc_buffers(res)
@@ -186,6 +195,7 @@ def main(argv=None):
     ap.add_argument("--launches", type=int, default=2)
     ap.add_argument("--shape", choices=["torus", "sq_union"], default="torus")
     ap.add_argument("--lists", type=int, nargs="?", const=1, default=0, choices=[0, 1, 2])
+    ap.add_argument("--grid-lists", type=int, default=2, choices=[0, 1, 2])
     a = ap.parse_args(argv)
     global _SHAPE
     _SHAPE = a.shape

@@ -477,3 +477,19 @@ def test_compensated_fp32_sums_are_as_close_to_fp64_as_fp64_sums(torus_tree):
           % (err[0], err[1], err[3]))
     assert err[3] <= 1.1 * err[1] + 1e-12, err
     assert err[3] <= 1.02 * err[0], err
+
+
+@pytest.mark.parametrize("k", [10, 15])
+def test_knn_cell_grouped_queries_dense_and_sparse(oracle_lib, k):
+    # the pipeline's k (10: zero repair, 10 slots per lane; 15: triangles) on
+    # many queries per cell and on a few per cell: exact either way
+    P, N = cloud(20000, seed=13)
+    rng = np.random.default_rng(21)
+    sel = rng.choice(len(P), 40000)
+    off = rng.uniform(-0.05, 0.05, (40000, 1)).astype(np.float32)
+    Q = np.ascontiguousarray(P[sel] + off * N[sel], np.float32)
+    ix = turbo.KnnIndex(cu(P))
+    dense = ix.query(cu(Q), k).cpu().numpy()
+    sparse = ix.query(cu(Q[:5000]), k).cpu().numpy()
+    assert np.array_equal(dense[:5000], sparse)
+    assert np.array_equal(sparse, oracle_lib.knn(P, Q[:5000], k))
