@@ -727,12 +727,22 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_replay(GwnArgs a) {
 // modes return at once): per node entry one dot product and one product per
 // sample, g (A n).(p - q), with the replay's roundings, so the sums keep
 // their bits.  The kernel is bound by the weights' HBM stream (256 bytes per
-// entry), so each warp streams its group's entries and weights through a
-// ring of kWreadRing chunks of kWreadChunk entries in shared memory with
-// cp.async (16-byte pieces, L2 only), two chunks in flight while it sums the
-// third; four 256-thread blocks per SM (64 registers, 52 KB of ring each).
-// The node terms a slot stands for were counted when it was written.
-constexpr int kWreadChunk = 8;
+// entry for grid cells, 128 for points), so each warp streams its group's
+// entries and weights through a ring of kWreadRing chunks in shared memory,
+// two chunks in flight while it sums the third.  Grid cells (long lists):
+// one lane hands each 16-entry chunk to the bulk-copy (TMA) engine as two
+// 1-D copies (the chunk's weights and its entries are contiguous in global
+// memory) that complete on the ring slot's mbarrier, two 256-thread blocks
+// per SM (104 KB of ring each).  Points (short lists): 8-entry chunks moved
+// by cp.async in 16-byte pieces spread over the lanes, four blocks per SM
+// (52 KB of ring each), which measured faster there.  The node terms a slot
+// stands for were counted when it was written.
+template <bool GRID>
+struct WreadCfg {
+    static constexpr int kChunk = GRID ? 16 : 8;
+    static constexpr bool kBulk = GRID;
+    static constexpr int kBlocks = GRID ? 2 : 4;
+};
 
 // the points of a multi-point leaf for one sample, out of line (rare in the
 // read path; its registers stay off the loop).  The running sum goes in and
@@ -762,55 +772,128 @@ __device__ __noinline__ LeafSum<Acc> leaf_points_ool(const float4* __restrict__ 
     return r;
 }
 constexpr int kWreadRing = 3;
-constexpr int kWreadWarpBytes = kWreadRing * kWreadChunk * (32 * 8 + 16);
-constexpr int kWreadSmem = kGwnWarps * kWreadWarpBytes;
+template <bool GRID>
+constexpr int wread_warp_bytes() {
+    return kWreadRing * WreadCfg<GRID>::kChunk * (32 * 8 + 16);
+}
+template <bool GRID>
+constexpr int wread_smem() {
+    return kGwnWarps * wread_warp_bytes<GRID>();
+}
+
+// 1-D bulk copies global -> shared (the TMA engine), completed on an
+// mbarrier: the barrier's phase completes when its one arrival (with the
+// expected byte count) and all the copies' bytes have landed.
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+// bounded: gives up (false) after about a second of suspended waits
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+    for (int it = 0; it < (1 << 22); ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(smem)), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
-// chunk c of entries [e0, e1) into ring slot r: the weights (16-byte
-// pieces spread over the lanes) and the entries (lanes 0..7)
-template <typename W>
-__device__ __forceinline__ void wread_issue(const W* __restrict__ wp, const int4* __restrict__ list,
+// chunk c of entries [e0, e1) into a ring slot: its weights (32 per entry)
+// and its entries.  Returns whether the chunk exists (was issued).
+// Bulk: two bulk copies issued by lane 0 onto the slot's barrier; sizes are
+// multiples of 16 bytes and both sources 16-byte aligned (256-byte aligned
+// buffers, whole entries of 16 bytes and of 32 weights).  The warp's reads of
+// the slot's previous chunk are complete (the caller's __syncwarp); the proxy
+// fence orders them before the copy's writes.
+// cp.async: 16-byte pieces spread over the lanes (entries on lanes 0..C-1),
+// one commit group per chunk, empty past the end.
+template <bool BULK, int C, typename W>
+__device__ __forceinline__ bool wread_issue(const W* __restrict__ wp, const int4* __restrict__ list,
                                             unsigned long long e0, unsigned long long e1, unsigned long long c,
-                                            W* ws, int4* ls, int lane) {
-    const unsigned long long first = e0 + c * kWreadChunk;
-    if (first < e1) {
-        constexpr int kPerEntry = 32 * (int)sizeof(W) / 16;  // 16-byte pieces per entry
-        constexpr int kPieces = kWreadChunk * kPerEntry;
-#pragma unroll
-        for (int r = 0; r < kPieces / 32; ++r) {
-            const int piece = lane + 32 * r;
-            const int k = piece / kPerEntry;  // entry of the piece
-            if (first + k < e1)
-                cp_async16(reinterpret_cast<char*>(ws) + piece * 16,
-                           reinterpret_cast<const char*>(wp + first * 32) + piece * 16);
+                                            W* ws, int4* ls, unsigned long long* bar, int lane) {
+    const unsigned long long first = e0 + c * C;
+    if constexpr (BULK) {
+        if (first >= e1) return false;
+        if (lane == 0) {
+            const unsigned cnt = (unsigned)(e1 - first < (unsigned long long)C ? e1 - first : C);
+            const unsigned wb = cnt * 32u * (unsigned)sizeof(W), lb = cnt * 16u;
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_expect_tx(bar, wb + lb);
+            bulk_copy_g2s(ws, wp + first * 32, wb, bar);
+            bulk_copy_g2s(ls, list + first, lb, bar);
         }
-        if (lane < kWreadChunk && first + lane < e1) cp_async16(ls + lane, list + first + lane);
+        return true;
+    } else {
+        const bool have = first < e1;
+        if (have) {
+            constexpr int kPerEntry = 32 * (int)sizeof(W) / 16;  // 16-byte pieces per entry
+            constexpr int kPieces = C * kPerEntry;
+            static_assert(kPieces % 32 == 0 && C <= 32, "pieces spread evenly over the lanes");
+#pragma unroll
+            for (int r = 0; r < kPieces / 32; ++r) {
+                const int piece = lane + 32 * r;
+                const int k = piece / kPerEntry;  // entry of the piece
+                if (first + k < e1)
+                    cp_async16(reinterpret_cast<char*>(ws) + piece * 16,
+                               reinterpret_cast<const char*>(wp + first * 32) + piece * 16);
+            }
+            if (lane < C && first + lane < e1) cp_async16(ls + lane, list + first + lane);
+        }
+        cp_async_commit();
+        return have;
     }
-    cp_async_commit();  // one group per chunk, empty past the end
 }
 
 template <bool GRID, bool SCREENED, int PREC, int SHAPE>
-__global__ void __launch_bounds__(kGwnWarps * 32, 4) k_gwn_wread(GwnArgs a) {
+__global__ void __launch_bounds__(kGwnWarps * 32, WreadCfg<GRID>::kBlocks) k_gwn_wread(GwnArgs a) {
     constexpr int NQ = nq_of<GRID>();
-    constexpr int C = kWreadChunk;
+    constexpr int C = WreadCfg<GRID>::kChunk;
+    constexpr bool BULK = WreadCfg<GRID>::kBulk;
+    constexpr int WB = wread_warp_bytes<GRID>();
     using WT = WeightOf<NQ>;
     using W = typename WT::T;
     static_assert(sizeof(W) <= 8, "ring sized for two samples per lane");
     using Acc = typename AccType<PREC>::T;
     extern __shared__ __align__(16) unsigned char wread_smem[];
+    __shared__ __align__(8) unsigned long long wbar[kGwnWarps][kWreadRing];
     const unsigned FULL = 0xffffffffu;
     GwnWeightState* const wst = a.wsel;
     if (wst->mode != 2) return;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    W* const wring = reinterpret_cast<W*>(wread_smem + warp * kWreadWarpBytes);
-    int4* const lring = reinterpret_cast<int4*>(wread_smem + warp * kWreadWarpBytes + kWreadRing * C * 32 * 8);
+    W* const wring = reinterpret_cast<W*>(wread_smem + warp * WB);
+    int4* const lring = reinterpret_cast<int4*>(wread_smem + warp * WB + kWreadRing * C * 32 * 8);
+    unsigned long long* const bar = wbar[warp];
+    if (BULK && lane == 0) {
+        for (int r = 0; r < kWreadRing; ++r) mbar_init(bar + r);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    unsigned parity = 0;  // bulk: bit r, the phase of ring slot r to wait for next
+    unsigned pend = 0;    // bulk: bit r, slot r has a chunk in flight
+    bool wait_ok = true;  // warp-uniform
     const W* const wp = reinterpret_cast<const W*>(a.wbuf) + (size_t)wst->slot * a.wstride;
     if (a.terms_total && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(a.terms_total, wst->node_terms[wst->slot]);
     const float sigma = a.sigma_dev ? *a.sigma_dev : a.sigma;
@@ -835,13 +918,27 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 4) k_gwn_wread(GwnArgs a) {
         const unsigned long long e0 = a.list_off[g], e1 = a.list_off[g + 1];
         const unsigned long long nchunk = (e1 - e0 + C - 1) / C;
         __syncwarp();  // the ring's last readers (previous group) are done
+        // a group's chunk c sits in ring slot c % kWreadRing (every issued
+        // chunk is waited for before its group ends, so no copy spans groups)
 #pragma unroll
         for (int c = 0; c < kWreadRing - 1; ++c)
-            wread_issue(wp, a.list, e0, e1, c, wring + c * C * 32, lring + c * C, lane);
+            if (wread_issue<BULK, C>(wp, a.list, e0, e1, c, wring + c * C * 32, lring + c * C, bar + c, lane))
+                pend |= 1u << c;
         for (unsigned long long c = 0; c < nchunk; ++c) {
-            cp_async_wait_1();  // chunk c has landed (c + 1 may be in flight)
-            __syncwarp();
             const int r = (int)(c % kWreadRing);
+            // chunk c has landed (c + 1 may be in flight)
+            if constexpr (BULK) {
+                // every lane waits (each needs the copy's bytes visible); after
+                // a wait that gave up, the slot's contents are unknown: the
+                // warp reads none of them (its entries index node records)
+                wait_ok = __all_sync(FULL, mbar_wait(bar + r, (parity >> r) & 1u));
+                if (!wait_ok) break;
+                parity ^= 1u << r;
+                pend &= ~(1u << r);
+            } else {
+                cp_async_wait_1();
+                __syncwarp();
+            }
             const W* wc = wring + r * C * 32;
             const int4* lc = lring + r * C;
             const unsigned long long first = e0 + c * C;
@@ -902,15 +999,28 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 4) k_gwn_wread(GwnArgs a) {
             __syncwarp();  // ring slot (c + 2) % 3 = (c - 1) % 3 was read in the previous pass
             const unsigned long long nx = c + kWreadRing - 1;
             const int rn = (int)(nx % kWreadRing);
-            wread_issue(wp, a.list, e0, e1, nx, wring + rn * C * 32, lring + rn * C, lane);
+            if (wread_issue<BULK, C>(wp, a.list, e0, e1, nx, wring + rn * C * 32, lring + rn * C, bar + rn, lane))
+                pend |= 1u << rn;
         }
 #pragma unroll
         for (int u = 0; u < NQ; ++u) {
             if (valid[u]) a.out[qi[u]] = (float)sum[u];
             my_terms += (unsigned long long)nt[u];
         }
+        if (!wait_ok) break;
     }
-    asm volatile("cp.async.wait_all;" ::: "memory");  // no copy outlives the block
+    if constexpr (BULK) {
+        // every issued chunk was waited for, so no copy outlives the block,
+        // unless a wait gave up (a copy that never landed): that is reported,
+        // and the chunks still in flight get one more bounded wait each
+        if (!wait_ok) {
+            if (lane == 0) atomicOr(&a.work[1], 16u);
+            for (int r = 0; r < kWreadRing; ++r)
+                if ((pend >> r) & 1u) (void)mbar_wait(bar + r, (parity >> r) & 1u);
+        }
+    } else {
+        asm volatile("cp.async.wait_all;" ::: "memory");  // no copy outlives the block
+    }
     if (a.terms_total) {
         for (int o = 16; o > 0; o >>= 1) my_terms += __shfl_down_sync(FULL, my_terms, o);
         if (lane == 0 && my_terms) atomicAdd(a.terms_total, my_terms);
@@ -1229,14 +1339,14 @@ static int listed_shape(GwnArgs& a, GwnList& L, const Octree& t, cudaStream_t s,
         int& bpw = bpw_dev[dev];
         if (!bpw) {
             DWG_CHECK_CUDA(cudaFuncSetAttribute(k_gwn_wread<GRID, SCREENED, PREC, SHAPE>,
-                                                cudaFuncAttributeMaxDynamicSharedMemorySize, kWreadSmem));
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, wread_smem<GRID>()));
             DWG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpw, k_gwn_wread<GRID, SCREENED, PREC, SHAPE>,
-                                                                         kGwnWarps * 32, kWreadSmem));
+                                                                         kGwnWarps * 32, wread_smem<GRID>()));
             if (bpw < 1) bpw = 1;
         }
         const long long all = (long long)num_sms() * bpw;
         const unsigned gw = (unsigned)(a.ngroups < all * kGwnWarps ? (a.ngroups + kGwnWarps - 1) / kGwnWarps : all);
-        k_gwn_wread<GRID, SCREENED, PREC, SHAPE><<<gw, kGwnWarps * 32, kWreadSmem, s>>>(a);
+        k_gwn_wread<GRID, SCREENED, PREC, SHAPE><<<gw, kGwnWarps * 32, wread_smem<GRID>(), s>>>(a);
         DWG_CHECK_LAUNCH();
     }
     return DWG_OK;

@@ -70,7 +70,8 @@ int dwg_octree_update_info(dwg_octree* tree, const float* normals_dev, const flo
 /* Sticky error word of the traversal kernels of this tree (synchronises):
  * 0 = none; bit 0 stack overflow, bit 1 malformed node links, bit 2 leaf
  * range outside the point array, bit 3 an opening threshold that failed its
- * self-check.  Any set bit makes the call return DWG_ERR_DEVICE. */
+ * self-check, bit 4 a bulk copy of the kept-weight reader that did not land
+ * within its bounded wait.  Any set bit makes the call return DWG_ERR_DEVICE. */
 int dwg_octree_status(const dwg_octree* tree, unsigned int* flags);
 /* Size of the interaction list dwg_gwn_grid keeps (params->lists >= 1): its
  * entries (16 bytes each) and the weight slots it holds (8 bytes per entry
