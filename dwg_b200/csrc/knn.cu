@@ -289,11 +289,13 @@ struct TopK {
     unsigned long long e[KMAX];
     unsigned long long mx;  // the k-th key (max of the set) or NONE
     int mpos;
+    int fill;  // keys entered so far, up to k: the slots fill in order before any maximum search
     __device__ __forceinline__ void init(int k) {
 #pragma unroll
         for (int q = 0; q < KMAX; ++q) e[q] = q < k ? ~0ull : 0ull;  // unused slots never become the max
         mx = ~0ull;
         mpos = 0;
+        fill = 0;
     }
     // k slots holding the key T: only keys below T enter, and T must bound
     // the k-th key from above so that every slot is replaced
@@ -302,6 +304,35 @@ struct TopK {
         for (int q = 0; q < KMAX; ++q) e[q] = q < k ? T : 0ull;
         mx = T;
         mpos = 0;
+        fill = 0;
+    }
+    // enter v (v < mx): the first k keys take the slots in turn (the
+    // maximum stays the initial key until the last slot is taken, then it is
+    // searched once), later keys replace the maximum
+    __device__ __forceinline__ void push(unsigned long long v, int k) {
+        if (fill < k) {
+#pragma unroll
+            for (int q = 0; q < KMAX; ++q)
+                if (q == fill) e[q] = v;
+            if (++fill == k) {
+                mx = e[0];
+                mpos = 0;
+#pragma unroll
+                for (int q = 1; q < KMAX; ++q)
+                    if (e[q] > mx) {
+                        mx = e[q];
+                        mpos = q;
+                    }
+            }
+        } else {
+            replace_max(v);
+        }
+    }
+    // drop e[0] of a sorted set: the keys move down one slot, NONE enters on top
+    __device__ __forceinline__ void shift_down() {
+#pragma unroll
+        for (int q = 0; q + 1 < KMAX; ++q) e[q] = e[q + 1];
+        e[KMAX - 1] = ~0ull;
     }
     // replace the maximum by v (v < mx) and find the new maximum (a warp's
     // lanes take the same steps whether or not their slots are all filled)
@@ -409,7 +440,7 @@ __device__ __forceinline__ void knn_pyramid(const KnnArgs& a, float qx, float qy
                 if (a.exclude && a.exclude[id]) continue;
                 const float d2 = sq3_rn(__fsub_rn(pp.x, qx), __fsub_rn(pp.y, qy), __fsub_rn(pp.z, qz));
                 const unsigned long long v = ((unsigned long long)__float_as_uint(d2) << 32) | (unsigned)id;
-                if (v < top.mx) top.replace_max(v);
+                if (v < top.mx) top.push(v, a.k);
             }
             continue;
         }
@@ -488,7 +519,7 @@ __global__ void __launch_bounds__(128, KMAX <= 10 ? 4 : 1) k_knn_thread(KnnArgs 
                             const float d2 =
                                 sq3_rn(__fsub_rn(pp.x, qx), __fsub_rn(pp.y, qy), __fsub_rn(pp.z, qz));
                             const unsigned long long v = ((unsigned long long)__float_as_uint(d2) << 32) | (unsigned)id;
-                            if (v < top.mx) top.replace_max(v);
+                            if (v < top.mx) top.push(v, k);
                         }
                     }
                 }
@@ -917,18 +948,26 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
             for (int t = lane; t < qn; t += 32) fb[atomicAdd(&work[1], 1)] = order[qs + t];
             continue;
         }
-        // stages C + D, per chunk of 32 queries: the points of the frontier
-        // cells within R of the centre are streamed through shared memory and
-        // every lane ranks them for its own query, starting from the bound
-        // kb[c] + |q - x_c| on its 16th distance
+        // stages C + D, per chunk of up to 32 queries: the points of the
+        // frontier cells within R of the centre are streamed through shared
+        // memory and ranked for every query, starting from the bound
+        // kb[c] + |q - x_c| on its 16th distance.  A chunk of nb queries gives
+        // each query G lanes (the largest power of two with nb * G <= 32): a
+        // lane ranks every G-th staged point for its query, and the G lanes'
+        // sets are merged at the end.  Cells hold a few queries, so this
+        // keeps the lanes busy instead of ranking for absent queries.
         const float kbc = kb[c];
         const float R2 = R * R;
         for (int base = 0; base < qn; base += 32) {
-            const bool has = base + lane < qn;
+            const int nb = qn - base < 32 ? qn - base : 32;
+            const int lg = nb > 16 ? 0 : nb > 8 ? 1 : nb > 4 ? 2 : nb > 2 ? 3 : nb > 1 ? 4 : 5;
+            const int G = 1 << lg;
+            const int u = lane >> lg, sl = lane & (G - 1);
+            const bool has = u < nb;
             long long qi = 0;
             float qx = x, qy = y, qz = z;
             if (has) {
-                qi = order[qs + base + lane];
+                qi = order[qs + base + u];
                 knn_load_query(a, qi, qx, qy, qz);
             }
             const float ex = qx - x, ey = qy - y, ez = qz - z;
@@ -939,12 +978,14 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
             int staged = 0;
             auto rank = [&]() {
                 __syncwarp();
-                for (int t = 0; t < staged; ++t) {
-                    const float4 pp = stage[w][t];
-                    const float d2 = sq3_rn(__fsub_rn(pp.x, qx), __fsub_rn(pp.y, qy), __fsub_rn(pp.z, qz));
-                    const unsigned long long v = ((unsigned long long)__float_as_uint(d2) << 32) |
-                                                 (unsigned)__float_as_int(pp.w);
-                    if (v < top.mx) top.replace_max(v);
+                if (has) {
+                    for (int t = sl; t < staged; t += G) {
+                        const float4 pp = stage[w][t];
+                        const float d2 = sq3_rn(__fsub_rn(pp.x, qx), __fsub_rn(pp.y, qy), __fsub_rn(pp.z, qz));
+                        const unsigned long long v = ((unsigned long long)__float_as_uint(d2) << 32) |
+                                                     (unsigned)__float_as_int(pp.w);
+                        if (v < top.mx) top.push(v, k);
+                    }
                 }
                 __syncwarp();
                 staged = 0;
@@ -1014,11 +1055,32 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
             }
             if (staged > 0) rank();
             top.sort();
-            if (has) {
+            if (G == 1) {
+                if (has) {
 #pragma unroll
-                for (int t = 0; t < KMAX; ++t) {
-                    const int o = t - (KMAX - k);
-                    if (o >= 0) a.out[qi * k + o] = top.e[t] == NONE ? -1 : (int)(unsigned)(top.e[t] & 0xffffffffu);
+                    for (int t = 0; t < KMAX; ++t) {
+                        const int o = t - (KMAX - k);
+                        if (o >= 0)
+                            a.out[qi * k + o] = top.e[t] == NONE ? -1 : (int)(unsigned)(top.e[t] & 0xffffffffu);
+                    }
+                }
+            } else {
+                // slots >= k hold 0 and sort first: drop them, then k rounds
+                // of the minimum over the G lanes' smallest keys (aligned
+                // groups, so the butterfly stays inside the group); the lane
+                // holding it drops it.  Keys are unique (one index each), the
+                // initial key T and NONE aside, which give -1 as before.
+#pragma unroll 1
+                for (int z = 0; z < KMAX - k; ++z) top.shift_down();
+#pragma unroll 1
+                for (int r = 0; r < k; ++r) {
+                    unsigned long long m = top.e[0];
+                    for (int o = 1; o < G; o <<= 1) {
+                        const unsigned long long v = __shfl_xor_sync(FULL, m, o);
+                        m = v < m ? v : m;
+                    }
+                    if (top.e[0] == m) top.shift_down();
+                    if (has && sl == 0) a.out[qi * k + r] = m == NONE ? -1 : (int)(unsigned)(m & 0xffffffffu);
                 }
             }
         }
