@@ -50,7 +50,11 @@ __global__ void k_knn_scatter(const float* __restrict__ P, int n, const int* __r
     pts[slot] = make_float4(P[(size_t)i * 3], P[(size_t)i * 3 + 1], P[(size_t)i * 3 + 2], __int_as_float(i));
 }
 
-// level 1 of the occupancy pyramid from the cell ranges
+// The occupancy pyramid: node c of level l >= 1 holds the mask of its
+// occupied children (bit t for the child 2 * (i, j, k) + (t & 1, t >> 1 & 1,
+// t >> 2), cells at level 1), so a node is occupied iff its byte is nonzero
+// and a walk skips empty children without loading them.
+// level 1 from the cell ranges
 __global__ void k_pyr_first(const int* __restrict__ cell_start, int G0, int G1, int G2, int D0, int D1, int D2,
                             unsigned char* __restrict__ occ) {
     long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -61,7 +65,7 @@ __global__ void k_pyr_first(const int* __restrict__ cell_start, int G0, int G1, 
         const int x = 2 * i + (t & 1), y = 2 * j + ((t >> 1) & 1), z = 2 * k + (t >> 2);
         if (x >= G0 || y >= G1 || z >= G2) continue;
         const long long f = x + (long long)G0 * (y + (long long)G1 * z);
-        o |= cell_start[f + 1] > cell_start[f] ? 1 : 0;
+        o |= (unsigned char)((cell_start[f + 1] > cell_start[f] ? 1 : 0) << t);
     }
     occ[c] = o;
 }
@@ -76,7 +80,7 @@ __global__ void k_pyr_next(const unsigned char* __restrict__ prev, int P0, int P
     for (int t = 0; t < 8; ++t) {
         const int x = 2 * i + (t & 1), y = 2 * j + ((t >> 1) & 1), z = 2 * k + (t >> 2);
         if (x >= P0 || y >= P1 || z >= P2) continue;
-        o |= prev[x + (long long)P0 * (y + (long long)P1 * z)];
+        o |= (unsigned char)((prev[x + (long long)P0 * (y + (long long)P1 * z)] != 0 ? 1 : 0) << t);
     }
     occ[c] = o;
 }
@@ -387,9 +391,11 @@ struct TopK {
 // Depth-first from the 1x1x1 top level, the children of a node in the order
 // of their octant's distance from the query's octant (same octant, then the
 // three face neighbours, the three edge neighbours, the opposite one); a
-// node is skipped when it is empty or its (eps-widened) box is farther than
-// the current k-th candidate.  The walk is stackless: a 4-bit child counter
-// per level in one 64-bit word and the current node's coordinates.
+// node is skipped when it is empty (its bit in the parent's child mask: no
+// load) or its (eps-widened) box is farther than the current k-th candidate.
+// The walk is stackless: a 4-bit child counter per level in one 64-bit word,
+// the child masks of the nodes on the path (a byte per level in two 64-bit
+// words) and the current node's coordinates.
 template <int KMAX>
 __device__ __forceinline__ void knn_pyramid(const KnnArgs& a, float qx, float qy, float qz, int cx, int cy, int cz,
                                             TopK<KMAX>& top) {
@@ -399,6 +405,13 @@ __device__ __forceinline__ void knn_pyramid(const KnnArgs& a, float qx, float qy
     const int top_l = a.levels;
     int lvl = top_l, ci = 0, cj = 0, ck = 0;
     unsigned long long ctr = 0;
+    // byte l of (mk1:mk0): the child mask of the path's node at level l
+    unsigned long long mk0 = 0ull, mk1 = 0ull;
+    {
+        const unsigned long long tm = (unsigned long long)a.occ[a.loff[top_l]] << (8 * (top_l & 7));
+        if (top_l < 8) mk0 = tm;
+        else mk1 = tm;
+    }
     for (;;) {
         const int sh = 4 * lvl;
         const int c = (int)((ctr >> sh) & 15ull);
@@ -419,9 +432,10 @@ __device__ __forceinline__ void knn_pyramid(const KnnArgs& a, float qx, float qy
         const float mz = a.g.lo2 + (float)((ck << lvl) + half) * h;
         const int qo = (qx >= mx ? 1 : 0) | (qy >= my ? 2 : 0) | (qz >= mz ? 4 : 0);
         const int oc = qo ^ (int)((0x76534210u >> (4 * c)) & 7u);
+        // empty or outside the grid (such children have no bit)
+        if (!(((lvl < 8 ? mk0 : mk1) >> (8 * (lvl & 7) + oc)) & 1ull)) continue;
         const int nl = lvl - 1;
         const int ni = (ci << 1) | (oc & 1), nj = (cj << 1) | ((oc >> 1) & 1), nk = (ck << 1) | (oc >> 2);
-        if (ni >= a.ldim[nl][0] || nj >= a.ldim[nl][1] || nk >= a.ldim[nl][2]) continue;
         const float kd2 = top.mx == NONE ? INFINITY : __uint_as_float((unsigned)(top.mx >> 32)) * 1.00001f;
         const float x0 = a.g.lo0 + (float)(ni << nl) * h - eps, x1 = a.g.lo0 + (float)((ni + 1) << nl) * h + eps;
         const float y0 = a.g.lo1 + (float)(nj << nl) * h - eps, y1 = a.g.lo1 + (float)((nj + 1) << nl) * h + eps;
@@ -445,7 +459,10 @@ __device__ __forceinline__ void knn_pyramid(const KnnArgs& a, float qx, float qy
             continue;
         }
         const int* D = a.ldim[nl];
-        if (!a.occ[a.loff[nl] + ni + (long long)D[0] * (nj + (long long)D[1] * nk)]) continue;
+        const unsigned long long cm = a.occ[a.loff[nl] + ni + (long long)D[0] * (nj + (long long)D[1] * nk)];
+        const int bs = 8 * (nl & 7);
+        if (nl < 8) mk0 = (mk0 & ~(0xffull << bs)) | (cm << bs);
+        else mk1 = (mk1 & ~(0xffull << bs)) | (cm << bs);
         lvl = nl;
         ci = ni;
         cj = nj;
