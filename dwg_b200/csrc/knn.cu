@@ -220,6 +220,10 @@ struct KnnArgs {
     // per-cell bound of the 16th-neighbour distance (null: none), seeds the
     // per-thread search of queries with k <= 16
     const float* __restrict__ kb;
+    // queries whose pyramid walk ran past kDeepBudget visits go on this list
+    // (null: no budget) and are finished by k_knn_deep
+    int* __restrict__ deep;
+    int* __restrict__ deep_count;
     // occupancy pyramid
     const unsigned char* __restrict__ occ;
     int levels;
@@ -395,9 +399,13 @@ struct TopK {
 // load) or its (eps-widened) box is farther than the current k-th candidate.
 // The walk is stackless: a 4-bit child counter per level in one 64-bit word,
 // the child masks of the nodes on the path (a byte per level in two 64-bit
-// words) and the current node's coordinates.
+// words) and the current node's coordinates.  With a deep list the walk
+// gives up after kDeepBudget child visits (returns false): a query that far
+// from its neighbours is finished by a warp of k_knn_deep instead of holding
+// a thread (and its warp) for the length of a long walk.
+constexpr int kDeepBudget = 1024;
 template <int KMAX>
-__device__ __forceinline__ void knn_pyramid(const KnnArgs& a, float qx, float qy, float qz, int cx, int cy, int cz,
+__device__ __forceinline__ bool knn_pyramid(const KnnArgs& a, float qx, float qy, float qz, int cx, int cy, int cz,
                                             TopK<KMAX>& top) {
     const unsigned long long NONE = ~0ull;
     const float h = a.g.h;
@@ -405,6 +413,7 @@ __device__ __forceinline__ void knn_pyramid(const KnnArgs& a, float qx, float qy
     const int top_l = a.levels;
     int lvl = top_l, ci = 0, cj = 0, ck = 0;
     unsigned long long ctr = 0;
+    int visits = 0;
     // byte l of (mk1:mk0): the child mask of the path's node at level l
     unsigned long long mk0 = 0ull, mk1 = 0ull;
     {
@@ -425,6 +434,7 @@ __device__ __forceinline__ void knn_pyramid(const KnnArgs& a, float qx, float qy
             continue;
         }
         ctr += 1ull << sh;
+        if (a.deep && ++visits > kDeepBudget) return false;
         // octant of the query about the node's midpoint
         const int half = 1 << (lvl - 1);
         const float mx = a.g.lo0 + (float)((ci << lvl) + half) * h;
@@ -468,6 +478,7 @@ __device__ __forceinline__ void knn_pyramid(const KnnArgs& a, float qx, float qy
         cj = nj;
         ck = nk;
     }
+    return true;
 }
 
 // One thread per query; queries are processed in the order of their coarse
@@ -494,6 +505,7 @@ __global__ void __launch_bounds__(128, KMAX <= 10 ? 4 : 1) k_knn_thread(KnnArgs 
         const int cy = cell_coord(qy, a.g.lo1, a.g.inv_h, a.g.G1);
         const int cz = cell_coord(qz, a.g.lo2, a.g.inv_h, a.g.G2);
         TopK<KMAX> top;
+        bool deferred = false;
         if (a.kb && k <= kKnnBoundK) {
             // start from k copies of the key of the bound kb[c] + |q - x_c|
             // on the 16th distance: everything beyond it is pruned at once
@@ -556,10 +568,14 @@ __global__ void __launch_bounds__(128, KMAX <= 10 ? 4 : 1) k_knn_thread(KnnArgs 
                 if (bd > 0.f && __uint_as_float((unsigned)(top.mx >> 32)) < bd * bd * 0.9999f) break;
             }
             if (r == 1 && a.levels > 0) {
-                knn_pyramid<KMAX>(a, qx, qy, qz, cx, cy, cz, top);
+                if (!knn_pyramid<KMAX>(a, qx, qy, qz, cx, cy, cz, top)) {
+                    a.deep[atomicAdd(a.deep_count, 1)] = (int)qi;  // at most once per query: the list holds nq
+                    deferred = true;
+                }
                 break;
             }
         }
+        if (deferred) continue;
         top.sort();
         // slots >= k hold 0 (below every key) and sort first; results start at KMAX - k
 #pragma unroll
@@ -1105,6 +1121,210 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
     }
 }
 
+// ------------------------------------------------------------ deep queries --
+// The queries whose per-thread walk ran past its budget (far from every
+// point, so the walk's bound tightens late), one warp per query, level by
+// level down the occupancy pyramid.  The frontier holds the nodes that may
+// contain one of the k nearest; a level's children come from the nodes'
+// child masks, and a child stays when its (eps-widened) box is within the
+// bound U of the query.  After each level U is lowered to the k-th smallest,
+// over the lanes, of each lane's smallest far-corner distance among the
+// children it kept: those are k distinct occupied nodes, so k points lie
+// within it.  At the cells, every lane ranks the points of its share of the
+// cells within U, and the 32 lanes' sets are merged.  A level whose children
+// do not fit the frontier is retried once with the lowered U; if they still
+// do not fit, the cells under the current level's nodes are enumerated.
+constexpr int kDeepWarps = 4;
+constexpr int kDeepNodes = 1024;
+
+// k-th smallest (1 <= k <= 32) of one value per lane, to every lane
+__device__ __forceinline__ float warp_kth_smallest(float v, int k) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int size = 2; size <= 32; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            const float o = __shfl_xor_sync(0xffffffffu, v, stride);
+            const bool asc = (lane & size) == 0 || size == 32;
+            const bool low = (lane & stride) == 0;
+            v = (low == asc) ? fminf(v, o) : fmaxf(v, o);
+        }
+    }
+    return __shfl_sync(0xffffffffu, v, k - 1);
+}
+
+// squared distances from q to the nearest and the farthest point of the
+// eps-widened box of node (ni, nj, nk) of level l
+__device__ __forceinline__ void node_d2(const KnnArgs& a, int l, int ni, int nj, int nk, float qx, float qy, float qz,
+                                        float eps, float& mind2, float& maxd2) {
+    const float h = a.g.h;
+    const float x0 = a.g.lo0 + (float)(ni << l) * h - eps, x1 = a.g.lo0 + (float)((ni + 1) << l) * h + eps;
+    const float y0 = a.g.lo1 + (float)(nj << l) * h - eps, y1 = a.g.lo1 + (float)((nj + 1) << l) * h + eps;
+    const float z0 = a.g.lo2 + (float)(nk << l) * h - eps, z1 = a.g.lo2 + (float)((nk + 1) << l) * h + eps;
+    const float dx = fmaxf(0.f, fmaxf(x0 - qx, qx - x1)), fx = fmaxf(qx - x0, x1 - qx);
+    const float dy = fmaxf(0.f, fmaxf(y0 - qy, qy - y1)), fy = fmaxf(qy - y0, y1 - qy);
+    const float dz = fmaxf(0.f, fmaxf(z0 - qz, qz - z1)), fz = fmaxf(qz - z0, z1 - qz);
+    mind2 = dx * dx + dy * dy + dz * dz;
+    maxd2 = fx * fx + fy * fy + fz * fz;
+}
+
+__device__ __forceinline__ int pack3(int i, int j, int k) { return i | (j << 10) | (k << 20); }
+
+template <int KMAX>
+__global__ void __launch_bounds__(kDeepWarps * 32) k_knn_deep(KnnArgs a, const int* __restrict__ list,
+                                                             const int* __restrict__ count, int* __restrict__ work) {
+    __shared__ int fco[kDeepWarps][2][kDeepNodes];
+    __shared__ unsigned char fmk[kDeepWarps][2][kDeepNodes];
+    if (a.gate_count && *a.gate_count <= a.gate_min) return;
+    const unsigned FULL = 0xffffffffu;
+    const unsigned long long NONE = ~0ull;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned below = (1u << lane) - 1u;
+    const int nd = *count;
+    const int k = a.k;
+    const float eps = 1e-4f * a.g.h + 1e-6f;
+    for (;;) {
+        int j = 0;
+        if (lane == 0) j = atomicAdd(work, 1);
+        j = __shfl_sync(FULL, j, 0);
+        if (j >= nd) break;
+        const long long qi = list[j];
+        float qx, qy, qz;
+        knn_load_query(a, qi, qx, qy, qz);
+        int* cur = fco[w][0];
+        unsigned char* curm = fmk[w][0];
+        int* nxt = fco[w][1];
+        unsigned char* nxtm = fmk[w][1];
+        int lvl = a.levels;
+        if (lane == 0) {
+            cur[0] = 0;
+            curm[0] = a.occ[a.loff[lvl]];
+        }
+        int nf = 1;
+        float U2 = INFINITY;
+        __syncwarp();
+        while (lvl > 0) {
+            const int nl = lvl - 1;
+            const int* D = a.ldim[nl];
+            int nn = 0;
+            for (int pass = 0; pass < 2; ++pass) {
+                float lmin = INFINITY;
+                nn = 0;
+                for (int b = 0; b < nf * 8; b += 32) {
+                    const int t = b + lane;
+                    bool keep = false;
+                    int cc = 0;
+                    unsigned char cm = 0;
+                    if (t < nf * 8 && ((curm[t >> 3] >> (t & 7)) & 1)) {
+                        const int pc = cur[t >> 3], oc = t & 7;
+                        const int ni = ((pc & 1023) << 1) | (oc & 1), nj = (((pc >> 10) & 1023) << 1) | ((oc >> 1) & 1),
+                                  nk = ((pc >> 20) << 1) | (oc >> 2);
+                        float mind2, maxd2;
+                        node_d2(a, nl, ni, nj, nk, qx, qy, qz, eps, mind2, maxd2);
+                        if (mind2 <= U2) {
+                            keep = true;
+                            lmin = fminf(lmin, maxd2);
+                            cc = pack3(ni, nj, nk);
+                            if (nl > 0) cm = a.occ[a.loff[nl] + ni + (long long)D[0] * (nj + (long long)D[1] * nk)];
+                        }
+                    }
+                    const unsigned bal = __ballot_sync(FULL, keep);
+                    const int pos = nn + __popc(bal & below);
+                    if (keep && pos < kDeepNodes) {
+                        nxt[pos] = cc;
+                        nxtm[pos] = cm;
+                    }
+                    nn += __popc(bal);
+                }
+                const float kth = warp_kth_smallest(lmin, k);
+                if (kth < INFINITY) U2 = fminf(U2, kth * 1.0001f);
+                if (nn <= kDeepNodes) break;
+            }
+            __syncwarp();
+            if (nn > kDeepNodes) break;  // the cells under this level's nodes are enumerated below
+            int* ti = cur;
+            cur = nxt;
+            nxt = ti;
+            unsigned char* tm = curm;
+            curm = nxtm;
+            nxtm = tm;
+            nf = nn;
+            lvl = nl;
+        }
+        // rank the points of the cells within U (cells of the frontier, or
+        // under its nodes of level lvl), a lane per point of 32 cells at a time
+        TopK<KMAX> top;
+        if (U2 < INFINITY)
+            top.init_bound(k, ((unsigned long long)__float_as_uint(U2) << 32) | 0xffffffffull);
+        else
+            top.init(k);
+        const int side = 1 << lvl;
+        const long long per = (long long)side * side * side;
+        const long long total = (long long)nf * per;
+        for (long long b = 0; b < total; b += 32) {
+            const long long t = b + lane;
+            int s0 = 0, cnt = 0;
+            if (t < total) {
+                const int pc = cur[t / per];
+                const int o = (int)(t % per);
+                const int ci = (pc & 1023) * side + o % side, cj = ((pc >> 10) & 1023) * side + (o / side) % side,
+                          ck = (pc >> 20) * side + o / (side * side);
+                if (ci < a.g.G0 && cj < a.g.G1 && ck < a.g.G2) {
+                    float mind2, maxd2;
+                    node_d2(a, 0, ci, cj, ck, qx, qy, qz, eps, mind2, maxd2);
+                    if (mind2 <= U2) {
+                        const int cell = ci + a.g.G0 * (cj + a.g.G1 * ck);
+                        s0 = a.cell_start[cell];
+                        cnt = a.cell_start[cell + 1] - s0;
+                    }
+                }
+            }
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const int excl = incl - cnt;
+            const int tot = __shfl_sync(FULL, incl, 31);
+            for (int pb = 0; pb < tot; pb += 32) {
+                const int tp = pb + lane;
+                int own = 0;
+#pragma unroll
+                for (int st = 16; st > 0; st >>= 1) {
+                    const int e = __shfl_sync(FULL, excl, own + st);
+                    if (e <= tp) own += st;
+                }
+                const int os0 = __shfl_sync(FULL, s0, own);
+                const int oex = __shfl_sync(FULL, excl, own);
+                if (tp < tot) {
+                    const float4 pp = a.pts[os0 + (tp - oex)];
+                    const float d2 = sq3_rn(__fsub_rn(pp.x, qx), __fsub_rn(pp.y, qy), __fsub_rn(pp.z, qz));
+                    const unsigned long long v = ((unsigned long long)__float_as_uint(d2) << 32) |
+                                                 (unsigned)__float_as_int(pp.w);
+                    if (v < top.mx) top.push(v, k);
+                }
+            }
+        }
+        // merge the 32 lanes' sets (as in k_knn_cells)
+        top.sort();
+#pragma unroll 1
+        for (int z = 0; z < KMAX - k; ++z) top.shift_down();
+#pragma unroll 1
+        for (int r = 0; r < k; ++r) {
+            unsigned long long m = top.e[0];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long v = __shfl_xor_sync(FULL, m, o);
+                m = v < m ? v : m;
+            }
+            if (top.e[0] == m) top.shift_down();
+            if (lane == 0) a.out[qi * k + r] = m == NONE ? -1 : (int)(unsigned)(m & 0xffffffffu);
+        }
+        __syncwarp();
+    }
+}
+
 template <int KMAX>
 static int knn_launch(const KnnArgs& a, long long nq, cudaStream_t s) {
     static int bps = 0;
@@ -1133,12 +1353,26 @@ static int cells_launch(const KnnIndex& ix, const KnnArgs& a, long long nq, cuda
         a, ix.c_active.ptr, ix.c_misc.ptr, ix.c_start.ptr, ix.c_count.ptr, ix.c_m.ptr, ix.kb.ptr, ix.q_order.ptr,
         ix.c_misc.ptr + 1, ix.c_fb.ptr);
     DWG_CHECK_LAUNCH();
-    // the queries of cells whose candidate sets did not fit
+    // the queries of cells whose candidate sets did not fit, per thread;
+    // those far from every point finish one warp each
     KnnArgs f = a;
     f.order = ix.c_fb.ptr;
     f.nq_dev_i32 = ix.c_misc.ptr + 2;
     f.kb = ix.kb.ptr;
-    return knn_launch<KMAX>(f, nq, s);
+    f.deep = ix.levels > 0 ? ix.c_deep.ptr : nullptr;
+    f.deep_count = ix.c_misc.ptr + 3;
+    DWG_TRY(knn_launch<KMAX>(f, nq, s));
+    if (f.deep) {
+        static int dbps = 0;
+        if (!dbps) {
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dbps, k_knn_deep<KMAX>, kDeepWarps * 32, 0);
+            if (dbps <= 0) dbps = 1;
+        }
+        k_knn_deep<KMAX><<<(unsigned)(num_sms() * dbps), kDeepWarps * 32, 0, s>>>(f, ix.c_deep.ptr, ix.c_misc.ptr + 3,
+                                                                              ix.c_misc.ptr + 4);
+        DWG_CHECK_LAUNCH();
+    }
+    return DWG_OK;
 }
 
 // queries grouped by cell (k <= 16, no exclusion), see k_knn_cells
@@ -1150,13 +1384,14 @@ static int knn_query_cells(const KnnIndex& ix, const KnnArgs& a0, long long nq, 
     DWG_TRY(ix.c_fill.reserve(ncell + 1));
     DWG_TRY(ix.c_m.reserve(ncell));
     DWG_TRY(ix.c_active.reserve(ncell));
-    DWG_TRY(ix.c_misc.reserve(4));
+    DWG_TRY(ix.c_misc.reserve(8));
     DWG_TRY(ix.q_key.reserve(nq));
     DWG_TRY(ix.q_order.reserve(nq));
     DWG_TRY(ix.c_fb.reserve(nq));
+    DWG_TRY(ix.c_deep.reserve(nq));
     DWG_CHECK_CUDA(cudaMemsetAsync(ix.c_count.ptr, 0, sizeof(int) * (ncell + 1), s));
     DWG_CHECK_CUDA(cudaMemsetAsync(ix.c_m.ptr, 0, sizeof(unsigned int) * ncell, s));
-    DWG_CHECK_CUDA(cudaMemsetAsync(ix.c_misc.ptr, 0, sizeof(int) * 4, s));
+    DWG_CHECK_CUDA(cudaMemsetAsync(ix.c_misc.ptr, 0, sizeof(int) * 8, s));
     KnnArgs a = a0;
     long long blocks = (nq + 255) / 256;
     const long long cap = (long long)num_sms() * 8;
@@ -1290,6 +1525,8 @@ int knn_query(const KnnIndex& ix, const KnnQuery& q, int k, int* out, cudaStream
     }
     a.order = nullptr;
     a.kb = nullptr;
+    a.deep = nullptr;
+    a.deep_count = nullptr;
     if (k <= kKnnBoundK && !q.exclude && ix.n >= kKnnBoundK && q.use_cells) return knn_query_cells(ix, a, q.nq, s);
     // bucket the queries spatially (counting sort on device counts, no host sync)
     DWG_TRY(ix.q_key.reserve(q.nq));

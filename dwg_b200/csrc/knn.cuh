@@ -30,7 +30,7 @@ struct KnnIndex {
     mutable bool kb_ready = false;
     bool kb_per_query = false;
     // workspace of the cell-grouped queries
-    mutable DevBuf<int> c_count, c_start, c_fill, c_active, c_misc, c_fb;
+    mutable DevBuf<int> c_count, c_start, c_fill, c_active, c_misc, c_fb, c_deep;
     mutable DevBuf<unsigned int> c_m;
     mutable DevBuf<unsigned char> c_scratch;
     // query bucketing workspace (grown on demand; not thread safe)

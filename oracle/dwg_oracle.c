@@ -1041,7 +1041,7 @@ int dwgo_diffuse_normals(const int* knn, const float* tri_normals,
 /* LoadZeroData + kNN on the non-zero subset + SimpleUpdateNonzeroNormals
  * (src/TurboDWG.cu:145-177,322-359,585-644); subsets keep index order. */
 void dwgo_zero_repair(const float* Lpos, int L, float* normals,
-                      const unsigned char* is_zero, int k) {
+                      const unsigned char* is_zero, int k, int nthreads) {
     int nz = 0, nn = 0;
     for (int i = 0; i < L; i++) {
         if (is_zero[i]) nz++;
@@ -1065,7 +1065,7 @@ void dwgo_zero_repair(const float* Lpos, int L, float* normals,
         }
     }
     int* nb = xmalloc((size_t)nz * kk * sizeof(int));
-    dwgo_knn(np, nn, zp, nz, kk, 1, nb);
+    dwgo_knn(np, nn, zp, nz, kk, nthreads, nb);
     for (int z = 0; z < nz; z++) {
         float s[3] = {0, 0, 0};
         for (int j = 0; j < kk; j++) {
@@ -1609,7 +1609,7 @@ dwgo_run* dwgo_reconstruct(const float* P, int n, const float* N_in,
         int zc = dwgo_diffuse_normals(nb, tnrm, T, prm->knn_tri, L, lnrm, isz);
         free(nb);
         run->zero_count[it] = zc;
-        if (zc > prm->knn_zero) dwgo_zero_repair(lpos, L, lnrm, isz, prm->knn_zero);
+        if (zc > prm->knn_zero) dwgo_zero_repair(lpos, L, lnrm, isz, prm->knn_zero, nthreads);
     }
     free(gfield);
     run->L = L;

@@ -106,7 +106,7 @@ int dwgo_diffuse_normals(const int* knn, const float* tri_normals,
                          long long T, int k, int L, float* normals,
                          unsigned char* is_zero);
 void dwgo_zero_repair(const float* Lpos, int L, float* normals,
-                      const unsigned char* is_zero, int k);
+                      const unsigned char* is_zero, int k, int nthreads);
 void dwgo_gauss_map(const float* P, int n, float* normals);
 void dwgo_load_normals(const int* knn, int k, long long nq,
                        const float* leaf_normals, float* out);

@@ -99,7 +99,7 @@ def lib():
     L.dwgo_knn.argtypes = [_f32p, C.c_int, _f32p, C.c_longlong, C.c_int, C.c_int, _i32p]
     L.dwgo_diffuse_normals.restype = C.c_int
     L.dwgo_diffuse_normals.argtypes = [_i32p, _f32p, C.c_longlong, C.c_int, C.c_int, _f32p, _u8p]
-    L.dwgo_zero_repair.argtypes = [_f32p, C.c_int, _f32p, _u8p, C.c_int]
+    L.dwgo_zero_repair.argtypes = [_f32p, C.c_int, _f32p, _u8p, C.c_int, C.c_int]
     L.dwgo_gauss_map.argtypes = [_f32p, C.c_int, _f32p]
     L.dwgo_load_normals.argtypes = [_i32p, C.c_int, C.c_longlong, _f32p, _f32p]
     L.dwgo_radii.argtypes = [_f32p, C.c_int, _i32p, C.c_int, _f32p]
@@ -349,10 +349,10 @@ def diffuse_normals(knn_idx, tri_normals, normals):
     return normals, isz[:L].astype(bool), zc
 
 
-def zero_repair(Lpos, normals, is_zero, k=10):
+def zero_repair(Lpos, normals, is_zero, k=10, nthreads=None):
     normals = _f32(normals).copy()
     lib().dwgo_zero_repair(_f32(Lpos).reshape(-1), len(normals), normals.reshape(-1),
-                           np.ascontiguousarray(is_zero, np.uint8), k)
+                           np.ascontiguousarray(is_zero, np.uint8), k, nthreads or NTHREADS)
     return normals
 
 

@@ -394,6 +394,30 @@ def test_zero_repair_large_grid_bit_exact(oracle_lib, dwg_lib):
     assert np.array_equal(n_dev.cpu().numpy(), ref)
 
 
+@pytest.mark.parametrize("k", [10, 16])
+def test_zero_repair_far_queries_bit_exact(oracle_lib, dwg_lib, k):
+    # a grid above 2^22 cells with the cap z > 0.8 of the sphere flagged: the
+    # flagged points near the pole lie ~50 cells from every unflagged point,
+    # so their per-thread walk runs past its visit budget and the warp-per-
+    # query search over the pyramid finishes them
+    rng = np.random.default_rng(13)
+    L = 420000
+    v = rng.standard_normal((L, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    Lpos = (0.45 * v).astype(np.float32)
+    N0 = rng.standard_normal((L, 3)).astype(np.float32)
+    N0 /= np.linalg.norm(N0, axis=1, keepdims=True)
+    isz = v[:, 2] > 0.8
+    ref = oracle_lib.zero_repair(Lpos, N0, isz, k)
+    pos_d, n_dev = cu(Lpos), cu(N0)
+    isz_d = cu(isz.astype(np.uint8))
+    zc = torch.tensor([int(isz.sum())], dtype=torch.int32, device=DEV)
+    ix = turbo.KnnIndex(pos_d)
+    capi.check(dwg_lib.dwg_zero_repair(ix._h, capi.ptr(n_dev), capi.ptr(isz_d), capi.ptr(zc), k, 10, None))
+    torch.cuda.synchronize()
+    assert np.array_equal(n_dev.cpu().numpy(), ref)
+
+
 @pytest.mark.parametrize("tile", [0, 2])
 def test_gwn_grid_lists_bit_identical(tile):
     # dwg_gwn_grid with lists records the grid's interaction lists on its first
