@@ -403,7 +403,7 @@ struct TopK {
 // gives up after kDeepBudget child visits (returns false): a query that far
 // from its neighbours is finished by a warp of k_knn_deep instead of holding
 // a thread (and its warp) for the length of a long walk.
-constexpr int kDeepBudget = 1024;
+constexpr int kDeepBudget = 512;
 template <int KMAX>
 __device__ __forceinline__ bool knn_pyramid(const KnnArgs& a, float qx, float qy, float qz, int cx, int cy, int cz,
                                             TopK<KMAX>& top) {

@@ -242,6 +242,12 @@ __device__ __forceinline__ double warp_max_d(double v) {
     return v;
 }
 
+// nodes with more points than this are summed by a whole block
+// (k_centres_big): a warp alone on the root would walk every point twice
+// while the rest of the GPU idles
+constexpr int kBigNode = 4096;
+constexpr int kBigThreads = 512;
+
 __global__ void k_centres(const int4* __restrict__ info, const float4* __restrict__ pa, int M,
                           double* __restrict__ cm_d, double* __restrict__ r_d, const int* __restrict__ lvl_of,
                           float4* __restrict__ node_a, float* __restrict__ node_r) {
@@ -250,6 +256,7 @@ __global__ void k_centres(const int4* __restrict__ info, const float4* __restric
     const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
     for (long long v = warp; v < M; v += nwarps) {
         int4 iv = info[v];
+        if (iv.y > kBigNode) continue;
         double sa = 0, sx = 0, sy = 0, sz = 0;
         for (int j = iv.x + lane; j < iv.x + iv.y; j += 32) {
             float4 p = pa[j];
@@ -286,6 +293,69 @@ __global__ void k_centres(const int4* __restrict__ info, const float4* __restric
                                     (iv.w & kLeafFlag) ? __int_as_float(iv.y) : 0.f);
             node_r[p] = (float)rm;
         }
+    }
+}
+
+// the nodes above kBigNode points, a block each: thread-strided partial
+// sums, then a fixed tree in shared memory (deterministic), the centre, and
+// the radius as the maximum over the points (exact whatever the order)
+__global__ void __launch_bounds__(kBigThreads) k_centres_big(const int4* __restrict__ info,
+                                                            const float4* __restrict__ pa, int M,
+                                                            double* __restrict__ cm_d, double* __restrict__ r_d,
+                                                            const int* __restrict__ lvl_of,
+                                                            float4* __restrict__ node_a, float* __restrict__ node_r) {
+    __shared__ double red[4][kBigThreads];
+    const int tid = threadIdx.x;
+    for (long long v = blockIdx.x; v < M; v += gridDim.x) {
+        const int4 iv = info[v];
+        if (iv.y <= kBigNode) continue;  // the same node for the whole block
+        double sa = 0, sx = 0, sy = 0, sz = 0;
+        for (int j = iv.x + tid; j < iv.x + iv.y; j += kBigThreads) {
+            const float4 p = pa[j];
+            const double a = p.w;
+            sa += a;
+            sx += a * (double)p.x;
+            sy += a * (double)p.y;
+            sz += a * (double)p.z;
+        }
+        red[0][tid] = sa;
+        red[1][tid] = sx;
+        red[2][tid] = sy;
+        red[3][tid] = sz;
+        __syncthreads();
+        for (int h = kBigThreads / 2; h > 0; h >>= 1) {
+            if (tid < h)
+                for (int q = 0; q < 4; ++q) red[q][tid] += red[q][tid + h];
+            __syncthreads();
+        }
+        sa = red[0][0];
+        const double cx = sa > 0 ? red[1][0] / sa : 0.0, cy = sa > 0 ? red[2][0] / sa : 0.0,
+                     cz = sa > 0 ? red[3][0] / sa : 0.0;
+        __syncthreads();  // every thread has read the sums before the radii reuse the buffer
+        double rm = 0;
+        for (int j = iv.x + tid; j < iv.x + iv.y; j += kBigThreads) {
+            const float4 p = pa[j];
+            const double dx = (double)p.x - cx, dy = (double)p.y - cy, dz = (double)p.z - cz;
+            rm = fmax(rm, sqrt(dx * dx + dy * dy + dz * dz));
+        }
+        red[0][tid] = rm;
+        __syncthreads();
+        for (int h = kBigThreads / 2; h > 0; h >>= 1) {
+            if (tid < h) red[0][tid] = fmax(red[0][tid], red[0][tid + h]);
+            __syncthreads();
+        }
+        if (tid == 0) {
+            rm = red[0][0];
+            cm_d[v * 3] = cx;
+            cm_d[v * 3 + 1] = cy;
+            cm_d[v * 3 + 2] = cz;
+            r_d[v] = rm;
+            const int p = lvl_of[v];
+            node_a[p] = make_float4((float)cx, (float)cy, (float)cz,
+                                    (iv.w & kLeafFlag) ? __int_as_float(iv.y) : 0.f);
+            node_r[p] = (float)rm;
+        }
+        __syncthreads();  // the buffer is free for the next node
     }
 }
 
@@ -680,6 +750,11 @@ int octree_update_centres(Octree& t, cudaStream_t s) {
     k_centres<<<moment_blocks(t.M), 256, 0, s>>>(t.info.ptr, t.pa.ptr, t.M, t.cm_d.ptr, t.r_d.ptr, t.lvl_of.ptr,
                                                   t.node_a.ptr, t.node_r.ptr);
     DWG_CHECK_LAUNCH();
+    if (t.n > kBigNode) {
+        k_centres_big<<<num_sms() * 2, kBigThreads, 0, s>>>(t.info.ptr, t.pa.ptr, t.M, t.cm_d.ptr, t.r_d.ptr,
+                                                            t.lvl_of.ptr, t.node_a.ptr, t.node_r.ptr);
+        DWG_CHECK_LAUNCH();
+    }
     t.thr_beta = -1.f;
     return DWG_OK;
 }
