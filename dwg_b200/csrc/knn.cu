@@ -223,6 +223,7 @@ struct KnnArgs {
     // queries whose pyramid walk ran past kDeepBudget visits go on this list
     // (null: no budget) and are finished by k_knn_deep
     int* __restrict__ deep;
+    float* __restrict__ deep_bound;  // per entry: a bound on the k-th squared distance (its walk's k-th key)
     int* __restrict__ deep_count;
     // occupancy pyramid
     const unsigned char* __restrict__ occ;
@@ -403,7 +404,7 @@ struct TopK {
 // gives up after kDeepBudget child visits (returns false): a query that far
 // from its neighbours is finished by a warp of k_knn_deep instead of holding
 // a thread (and its warp) for the length of a long walk.
-constexpr int kDeepBudget = 512;
+constexpr int kDeepBudget = 128;
 template <int KMAX>
 __device__ __forceinline__ bool knn_pyramid(const KnnArgs& a, float qx, float qy, float qz, int cx, int cy, int cz,
                                             TopK<KMAX>& top) {
@@ -569,7 +570,12 @@ __global__ void __launch_bounds__(128, KMAX <= 10 ? 4 : 1) k_knn_thread(KnnArgs 
             }
             if (r == 1 && a.levels > 0) {
                 if (!knn_pyramid<KMAX>(a, qx, qy, qz, cx, cy, cz, top)) {
-                    a.deep[atomicAdd(a.deep_count, 1)] = (int)qi;  // at most once per query: the list holds nq
+                    // at most once per query: the list holds nq.  The walk's
+                    // current maximum (its k-th key, or the initial bound)
+                    // bounds the k-th squared distance
+                    const int pos = atomicAdd(a.deep_count, 1);
+                    a.deep[pos] = (int)qi;
+                    a.deep_bound[pos] = top.mx == NONE ? INFINITY : __uint_as_float((unsigned)(top.mx >> 32));
                     deferred = true;
                 }
                 break;
@@ -1172,6 +1178,7 @@ __device__ __forceinline__ int pack3(int i, int j, int k) { return i | (j << 10)
 
 template <int KMAX>
 __global__ void __launch_bounds__(kDeepWarps * 32) k_knn_deep(KnnArgs a, const int* __restrict__ list,
+                                                             const float* __restrict__ bound,
                                                              const int* __restrict__ count, int* __restrict__ work) {
     __shared__ int fco[kDeepWarps][2][kDeepNodes];
     __shared__ unsigned char fmk[kDeepWarps][2][kDeepNodes];
@@ -1201,7 +1208,7 @@ __global__ void __launch_bounds__(kDeepWarps * 32) k_knn_deep(KnnArgs a, const i
             curm[0] = a.occ[a.loff[lvl]];
         }
         int nf = 1;
-        float U2 = INFINITY;
+        float U2 = bound[j];  // from the per-thread walk
         __syncwarp();
         while (lvl > 0) {
             const int nl = lvl - 1;
@@ -1360,6 +1367,7 @@ static int cells_launch(const KnnIndex& ix, const KnnArgs& a, long long nq, cuda
     f.nq_dev_i32 = ix.c_misc.ptr + 2;
     f.kb = ix.kb.ptr;
     f.deep = ix.levels > 0 ? ix.c_deep.ptr : nullptr;
+    f.deep_bound = ix.c_deep_bound.ptr;
     f.deep_count = ix.c_misc.ptr + 3;
     DWG_TRY(knn_launch<KMAX>(f, nq, s));
     if (f.deep) {
@@ -1368,8 +1376,8 @@ static int cells_launch(const KnnIndex& ix, const KnnArgs& a, long long nq, cuda
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dbps, k_knn_deep<KMAX>, kDeepWarps * 32, 0);
             if (dbps <= 0) dbps = 1;
         }
-        k_knn_deep<KMAX><<<(unsigned)(num_sms() * dbps), kDeepWarps * 32, 0, s>>>(f, ix.c_deep.ptr, ix.c_misc.ptr + 3,
-                                                                              ix.c_misc.ptr + 4);
+        k_knn_deep<KMAX><<<(unsigned)(num_sms() * dbps), kDeepWarps * 32, 0, s>>>(
+            f, ix.c_deep.ptr, ix.c_deep_bound.ptr, ix.c_misc.ptr + 3, ix.c_misc.ptr + 4);
         DWG_CHECK_LAUNCH();
     }
     return DWG_OK;
@@ -1389,6 +1397,7 @@ static int knn_query_cells(const KnnIndex& ix, const KnnArgs& a0, long long nq, 
     DWG_TRY(ix.q_order.reserve(nq));
     DWG_TRY(ix.c_fb.reserve(nq));
     DWG_TRY(ix.c_deep.reserve(nq));
+    DWG_TRY(ix.c_deep_bound.reserve(nq));
     DWG_CHECK_CUDA(cudaMemsetAsync(ix.c_count.ptr, 0, sizeof(int) * (ncell + 1), s));
     DWG_CHECK_CUDA(cudaMemsetAsync(ix.c_m.ptr, 0, sizeof(unsigned int) * ncell, s));
     DWG_CHECK_CUDA(cudaMemsetAsync(ix.c_misc.ptr, 0, sizeof(int) * 8, s));
@@ -1526,6 +1535,7 @@ int knn_query(const KnnIndex& ix, const KnnQuery& q, int k, int* out, cudaStream
     a.order = nullptr;
     a.kb = nullptr;
     a.deep = nullptr;
+    a.deep_bound = nullptr;
     a.deep_count = nullptr;
     if (k <= kKnnBoundK && !q.exclude && ix.n >= kKnnBoundK && q.use_cells) return knn_query_cells(ix, a, q.nq, s);
     // bucket the queries spatially (counting sort on device counts, no host sync)

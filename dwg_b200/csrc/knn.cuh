@@ -32,6 +32,7 @@ struct KnnIndex {
     // workspace of the cell-grouped queries
     mutable DevBuf<int> c_count, c_start, c_fill, c_active, c_misc, c_fb, c_deep;
     mutable DevBuf<unsigned int> c_m;
+    mutable DevBuf<float> c_deep_bound;
     mutable DevBuf<unsigned char> c_scratch;
     // query bucketing workspace (grown on demand; not thread safe)
     int morton_shift = 0;
