@@ -598,9 +598,9 @@ def knn_roofline(a, lib, capi, turbo, torch, dev, P, peaks):
 
 
 def _traffic(kernel, workload):
-    """DRAM bytes of one launch from the committed ncu summary (profiles/traffic.json)."""
+    """DRAM bytes of one launch from the committed ncu figures (profiles/traffic.txt, JSON)."""
     try:
-        d = json.load(open(os.path.join(ROOT, "profiles", "traffic.json")))
+        d = json.load(open(os.path.join(ROOT, "profiles", "traffic.txt")))
         return d.get(f"{kernel}:{workload}")
     except Exception:
         return None
@@ -916,7 +916,9 @@ class CpuWindingPath:
         frac_leaf = (self.a.iters * len(self.L) + len(self.P)) / self.queries
         nl = int(round(n * frac_leaf))
         ng = n - nl
-        sel = rng.choice(self.ng, ng, replace=False)
+        # distinct samples while the grid has enough of them (a small grid
+        # timed for seconds needs more queries than it has samples)
+        sel = rng.choice(self.ng, ng, replace=ng > self.ng)
         x, y, z = sel % self.res[0], (sel // self.res[0]) % self.res[1], sel // (self.res[0] * self.res[1])
         Qg = (self.org[None, :] + np.stack([x, y, z], 1).astype(np.float32) * self.h).astype(np.float32)
         Ql = self.L[rng.choice(len(self.L), nl, replace=True)]
