@@ -399,6 +399,9 @@ def _pipeline_tensors(lib, capi, torch, dev, h, what, shape):
     t = torch.empty(shape, dtype=torch.float32, device=dev)
     nbytes = int(np.prod(shape)) * 4
     cudart_copy(torch, t, ptr.value, nbytes)
+    # the copy runs on torch's stream; it must be done before the pipeline
+    # is destroyed (dwg_pipeline_destroy waits for the pipeline's stream only)
+    torch.cuda.current_stream(dev).synchronize()
     return t
 
 

@@ -8,7 +8,12 @@ Batch::~Batch() {
     if (s) cudaStreamSynchronize(s);
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (graph) cudaGraphDestroy(graph);
-    clouds.clear();  // each pipeline synchronises its own stream
+    {
+        // each pipeline synchronises its own stream first, and the batch's
+        // stream (its persistent launch reads every cloud) was drained above
+        FreeScope idle(nullptr, true);
+        clouds.clear();
+    }
     for (cudaEvent_t e : ev_done)
         if (e) cudaEventDestroy(e);
     if (ev_fork) cudaEventDestroy(ev_fork);

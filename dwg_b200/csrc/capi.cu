@@ -144,24 +144,52 @@ void graph_exec_release(cudaGraphExec_t e) {
     else cudaGraphExecDestroy(e);
 }
 
+namespace {
+struct FreeState {
+    bool active = false, idle = false;
+    cudaStream_t stream = nullptr;
+};
+thread_local FreeState t_free;
+std::mutex g_side_mu;
+cudaStream_t g_side[64] = {};  // per device: allocations and idle releases (never destroyed)
+
+cudaStream_t side_stream(int dev) {
+    if (dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(g_side_mu);
+    if (!g_side[dev]) {
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+            unsigned long long keep = ~0ull;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        cudaStream_t s = nullptr;
+        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return nullptr;
+        g_side[dev] = s;
+    }
+    return g_side[dev];
+}
+}  // namespace
+
+FreeScope::FreeScope(cudaStream_t stream, bool idle)
+    : prev_active_(t_free.active), prev_idle_(t_free.idle), prev_stream_(t_free.stream) {
+    t_free.active = true;
+    t_free.idle = idle;
+    t_free.stream = stream;
+}
+
+FreeScope::~FreeScope() {
+    t_free.active = prev_active_;
+    t_free.idle = prev_idle_;
+    t_free.stream = prev_stream_;
+}
+
 int pool_alloc(void** p, size_t bytes) {
-    static std::mutex mu;
-    static bool configured[64] = {false};
     int dev = 0;
     DWG_CHECK_CUDA(cudaGetDevice(&dev));
-    if (dev >= 0 && dev < 64) {
-        std::lock_guard<std::mutex> lock(mu);
-        if (!configured[dev]) {
-            cudaMemPool_t pool;
-            if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
-                unsigned long long keep = ~0ull;
-                cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
-            }
-            configured[dev] = true;
-        }
-    }
-    cudaError_t e = cudaMallocAsync(p, bytes, cudaStreamLegacy);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
+    cudaStream_t side = side_stream(dev);
+    DWG_REQUIRE(side, "device allocation: no allocation stream on device %d", dev);
+    cudaError_t e = cudaMallocAsync(p, bytes, side);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(side);  // complete before any stream uses it
     if (e != cudaSuccess) {
         // the code is returned; a failed allocation must not stay behind as
         // the runtime's last error (callers that fall back would meet it at
@@ -181,14 +209,24 @@ int pool_alloc(void** p, size_t bytes) {
 
 void pool_free(void* p) {
     if (!p) return;
+    int dev = -1;
     {
         std::lock_guard<std::mutex> lock(g_mem_mu);
         auto it = g_sizes.find(p);
         if (it != g_sizes.end()) {
-            const int dev = it->second.first;
+            dev = it->second.first;
             g_live[dev] -= std::min(g_live[dev], it->second.second);
             g_sizes.erase(it);
         }
+    }
+    if (t_free.active) {
+        cudaStream_t s = t_free.stream;
+        if (t_free.idle) {
+            if (dev < 0) cudaGetDevice(&dev);
+            s = side_stream(dev);
+        }
+        if (s && cudaFreeAsync(p, s) == cudaSuccess) return;
+        cudaGetLastError();
     }
     // wait for every stream's use of the block, then return it to the pool
     if (cudaDeviceSynchronize() != cudaSuccess) return;
@@ -714,7 +752,12 @@ int dwg_slab_range(int samples, int rank, int world, int* z0, int* nz) {
 }
 
 int dwg_pipeline_destroy(dwg_pipeline* p) {
-    if (p) cudaStreamSynchronize(p->p.s);
+    if (!p) return DWG_OK;
+    // the pipeline's stream is the only one its buffers were used on (the
+    // caller's stream joins it through events): once it is drained, every
+    // block goes back to the pool at once, without waiting on other streams
+    cudaStreamSynchronize(p->p.s);
+    FreeScope idle(nullptr, true);
     delete p;
     return DWG_OK;
 }

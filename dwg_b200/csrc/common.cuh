@@ -49,10 +49,24 @@ struct Status {
 // Device memory comes from the device's stream-ordered pool, which keeps
 // freed blocks mapped (release threshold = unlimited): building and tearing
 // down a pipeline per cloud then costs no page-table work.  An allocation is
-// made complete before it is returned; a release first waits for the device
-// to finish its work, like cudaFree.
+// made on a private stream of the device and is complete when it is returned
+// (no other stream waits).  A release made while a FreeScope of the calling
+// thread is alive is ordered on the scope's stream (after the work queued
+// there: the owner's stream, which is the only one that used the block) or,
+// for an idle scope, made at once (the owner's stream was drained); any
+// other release first waits for the device to finish its work, like cudaFree.
 int pool_alloc(void** p, size_t bytes);
 void pool_free(void* p);
+struct FreeScope {
+    FreeScope(cudaStream_t stream, bool idle);
+    ~FreeScope();
+    FreeScope(const FreeScope&) = delete;
+    FreeScope& operator=(const FreeScope&) = delete;
+
+  private:
+    bool prev_active_, prev_idle_;
+    cudaStream_t prev_stream_;
+};
 
 // Device memory this library can still count on: the free memory it first
 // saw on the current device (plus what it held then) minus the blocks it

@@ -327,6 +327,9 @@ int Pipeline::setup(const float* points_dev, const float* normals_dev, int n_poi
     s = stream_acquire();
     ev = event_acquire();
     DWG_REQUIRE(s && ev, "pipeline: no CUDA stream or event");
+    // setup's work, its temporaries included, runs on s alone: releases are
+    // ordered there instead of waiting for the device
+    FreeScope on_s(s, false);
     DWG_TRY(join_in());
     n = n_points;
     DWG_TRY(mc_upload_tables());

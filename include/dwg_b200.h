@@ -347,6 +347,10 @@ typedef struct dwg_pipeline dwg_pipeline;
 /* points_dev: n normalised points; normals_dev: input normals (in_normal 0/1) or NULL. */
 int dwg_pipeline_create(const float* points_dev, const float* normals_dev, int n,
                         const dwg_params* params, void* stream, dwg_pipeline** out);
+/* Waits for the pipeline's own stream and returns its device memory to the
+ * pool without waiting for other streams: work that the caller queued on
+ * another stream and that reads the pipeline's buffers (dwg_pipeline_device_ptr)
+ * must be finished first. */
 int dwg_pipeline_destroy(dwg_pipeline* p);
 /* run `n_iters` diffusion iterations (continuing the count) */
 int dwg_pipeline_iterate(dwg_pipeline* p, int n_iters);
