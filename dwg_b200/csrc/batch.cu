@@ -2,6 +2,8 @@
 // with the grid sums of all clouds in one persistent launch.
 #include "batch.cuh"
 
+#include <algorithm>
+
 namespace dwg {
 
 Batch::~Batch() {
@@ -57,15 +59,60 @@ int Batch::setup(const float* const* points_dev, const int* counts, int n, const
             set_error("batch: cloud %d: %s", i, msg.c_str());
             return st;
         }
-        // the batch's persistent launch sums the grids of later iterations;
-        // lists of the first iteration's grid would only hold memory
-        clouds.back()->p.grid_batched = true;
     }
-    // the grid sums of every cloud, one work list
-    std::vector<GwnBatchItem> items((size_t)n);
+    // what the clouds' grid lists and weights may not take: room for the
+    // workspaces that the first iteration sizes (marching cubes, kNN, repair)
+    reserve = device_free_bytes() / 4;
+    return join_out();
+}
+
+// Weight slots for the clouds' kept grid lists, then the grid sums of the
+// clouds without lists as one work list.  Every listed cloud with weights
+// wanted gets one slot (its most used sigma) in order of list size while
+// they fit above the reserve, then a second, and so on: the weights save
+// about the same time per byte in every cloud, the first slot the most.
+int Batch::prepare_grid() {
+    const int n = (int)clouds.size();
+    std::vector<int> order;
+    for (int i = 0; i < n; ++i) {
+        const GwnList& L = clouds[i]->p.glist;
+        if (clouds[i]->p.prm.grid_lists && L.valid && !L.too_big && L.wslots > 0 && L.wstate.ptr && L.entries)
+            order.push_back(i);
+    }
+    std::sort(order.begin(), order.end(),
+              [&](int a, int b) { return clouds[a]->p.glist.entries > clouds[b]->p.glist.entries; });
+    std::vector<int> slots((size_t)n, 0);
+    {
+        // the first iteration has sized every workspace the graph uses; the
+        // final pass runs after the lists are released (finalize), so a
+        // small margin stays free
+        const size_t keep = std::min(reserve, (size_t)4 << 30);
+        const size_t fr = device_free_bytes();
+        size_t room = fr > keep ? fr - keep : 0;
+        for (int pass = 1; pass <= kGwnWeightSlots; ++pass)
+            for (int i : order) {
+                const GwnList& L = clouds[i]->p.glist;
+                const size_t need = (size_t)L.entries * 32 * sizeof(float2);  // one grid slot
+                if (L.wslots < pass || slots[i] != pass - 1 || need > room) continue;
+                slots[i] = pass;
+                room -= need;
+            }
+    }
+    for (int i : order)
+        if (slots[i] > 0 && gwn_list_add_weights(clouds[i]->p.glist, slots[i], clouds[i]->p.s) != DWG_OK) {
+            cudaGetLastError();  // no room after all: this cloud replays its lists without weights
+        }
+    std::vector<GwnBatchItem> items;
+    listed.assign((size_t)n, 0);
     for (int i = 0; i < n; ++i) {
         Pipeline& p = clouds[i]->p;
-        GwnBatchItem& it = items[i];
+        if (p.prm.grid_lists && p.glist.valid && !p.glist.too_big) {
+            listed[i] = 1;
+            continue;
+        }
+        p.grid_batched = true;
+        items.emplace_back();
+        GwnBatchItem& it = items.back();
         it.tree = &p.t2;
         for (int d = 0; d < 3; ++d) {
             it.res[d] = p.gres[d];
@@ -77,8 +124,9 @@ int Batch::setup(const float* const* points_dev, const int* counts, int n, const
         it.sigma_dev = p.cur_sigma.ptr;
         it.beta = p.prm.beta;
     }
-    DWG_TRY(gwn_batch_prepare(grid, items.data(), n, clouds[0]->p.gwn_params(), s));
-    return join_out();
+    unlisted = (int)items.size();
+    if (unlisted) DWG_TRY(gwn_batch_prepare(grid, items.data(), unlisted, clouds[0]->p.gwn_params(), s));
+    return DWG_OK;
 }
 
 // one iteration of every cloud on the batch stream, as one capture
@@ -94,13 +142,18 @@ int Batch::capture() {
         Pipeline& p = clouds[i]->p;
         if (cudaStreamWaitEvent(p.s, ev_fork, 0) != cudaSuccess) fail(DWG_ERR_CUDA);
         if (st == DWG_OK) fail(p.iterate_pre());
+        if (listed[i]) {  // the whole iteration in this cloud's branch
+            if (st == DWG_OK) fail(p.iterate_grid());
+            if (st == DWG_OK) fail(p.iterate_post());
+        }
         if (st == DWG_OK && cudaEventRecord(ev_done[i], p.s) != cudaSuccess) fail(DWG_ERR_CUDA);
         if (st == DWG_OK && cudaStreamWaitEvent(s, ev_done[i], 0) != cudaSuccess) fail(DWG_ERR_CUDA);
     }
-    if (st == DWG_OK) fail(gwn_batch_launch(grid, s));
+    if (st == DWG_OK && unlisted) fail(gwn_batch_launch(grid, s));
     if (st == DWG_OK && cudaEventRecord(ev_mid, s) != cudaSuccess) fail(DWG_ERR_CUDA);
     for (int i = 0; i < n && st == DWG_OK; ++i) {
         Pipeline& p = clouds[i]->p;
+        if (listed[i]) continue;
         if (cudaStreamWaitEvent(p.s, ev_mid, 0) != cudaSuccess) fail(DWG_ERR_CUDA);
         if (st == DWG_OK) fail(p.iterate_post());
         if (st == DWG_OK && cudaEventRecord(ev_done[n + i], p.s) != cudaSuccess) fail(DWG_ERR_CUDA);
@@ -138,9 +191,23 @@ int Batch::iterate(int n_iters) {
         if (iter == 0) {
             // the first iteration runs eagerly per cloud: it sizes the
             // workspaces (marching cubes, kNN, repair) that the graph reuses
-            for (auto& c : clouds) DWG_TRY(c->p.iterate(1));
+            // and records each cloud's grid lists (16 bytes per entry) within
+            // what is left above the reserve, without weights: those (256
+            // bytes per entry and sigma) are handed out once every cloud's
+            // lists are known (prepare_grid)
+            for (auto& c : clouds) {
+                Pipeline& p = c->p;
+                const size_t fr = device_free_bytes();
+                const size_t room = fr > reserve ? fr - reserve : 0;
+                p.glist_budget = std::min(p.glist_budget, room > 0 ? room : (size_t)1);
+                p.glist.wmax = 1;
+                DWG_TRY(p.iterate(1));
+            }
         } else {
-            if (!graph_exec) DWG_TRY(capture());
+            if (!graph_exec) {
+                DWG_TRY(prepare_grid());
+                DWG_TRY(capture());
+            }
             DWG_CHECK_CUDA(cudaGraphLaunch(graph_exec, s));
             for (auto& c : clouds) ++c->p.iter;
         }
@@ -152,6 +219,13 @@ int Batch::iterate(int n_iters) {
 int Batch::finalize() {
     DWG_REQUIRE(!finalized, "batch: already finalized");
     DWG_TRY(join_in());
+    // the iteration grids' lists and weights are done with: their memory
+    // goes to the final passes (the batch stream waited for every cloud)
+    DWG_CHECK_CUDA(cudaStreamSynchronize(s));
+    {
+        FreeScope idle(nullptr, true);
+        for (auto& c : clouds) gwn_list_release(c->p.glist);
+    }
     for (auto& c : clouds) DWG_TRY(c->p.finalize());
     finalized = true;
     return join_out();

@@ -1,10 +1,12 @@
 // batch.cuh -- many clouds of uneven size reconstructed together.
 //
-// Every cloud is a Pipeline with its own stream.  One iteration of all
-// clouds is captured once as a single CUDA graph: the per-cloud phases
-// before the grid sums run as parallel branches, the grid sums of all clouds
-// are one persistent launch (a shared work list of bricks, so small clouds do
-// not leave SMs idle), and the per-cloud phases after it branch out again.
+// Every cloud is a Pipeline with its own stream.  In the first iteration
+// (eager, cloud by cloud) each cloud records its grid's interaction lists and
+// keeps screening weights while they fit a memory budget shared by the
+// batch.  Every later iteration of all clouds is one CUDA graph: a cloud with
+// kept lists runs its whole iteration as its own branch; the grids of the
+// others are summed by one persistent launch (a shared work list of bricks,
+// so small clouds do not leave SMs idle) between their branches' phases.
 #pragma once
 
 #include <memory>
@@ -25,6 +27,9 @@ struct Batch {
     cudaEvent_t ev_fork = nullptr, ev_mid = nullptr;
     std::vector<cudaEvent_t> ev_done;
     GwnBatch grid;
+    std::vector<char> listed;       // per cloud: its grid replays kept lists in its own branch
+    int unlisted = 0;               // clouds summed by the persistent launch
+    size_t reserve = 0;             // bytes kept free for the first iteration's workspaces
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     int iter = 0;
@@ -39,6 +44,7 @@ struct Batch {
 
   private:
     int capture();
+    int prepare_grid();
     int join_in();
     int join_out();
 };

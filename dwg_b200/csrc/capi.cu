@@ -790,6 +790,10 @@ int dwg_pipeline_size(dwg_pipeline* p, const char* what, long long* value) {
             *value = (long long)q.gres[0] * q.gres[1] * q.gnz;
         else if (!strcmp(what, "final_grid"))
             *value = (long long)q.fres[0] * q.fres[1] * q.fnz;
+        else if (!strcmp(what, "grid_list_entries"))  // 0: the grid is traversed
+            *value = q.glist.valid && !q.glist.too_big ? (long long)q.glist.entries : 0;
+        else if (!strcmp(what, "grid_weight_slots"))
+            *value = q.glist.valid && !q.glist.too_big ? q.glist.nslots : 0;
         else if (!strcmp(what, "triangles")) {
             DWG_REQUIRE(q.finalized, "pipeline_size: not finalized");
             unsigned long long T = 0;

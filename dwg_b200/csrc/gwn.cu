@@ -1045,7 +1045,7 @@ __global__ void k_weight_select(GwnWeightState* __restrict__ w, const float* __r
             return;
         }
     for (int c = 0; c < w->nslots; ++c)
-        if (!w->valid[c]) {
+        if (!w->valid[c] && (w->pref[c] == 0.f || w->pref[c] == sg)) {
             w->mode = 1;
             w->slot = c;
             w->sigma[c] = sg;
@@ -1055,7 +1055,19 @@ __global__ void k_weight_select(GwnWeightState* __restrict__ w, const float* __r
         }
 }
 
-__global__ void k_weight_reset(GwnWeightState* __restrict__ w, int nslots) {
+struct SlotPrefs {
+    float s[kGwnWeightSlots];
+};
+// the sigmas that L's slots are kept for: L.pref when it holds fewer slots
+// than it wants, else none (every sigma of the schedule has a slot)
+static SlotPrefs slot_prefs(const GwnList& L, int nslots) {
+    SlotPrefs p{};
+    if (nslots < L.wslots)
+        for (int c = 0; c < nslots && c < kGwnWeightSlots; ++c) p.s[c] = L.pref[c];
+    return p;
+}
+
+__global__ void k_weight_reset(GwnWeightState* __restrict__ w, int nslots, SlotPrefs pref) {
     w->mode = 0;
     w->slot = 0;
     w->nslots = nslots;
@@ -1064,13 +1076,44 @@ __global__ void k_weight_reset(GwnWeightState* __restrict__ w, int nslots) {
         w->valid[c] = 0;
         w->sigma[c] = 0.f;
         w->screen[c] = 0.f;
+        w->pref[c] = pref.s[c];
         w->node_terms[c] = 0;
     }
 }
 
 int gwn_list_drop_weights(GwnList& L, cudaStream_t s) {
     if (!L.valid || L.nslots <= 0) return DWG_OK;
-    k_weight_reset<<<1, 1, 0, s>>>(L.wstate.ptr, L.nslots);
+    k_weight_reset<<<1, 1, 0, s>>>(L.wstate.ptr, L.nslots, slot_prefs(L, L.nslots));
+    DWG_CHECK_LAUNCH();
+    return DWG_OK;
+}
+
+void gwn_list_release(GwnList& L) {
+    L.count.release();
+    L.off.release();
+    L.ent.release();
+    L.scratch.release();
+    L.w.release();
+    L.wstate.release();
+    L.nslots = 0;
+    L.entries = 0;
+    L.ngroups = 0;
+    L.valid = false;
+    L.too_big = false;
+}
+
+int gwn_list_add_weights(GwnList& L, int nslots, cudaStream_t s) {
+    // the weight state exists when the recording could keep weights (screened
+    // terms with the MUFU approximations)
+    DWG_REQUIRE(L.valid && !L.too_big && L.wstate.ptr && L.nslots == 0 && L.entries > 0,
+                "gwn lists: no recorded list without weights to add them to");
+    DWG_REQUIRE(nslots >= 1 && nslots <= L.wslots && nslots <= kGwnWeightSlots, "gwn lists: bad slot count %d",
+                nslots);
+    const size_t wb = L.grid ? sizeof(WeightOf<nq_of<true>()>::T) : sizeof(WeightOf<nq_of<false>()>::T);
+    const size_t per = (size_t)L.entries * 32 * wb;
+    DWG_TRY(L.w.reserve(((size_t)nslots * per + sizeof(float2) - 1) / sizeof(float2)));
+    L.nslots = nslots;
+    k_weight_reset<<<1, 1, 0, s>>>(L.wstate.ptr, nslots, slot_prefs(L, nslots));
     DWG_CHECK_LAUNCH();
     return DWG_OK;
 }
@@ -1308,13 +1351,17 @@ static int listed_shape(GwnArgs& a, GwnList& L, const Octree& t, cudaStream_t s,
         if (SCREENED && PREC != 2 && L.wslots > 0 && total > 0) {
             const size_t fr = device_free_bytes();
             const unsigned long long per = total * 32ull * sizeof(W);
-            const unsigned long long cap = std::min<unsigned long long>(fr / 3, 64ull << 30);
+            unsigned long long cap = std::min<unsigned long long>(fr / 3, 64ull << 30);
+            if (L.wmax) {  // a budget shared with the entries just kept
+                const unsigned long long lb = total * (unsigned long long)sizeof(int4);
+                cap = std::min<unsigned long long>(cap, L.wmax > lb ? L.wmax - lb : 0);
+            }
             int n = (int)std::min<unsigned long long>((unsigned long long)std::min(L.wslots, kGwnWeightSlots),
                                                       cap / per);
             if (n > 0 && L.w.reserve(((size_t)n * per + sizeof(float2) - 1) / sizeof(float2)) != DWG_OK) n = 0;
             L.nslots = n;
             DWG_TRY(L.wstate.reserve(1));
-            k_weight_reset<<<1, 1, 0, s>>>(L.wstate.ptr, n);
+            k_weight_reset<<<1, 1, 0, s>>>(L.wstate.ptr, n, slot_prefs(L, n));
             DWG_CHECK_LAUNCH();
         }
     }

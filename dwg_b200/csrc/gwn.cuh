@@ -46,6 +46,7 @@ struct GwnWeightState {
     int mode, slot, nslots, pad;  // mode: 0 evaluate, 1 evaluate and write slot, 2 read slot
     int valid[kGwnWeightSlots];
     float sigma[kGwnWeightSlots], screen[kGwnWeightSlots];
+    float pref[kGwnWeightSlots];  // the sigma a free slot is kept for (0: any)
     unsigned long long node_terms[kGwnWeightSlots];  // node terms a slot stands for
     unsigned int work;                               // group counter of the reading launch
 };
@@ -59,6 +60,10 @@ struct GwnList {
     DevBuf<GwnWeightState> wstate;
     int wslots = 0;                      // weight slots wanted (0: none)
     int nslots = 0;                      // weight slots held
+    size_t wmax = 0;                     // entries and weights together at most this many bytes (0: no such cap)
+    // when fewer slots are held than wanted, slot c is kept for sigma pref[c]
+    // (the owner's most used sigmas first; 0: the first sigma that comes)
+    float pref[kGwnWeightSlots] = {0.f, 0.f, 0.f, 0.f};
     long long ngroups = 0;
     unsigned long long entries = 0;
     // what the recorded decisions depend on besides the tree's centres (the
@@ -100,6 +105,11 @@ int gwn_eval_thread(const Octree& t, const GwnQuery& q, const dwg_gwn_params& p,
 // depend on the points' screening radii when use_radii is set, so new radii
 // make them stale.  Stream-ordered, no host synchronisation.
 int gwn_list_drop_weights(GwnList& L, cudaStream_t s);
+// weight slots for a kept list that holds none yet (nslots <= L.wslots),
+// written by the next replay of each sigma; DWG_ERR_NOMEM leaves it without
+int gwn_list_add_weights(GwnList& L, int nslots, cudaStream_t s);
+// give back a list's memory (entries and weights); the next call records again
+void gwn_list_release(GwnList& L);
 
 // Grid sums of many clouds in one persistent launch (screened).  prepare()
 // records the clouds' octrees, grids and outputs once (host work, not

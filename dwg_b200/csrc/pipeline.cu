@@ -14,6 +14,7 @@
 #include <cub/cub.cuh>
 
 #include <cmath>
+#include <utility>
 #include <vector>
 
 #include "pipeline.cuh"
@@ -464,6 +465,31 @@ int Pipeline::setup(const float* points_dev, const float* normals_dev, int n_poi
         // the grid's interaction lists may take a quarter of the free memory, at most 16 GB
         const size_t fr = device_free_bytes();
         glist_budget = fr / 4 < ((size_t)16 << 30) ? fr / 4 : ((size_t)16 << 30);
+    }
+    {
+        // when fewer weight slots fit than the schedule has sigmas, the slots
+        // go to the sigmas of the most iterations (lambda before the first
+        // iterations' 20)
+        const int iters = p.total_iter > 0 ? p.total_iter : 1;
+        float sg[kGwnWeightSlots] = {};
+        int cnt[kGwnWeightSlots] = {}, m = 0;
+        for (int t = 0; t < iters; ++t) {
+            const float v = sigma_at(t, p.lambda);
+            int c = 0;
+            while (c < m && sg[c] != v) ++c;
+            if (c == m) {
+                if (m == kGwnWeightSlots) continue;
+                sg[m++] = v;
+            }
+            ++cnt[c];
+        }
+        for (int a = 0; a < m; ++a)  // most iterations first, first use breaking ties
+            for (int b = a + 1; b < m; ++b)
+                if (cnt[b] > cnt[a]) {
+                    std::swap(cnt[a], cnt[b]);
+                    std::swap(sg[a], sg[b]);
+                }
+        for (int c = 0; c < kGwnWeightSlots; ++c) glist.pref[c] = llist.pref[c] = c < m ? sg[c] : 0.f;
     }
     DWG_TRY(wleaf.reserve(L));
     DWG_TRY(cent.reserve((size_t)cap * 3));

@@ -357,7 +357,10 @@ int dwg_pipeline_iterate(dwg_pipeline* p, int n_iters);
 /* final meshing pass; the mesh stays on the device */
 int dwg_pipeline_finalize(dwg_pipeline* p);
 /* sizes: "leaves", "points", "triangles" (final mesh; synchronises),
- * "iterations", "grid" (iteration grid samples), "final_grid" */
+ * "iterations", "grid" (iteration grid samples), "final_grid",
+ * "grid_list_entries" (interaction-list entries the iteration grid keeps,
+ * 16 bytes each; 0 when it is traversed) and "grid_weight_slots" (sigmas
+ * whose screening weights it keeps, 256 bytes per entry each) */
 int dwg_pipeline_size(dwg_pipeline* p, const char* what, long long* value);
 /* copy a result to host memory (synchronises): "leaf_pos" [L*3], "leaf_nrm" [L*3],
  * "point_nrm" [N*3], "tris" [T*9], "iso" [iters], "tri_count" [iters] (int64),
