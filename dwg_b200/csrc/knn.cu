@@ -53,36 +53,51 @@ __global__ void k_knn_scatter(const float* __restrict__ P, int n, const int* __r
 // The occupancy pyramid: node c of level l >= 1 holds the mask of its
 // occupied children (bit t for the child 2 * (i, j, k) + (t & 1, t >> 1 & 1,
 // t >> 2), cells at level 1), so a node is occupied iff its byte is nonzero
-// and a walk skips empty children without loading them.
-// level 1 from the cell ranges
-__global__ void k_pyr_first(const int* __restrict__ cell_start, int G0, int G1, int G2, int D0, int D1, int D2,
-                            unsigned char* __restrict__ occ) {
-    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (c >= (long long)D0 * D1 * D2) return;
-    const int i = (int)(c % D0), j = (int)((c / D0) % D1), k = (int)(c / ((long long)D0 * D1));
-    unsigned char o = 0;
-    for (int t = 0; t < 8; ++t) {
-        const int x = 2 * i + (t & 1), y = 2 * j + ((t >> 1) & 1), z = 2 * k + (t >> 2);
-        if (x >= G0 || y >= G1 || z >= G2) continue;
-        const long long f = x + (long long)G0 * (y + (long long)G1 * z);
-        o |= (unsigned char)((cell_start[f + 1] > cell_start[f] ? 1 : 0) << t);
-    }
-    occ[c] = o;
+// and a walk skips empty children without loading them.  One launch fills
+// every level of a zeroed pyramid: a thread per level-1 node ORs in its mask,
+// then climbs while it is the first child to make its parent nonzero (the old
+// byte of the OR), so every occupied node's bit reaches its parent once and
+// no thread waits for another.
+struct PyrDims {
+    int levels;
+    int ldim[KnnIndex::kMaxLevels][3];
+    long long loff[KnnIndex::kMaxLevels];
+};
+
+// OR v into the byte at p (a 32-bit atomic on its word; the buffer is padded
+// to whole words); returns the byte before
+__device__ __forceinline__ unsigned atomic_or_byte(unsigned char* p, unsigned v) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    unsigned* w = reinterpret_cast<unsigned*>(a & ~(uintptr_t)3);
+    const unsigned sh = (unsigned)(a & 3) * 8u;
+    return (atomicOr(w, v << sh) >> sh) & 0xffu;
 }
 
-// level l >= 2 from level l - 1
-__global__ void k_pyr_next(const unsigned char* __restrict__ prev, int P0, int P1, int P2, int D0, int D1, int D2,
+__global__ void k_pyr_fill(const int* __restrict__ cell_start, int G0, int G1, int G2, PyrDims pd,
                            unsigned char* __restrict__ occ) {
-    long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (c >= (long long)D0 * D1 * D2) return;
-    const int i = (int)(c % D0), j = (int)((c / D0) % D1), k = (int)(c / ((long long)D0 * D1));
-    unsigned char o = 0;
-    for (int t = 0; t < 8; ++t) {
-        const int x = 2 * i + (t & 1), y = 2 * j + ((t >> 1) & 1), z = 2 * k + (t >> 2);
-        if (x >= P0 || y >= P1 || z >= P2) continue;
-        o |= (unsigned char)((prev[x + (long long)P0 * (y + (long long)P1 * z)] != 0 ? 1 : 0) << t);
+    const int D0 = pd.ldim[1][0], D1 = pd.ldim[1][1], D2 = pd.ldim[1][2];
+    const long long m = (long long)D0 * D1 * D2;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < m;
+         c += (long long)gridDim.x * blockDim.x) {
+        int i = (int)(c % D0), j = (int)((c / D0) % D1), k = (int)(c / ((long long)D0 * D1));
+        unsigned o = 0;
+        for (int t = 0; t < 8; ++t) {
+            const int x = 2 * i + (t & 1), y = 2 * j + ((t >> 1) & 1), z = 2 * k + (t >> 2);
+            if (x >= G0 || y >= G1 || z >= G2) continue;
+            const long long f = x + (long long)G0 * (y + (long long)G1 * z);
+            o |= (cell_start[f + 1] > cell_start[f] ? 1u : 0u) << t;
+        }
+        if (!o) continue;
+        atomic_or_byte(occ + pd.loff[1] + c, o);
+        for (int l = 2; l <= pd.levels; ++l) {
+            const int t = (i & 1) | ((j & 1) << 1) | ((k & 1) << 2);
+            i >>= 1;
+            j >>= 1;
+            k >>= 1;
+            const long long p = pd.loff[l] + i + (long long)pd.ldim[l][0] * (j + (long long)pd.ldim[l][1] * k);
+            if (atomic_or_byte(occ + p, 1u << t) != 0) break;  // the parent was occupied: its ancestors know
+        }
     }
-    occ[c] = o;
 }
 
 // level dimensions and offsets of the occupancy pyramid of ix's grid
@@ -105,24 +120,27 @@ static int pyramid_dims(KnnIndex& ix) {
         total += (long long)d[0] * d[1] * d[2];
     }
     ix.levels = L;
-    if (L > 0) DWG_TRY(ix.occ.reserve(total));
+    // padded to whole 32-bit words (the fill ORs bytes through word atomics)
+    if (L > 0) DWG_TRY(ix.occ.reserve((size_t)total + 4));
     return DWG_OK;
 }
 
-// the occupancy flags of every level from ix.cell_start (stream-ordered)
+// the occupancy masks of every level from ix.cell_start (stream-ordered)
 static int pyramid_fill(KnnIndex& ix, cudaStream_t s) {
-    for (int l = 1; l <= ix.levels; ++l) {
-        const int* D = ix.ldim[l];
-        const long long m = (long long)D[0] * D[1] * D[2];
-        if (l == 1)
-            k_pyr_first<<<div_up(m, 256), 256, 0, s>>>(ix.cell_start.ptr, ix.G[0], ix.G[1], ix.G[2], D[0], D[1], D[2],
-                                                       ix.occ.ptr + ix.loff[1]);
-        else
-            k_pyr_next<<<div_up(m, 256), 256, 0, s>>>(ix.occ.ptr + ix.loff[l - 1], ix.ldim[l - 1][0],
-                                                      ix.ldim[l - 1][1], ix.ldim[l - 1][2], D[0], D[1], D[2],
-                                                      ix.occ.ptr + ix.loff[l]);
-        DWG_CHECK_LAUNCH();
+    if (ix.levels < 1) return DWG_OK;
+    PyrDims pd;
+    pd.levels = ix.levels;
+    for (int l = 0; l < KnnIndex::kMaxLevels; ++l) {
+        pd.loff[l] = ix.loff[l];
+        for (int d = 0; d < 3; ++d) pd.ldim[l][d] = ix.ldim[l][d];
     }
+    DWG_CHECK_CUDA(cudaMemsetAsync(ix.occ.ptr, 0, ix.occ.n, s));
+    const long long m = (long long)ix.ldim[1][0] * ix.ldim[1][1] * ix.ldim[1][2];
+    long long blocks = div_up(m, 256);
+    const long long cap = (long long)num_sms() * 8;
+    if (blocks > cap) blocks = cap;
+    k_pyr_fill<<<(unsigned)blocks, 256, 0, s>>>(ix.cell_start.ptr, ix.G[0], ix.G[1], ix.G[2], pd, ix.occ.ptr);
+    DWG_CHECK_LAUNCH();
     return DWG_OK;
 }
 
