@@ -733,9 +733,9 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_replay(GwnArgs a) {
 // one lane hands each 16-entry chunk to the bulk-copy (TMA) engine as two
 // 1-D copies (the chunk's weights and its entries are contiguous in global
 // memory) that complete on the ring slot's mbarrier, two 256-thread blocks
-// per SM (104 KB of ring each).  Points (short lists): 8-entry chunks moved
+// per SM (106 KB of ring and records each).  Points (short lists): 8-entry chunks moved
 // by cp.async in 16-byte pieces spread over the lanes, four blocks per SM
-// (52 KB of ring each), which measured faster there.  The node terms a slot
+// (53 KB of ring and records each), which measured faster there.  The node terms a slot
 // stands for were counted when it was written.
 template <bool GRID>
 struct WreadCfg {
@@ -772,9 +772,12 @@ __device__ __noinline__ LeafSum<Acc> leaf_points_ool(const float4* __restrict__ 
     return r;
 }
 constexpr int kWreadRing = 3;
+// per warp: the ring's weights (3 slots x C entries x 32 lanes x 8 bytes),
+// its entries (16 bytes each), then the node records of the chunk being
+// summed (two float4 per entry)
 template <bool GRID>
 constexpr int wread_warp_bytes() {
-    return kWreadRing * WreadCfg<GRID>::kChunk * (32 * 8 + 16);
+    return kWreadRing * WreadCfg<GRID>::kChunk * (32 * 8 + 16) + 2 * WreadCfg<GRID>::kChunk * 16;
 }
 template <bool GRID>
 constexpr int wread_smem() {
@@ -885,6 +888,7 @@ __global__ void __launch_bounds__(kGwnWarps * 32, WreadCfg<GRID>::kBlocks) k_gwn
     const int warp = threadIdx.x >> 5;
     W* const wring = reinterpret_cast<W*>(wread_smem + warp * WB);
     int4* const lring = reinterpret_cast<int4*>(wread_smem + warp * WB + kWreadRing * C * 32 * 8);
+    float4* const rec = reinterpret_cast<float4*>(wread_smem + warp * WB + kWreadRing * C * (32 * 8 + 16));
     unsigned long long* const bar = wbar[warp];
     if (BULK && lane == 0) {
         for (int r = 0; r < kWreadRing; ++r) mbar_init(bar + r);
@@ -943,19 +947,21 @@ __global__ void __launch_bounds__(kGwnWarps * 32, WreadCfg<GRID>::kBlocks) k_gwn
             const int4* lc = lring + r * C;
             const unsigned long long first = e0 + c * C;
             const int cnt = e1 - first < (unsigned long long)C ? (int)(e1 - first) : C;
-            // a full chunk of node entries (the common case): unrolled, the
-            // next entry's node record loaded while this one is summed
+            // a full chunk of node entries (the common case): the C node
+            // records are loaded at once, a lane each, into shared memory
+            // (one round trip per chunk rather than one per entry), then
+            // summed unrolled
             const bool full = cnt == C && __ballot_sync(FULL, lc[lane & (C - 1)].x < 0) == 0;
             if (full) {
-                float4 na = a.node_a[lc[0].x], nb = a.node_b[lc[0].x];
+                if (lane < C) {
+                    const int x = lc[lane].x;
+                    rec[lane] = a.node_a[x];
+                    rec[C + lane] = a.node_b[x];
+                }
+                __syncwarp();  // the warp's previous readers passed the chunk-end __syncwarp
 #pragma unroll
                 for (int k = 0; k < C; ++k) {
-                    float4 na_n = na, nb_n = nb;
-                    if (k + 1 < C) {
-                        const int xn = lc[k + 1].x;
-                        na_n = a.node_a[xn];
-                        nb_n = a.node_b[xn];
-                    }
+                    const float4 na = rec[k], nb = rec[C + k];
                     float wu[NQ];
                     WT::unpack(wc[k * 32 + lane], wu);
 #pragma unroll
@@ -964,8 +970,6 @@ __global__ void __launch_bounds__(kGwnWarps * 32, WreadCfg<GRID>::kBlocks) k_gwn
                                                   __fsub_rn(na.z, qz[u]));
                         sum[u] += (Acc)__fmul_rn(wu[u], dd);
                     }
-                    na = na_n;
-                    nb = nb_n;
                 }
             }
             for (int k = full ? C : 0; k < cnt; ++k) {
