@@ -728,21 +728,15 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_replay(GwnArgs a) {
 // sample, g (A n).(p - q), with the replay's roundings, so the sums keep
 // their bits.  The kernel is bound by the weights' HBM stream (256 bytes per
 // entry for grid cells, 128 for points), so each warp streams its group's
-// entries and weights through a ring of kWreadRing chunks in shared memory,
-// two chunks in flight while it sums the third.  Grid cells (long lists):
-// one lane hands each 16-entry chunk to the bulk-copy (TMA) engine as two
-// 1-D copies (the chunk's weights and its entries are contiguous in global
-// memory) that complete on the ring slot's mbarrier, two 256-thread blocks
-// per SM (106 KB of ring and records each).  Points (short lists): 8-entry chunks moved
-// by cp.async in 16-byte pieces spread over the lanes, four blocks per SM
-// (53 KB of ring and records each), which measured faster there.  The node terms a slot
-// stands for were counted when it was written.
-template <bool GRID>
-struct WreadCfg {
-    static constexpr int kChunk = GRID ? 16 : 8;
-    static constexpr bool kBulk = GRID;
-    static constexpr int kBlocks = GRID ? 2 : 4;
-};
+// entries and weights through a ring of kWreadRing chunks of kWreadChunk
+// entries in shared memory, two chunks in flight while it sums the third:
+// one lane hands each chunk to the bulk-copy (TMA) engine as two 1-D copies
+// (the chunk's weights and its entries are contiguous in global memory) that
+// complete on the ring slot's mbarrier; two 256-thread blocks per SM (106 KB
+// of ring and node records each).  The node terms a slot stands for were
+// counted when it was written.
+constexpr int kWreadChunk = 16;
+constexpr int kWreadBlocks = 2;
 
 // the points of a multi-point leaf for one sample, out of line (rare in the
 // read path; its registers stay off the loop).  The running sum goes in and
@@ -772,17 +766,11 @@ __device__ __noinline__ LeafSum<Acc> leaf_points_ool(const float4* __restrict__ 
     return r;
 }
 constexpr int kWreadRing = 3;
-// per warp: the ring's weights (3 slots x C entries x 32 lanes x 8 bytes),
-// its entries (16 bytes each), then the node records of the chunk being
-// summed (two float4 per entry)
-template <bool GRID>
-constexpr int wread_warp_bytes() {
-    return kWreadRing * WreadCfg<GRID>::kChunk * (32 * 8 + 16) + 2 * WreadCfg<GRID>::kChunk * 16;
-}
-template <bool GRID>
-constexpr int wread_smem() {
-    return kGwnWarps * wread_warp_bytes<GRID>();
-}
+// per warp: the ring's weights (3 slots x C entries x 32 lanes x 8 bytes;
+// point weights use half), its entries (16 bytes each), then the node
+// records of the chunk being summed (two float4 per entry)
+constexpr int kWreadWarpBytes = kWreadRing * kWreadChunk * (32 * 8 + 16) + 2 * kWreadChunk * 16;
+constexpr int kWreadSmem = kGwnWarps * kWreadWarpBytes;
 
 // 1-D bulk copies global -> shared (the TMA engine), completed on an
 // mbarrier: the barrier's phase completes when its one arrival (with the
@@ -817,64 +805,36 @@ __device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsign
                  : "memory");
 }
 
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(smem)), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
-
 // chunk c of entries [e0, e1) into a ring slot: its weights (32 per entry)
-// and its entries.  Returns whether the chunk exists (was issued).
-// Bulk: two bulk copies issued by lane 0 onto the slot's barrier; sizes are
-// multiples of 16 bytes and both sources 16-byte aligned (256-byte aligned
-// buffers, whole entries of 16 bytes and of 32 weights).  The warp's reads of
-// the slot's previous chunk are complete (the caller's __syncwarp); the proxy
-// fence orders them before the copy's writes.
-// cp.async: 16-byte pieces spread over the lanes (entries on lanes 0..C-1),
-// one commit group per chunk, empty past the end.
-template <bool BULK, int C, typename W>
+// and its entries, two bulk copies issued by lane 0 onto the slot's barrier.
+// Returns whether the chunk exists (was issued).  Sizes are multiples of 16
+// bytes and both sources 16-byte aligned (256-byte aligned buffers, whole
+// entries of 16 bytes and of 32 weights).  The warp's reads of the slot's
+// previous chunk are complete (the caller's __syncwarp); the proxy fence
+// orders them before the copy's writes.
+template <typename W>
 __device__ __forceinline__ bool wread_issue(const W* __restrict__ wp, const int4* __restrict__ list,
                                             unsigned long long e0, unsigned long long e1, unsigned long long c,
                                             W* ws, int4* ls, unsigned long long* bar, int lane) {
-    const unsigned long long first = e0 + c * C;
-    if constexpr (BULK) {
-        if (first >= e1) return false;
-        if (lane == 0) {
-            const unsigned cnt = (unsigned)(e1 - first < (unsigned long long)C ? e1 - first : C);
-            const unsigned wb = cnt * 32u * (unsigned)sizeof(W), lb = cnt * 16u;
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            mbar_expect_tx(bar, wb + lb);
-            bulk_copy_g2s(ws, wp + first * 32, wb, bar);
-            bulk_copy_g2s(ls, list + first, lb, bar);
-        }
-        return true;
-    } else {
-        const bool have = first < e1;
-        if (have) {
-            constexpr int kPerEntry = 32 * (int)sizeof(W) / 16;  // 16-byte pieces per entry
-            constexpr int kPieces = C * kPerEntry;
-            static_assert(kPieces % 32 == 0 && C <= 32, "pieces spread evenly over the lanes");
-#pragma unroll
-            for (int r = 0; r < kPieces / 32; ++r) {
-                const int piece = lane + 32 * r;
-                const int k = piece / kPerEntry;  // entry of the piece
-                if (first + k < e1)
-                    cp_async16(reinterpret_cast<char*>(ws) + piece * 16,
-                               reinterpret_cast<const char*>(wp + first * 32) + piece * 16);
-            }
-            if (lane < C && first + lane < e1) cp_async16(ls + lane, list + first + lane);
-        }
-        cp_async_commit();
-        return have;
+    const unsigned long long first = e0 + c * kWreadChunk;
+    if (first >= e1) return false;
+    if (lane == 0) {
+        const unsigned cnt =
+            (unsigned)(e1 - first < (unsigned long long)kWreadChunk ? e1 - first : kWreadChunk);
+        const unsigned wb = cnt * 32u * (unsigned)sizeof(W), lb = cnt * 16u;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(bar, wb + lb);
+        bulk_copy_g2s(ws, wp + first * 32, wb, bar);
+        bulk_copy_g2s(ls, list + first, lb, bar);
     }
+    return true;
 }
 
 template <bool GRID, bool SCREENED, int PREC, int SHAPE>
-__global__ void __launch_bounds__(kGwnWarps * 32, WreadCfg<GRID>::kBlocks) k_gwn_wread(GwnArgs a) {
+__global__ void __launch_bounds__(kGwnWarps * 32, kWreadBlocks) k_gwn_wread(GwnArgs a) {
     constexpr int NQ = nq_of<GRID>();
-    constexpr int C = WreadCfg<GRID>::kChunk;
-    constexpr bool BULK = WreadCfg<GRID>::kBulk;
-    constexpr int WB = wread_warp_bytes<GRID>();
+    constexpr int C = kWreadChunk;
+    constexpr int WB = kWreadWarpBytes;
     using WT = WeightOf<NQ>;
     using W = typename WT::T;
     static_assert(sizeof(W) <= 8, "ring sized for two samples per lane");
@@ -890,13 +850,13 @@ __global__ void __launch_bounds__(kGwnWarps * 32, WreadCfg<GRID>::kBlocks) k_gwn
     int4* const lring = reinterpret_cast<int4*>(wread_smem + warp * WB + kWreadRing * C * 32 * 8);
     float4* const rec = reinterpret_cast<float4*>(wread_smem + warp * WB + kWreadRing * C * (32 * 8 + 16));
     unsigned long long* const bar = wbar[warp];
-    if (BULK && lane == 0) {
+    if (lane == 0) {
         for (int r = 0; r < kWreadRing; ++r) mbar_init(bar + r);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncwarp();
-    unsigned parity = 0;  // bulk: bit r, the phase of ring slot r to wait for next
-    unsigned pend = 0;    // bulk: bit r, slot r has a chunk in flight
+    unsigned parity = 0;  // bit r: the phase of ring slot r to wait for next
+    unsigned pend = 0;    // bit r: slot r has a chunk in flight
     bool wait_ok = true;  // warp-uniform
     const W* const wp = reinterpret_cast<const W*>(a.wbuf) + (size_t)wst->slot * a.wstride;
     if (a.terms_total && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(a.terms_total, wst->node_terms[wst->slot]);
@@ -926,23 +886,18 @@ __global__ void __launch_bounds__(kGwnWarps * 32, WreadCfg<GRID>::kBlocks) k_gwn
         // chunk is waited for before its group ends, so no copy spans groups)
 #pragma unroll
         for (int c = 0; c < kWreadRing - 1; ++c)
-            if (wread_issue<BULK, C>(wp, a.list, e0, e1, c, wring + c * C * 32, lring + c * C, bar + c, lane))
+            if (wread_issue(wp, a.list, e0, e1, c, wring + c * C * 32, lring + c * C, bar + c, lane))
                 pend |= 1u << c;
         for (unsigned long long c = 0; c < nchunk; ++c) {
             const int r = (int)(c % kWreadRing);
-            // chunk c has landed (c + 1 may be in flight)
-            if constexpr (BULK) {
-                // every lane waits (each needs the copy's bytes visible); after
-                // a wait that gave up, the slot's contents are unknown: the
-                // warp reads none of them (its entries index node records)
-                wait_ok = __all_sync(FULL, mbar_wait(bar + r, (parity >> r) & 1u));
-                if (!wait_ok) break;
-                parity ^= 1u << r;
-                pend &= ~(1u << r);
-            } else {
-                cp_async_wait_1();
-                __syncwarp();
-            }
+            // chunk c has landed (c + 1 may be in flight): every lane waits
+            // (each needs the copy's bytes visible); after a wait that gave
+            // up, the slot's contents are unknown: the warp reads none of
+            // them (its entries index node records)
+            wait_ok = __all_sync(FULL, mbar_wait(bar + r, (parity >> r) & 1u));
+            if (!wait_ok) break;
+            parity ^= 1u << r;
+            pend &= ~(1u << r);
             const W* wc = wring + r * C * 32;
             const int4* lc = lring + r * C;
             const unsigned long long first = e0 + c * C;
@@ -1003,7 +958,7 @@ __global__ void __launch_bounds__(kGwnWarps * 32, WreadCfg<GRID>::kBlocks) k_gwn
             __syncwarp();  // ring slot (c + 2) % 3 = (c - 1) % 3 was read in the previous pass
             const unsigned long long nx = c + kWreadRing - 1;
             const int rn = (int)(nx % kWreadRing);
-            if (wread_issue<BULK, C>(wp, a.list, e0, e1, nx, wring + rn * C * 32, lring + rn * C, bar + rn, lane))
+            if (wread_issue(wp, a.list, e0, e1, nx, wring + rn * C * 32, lring + rn * C, bar + rn, lane))
                 pend |= 1u << rn;
         }
 #pragma unroll
@@ -1013,17 +968,13 @@ __global__ void __launch_bounds__(kGwnWarps * 32, WreadCfg<GRID>::kBlocks) k_gwn
         }
         if (!wait_ok) break;
     }
-    if constexpr (BULK) {
-        // every issued chunk was waited for, so no copy outlives the block,
-        // unless a wait gave up (a copy that never landed): that is reported,
-        // and the chunks still in flight get one more bounded wait each
-        if (!wait_ok) {
-            if (lane == 0) atomicOr(&a.work[1], 16u);
-            for (int r = 0; r < kWreadRing; ++r)
-                if ((pend >> r) & 1u) (void)mbar_wait(bar + r, (parity >> r) & 1u);
-        }
-    } else {
-        asm volatile("cp.async.wait_all;" ::: "memory");  // no copy outlives the block
+    // every issued chunk was waited for, so no copy outlives the block,
+    // unless a wait gave up (a copy that never landed): that is reported,
+    // and the chunks still in flight get one more bounded wait each
+    if (!wait_ok) {
+        if (lane == 0) atomicOr(&a.work[1], 16u);
+        for (int r = 0; r < kWreadRing; ++r)
+            if ((pend >> r) & 1u) (void)mbar_wait(bar + r, (parity >> r) & 1u);
     }
     if (a.terms_total) {
         for (int o = 16; o > 0; o >>= 1) my_terms += __shfl_down_sync(FULL, my_terms, o);
@@ -1390,14 +1341,14 @@ static int listed_shape(GwnArgs& a, GwnList& L, const Octree& t, cudaStream_t s,
         int& bpw = bpw_dev[dev];
         if (!bpw) {
             DWG_CHECK_CUDA(cudaFuncSetAttribute(k_gwn_wread<GRID, SCREENED, PREC, SHAPE>,
-                                                cudaFuncAttributeMaxDynamicSharedMemorySize, wread_smem<GRID>()));
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, kWreadSmem));
             DWG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpw, k_gwn_wread<GRID, SCREENED, PREC, SHAPE>,
-                                                                         kGwnWarps * 32, wread_smem<GRID>()));
+                                                                         kGwnWarps * 32, kWreadSmem));
             if (bpw < 1) bpw = 1;
         }
         const long long all = (long long)num_sms() * bpw;
         const unsigned gw = (unsigned)(a.ngroups < all * kGwnWarps ? (a.ngroups + kGwnWarps - 1) / kGwnWarps : all);
-        k_gwn_wread<GRID, SCREENED, PREC, SHAPE><<<gw, kGwnWarps * 32, wread_smem<GRID>(), s>>>(a);
+        k_gwn_wread<GRID, SCREENED, PREC, SHAPE><<<gw, kGwnWarps * 32, kWreadSmem, s>>>(a);
         DWG_CHECK_LAUNCH();
     }
     return DWG_OK;
