@@ -641,8 +641,11 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_replay(GwnArgs a) {
     using WT = WeightOf<NQ>;
     using W = typename WT::T;
     using Acc = typename AccType<PREC>::T;
+    __shared__ float4 rrec[kGwnWarps][64];  // per warp: the batch's node records (a, then b)
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
+    float4* const ra = rrec[threadIdx.x >> 5];
+    float4* const rb = ra + 32;
     const float sigma = a.sigma_dev ? *a.sigma_dev : a.sigma;
     const float sigma_l2e = sigma * 1.4426950408889634f;
     int wmode = 0;
@@ -671,10 +674,17 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_replay(GwnArgs a) {
         }
         const unsigned long long e0 = a.list_off[g], e1 = a.list_off[g + 1];
         // the group's entries arrive 32 at a time in one coalesced load and
-        // are handed out by shuffles (no dependent global load per entry)
+        // are handed out by shuffles; their node records are loaded at the
+        // same time, a lane each, into shared memory (no dependent global
+        // load per entry)
         for (unsigned long long base = e0; base < e1; base += 32) {
             const int4 mine = base + lane < e1 ? a.list[base + lane] : make_int4(0, 0, 0, 0);
             const int cnt = e1 - base < 32 ? (int)(e1 - base) : 32;
+            if (base + lane < e1 && mine.x >= 0) {
+                ra[lane] = a.node_a[mine.x];
+                rb[lane] = a.node_b[mine.x];
+            }
+            __syncwarp();
             for (int j = 0; j < cnt; ++j) {
                 const int ex = __shfl_sync(FULL, mine.x, j);
                 const unsigned m[3] = {(unsigned)__shfl_sync(FULL, mine.y, j), (unsigned)__shfl_sync(FULL, mine.z, j),
@@ -689,7 +699,7 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_replay(GwnArgs a) {
                             leaf_terms<SCREENED, PREC>(a, st, pc, qx[u], qy[u], qz[u], sigma, sigma_l2e, sum[u],
                                                        nt[u]);
                 } else {
-                    const float4 na = a.node_a[ex], nb = a.node_b[ex];
+                    const float4 na = ra[j], nb = rb[j];
                     float gw[NQ];
 #pragma unroll
                     for (int u = 0; u < NQ; ++u) {
@@ -705,6 +715,7 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_replay(GwnArgs a) {
                     if (wmode == 1) __stcs(wp + (base + j) * 32 + lane, WT::pack(gw));
                 }
             }
+            __syncwarp();  // the records are read before the next batch's overwrite them
         }
 #pragma unroll
         for (int u = 0; u < NQ; ++u) {
