@@ -412,7 +412,8 @@ __device__ __forceinline__ float node_term(const GwnArgs& a, const float4& na, c
 // traversal only.
 template <bool GRID, bool SCREENED, int PREC, int SHAPE, int NQ, int ORDER, int MODE = 0>
 __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g, int lane,
-                                         int* __restrict__ stk_node, unsigned* __restrict__ stk_mask, float sigma,
+                                         int* __restrict__ stk_node, unsigned* __restrict__ stk_mask,
+                                         unsigned* __restrict__ stk_meta, float4* __restrict__ crec, float sigma,
                                          float sigma_l2e) {
     const unsigned FULL = 0xffffffffu;
     bool valid[NQ];
@@ -521,6 +522,7 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
             if (sp < kGwnStack) {
                 if (lane == 0) {
                     stk_node[sp] = cidx;
+                    stk_meta[sp] = meta;  // its children's place: no load when it is popped
 #pragma unroll
                     for (int u = 0; u < NQ; ++u) stk_mask[sp * NQ + u] = nm[u];
                 }
@@ -543,6 +545,7 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
             for (int u = 0; u < NQ; ++u) m[u] = __ballot_sync(FULL, valid[u]);
             if (lane == 0) {
                 stk_node[0] = 0;
+                stk_meta[0] = rm;
 #pragma unroll
                 for (int u = 0; u < NQ; ++u) stk_mask[u] = m[u];
             }
@@ -553,6 +556,7 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
         __syncwarp();
         --sp;
         const int node = stk_node[sp];
+        const unsigned pm = stk_meta[sp];
         bool act[NQ];
 #pragma unroll
         for (int u = 0; u < NQ; ++u) act[u] = (stk_mask[sp * NQ + u] >> lane) & 1u;
@@ -561,7 +565,6 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
             if (lane == 0) atomicOr(&a.work[1], 2u);
             continue;
         }
-        const unsigned pm = (unsigned)__float_as_int(a.node_b[node].w);
         const int first = (int)(pm & kMetaIndex);
         const int nch = (int)((pm >> 28) & 7u) + 1;
         // structural guard: children come after the parent, inside the table
@@ -569,16 +572,17 @@ __device__ __forceinline__ int gwn_group(const GwnArgs& a, unsigned long long g,
             if (lane == 0) atomicOr(&a.work[1], 2u);
             continue;
         }
-        float4 na = a.node_a[first], nb = a.node_b[first];
+        // the (at most 8, contiguous) children's records at once, a lane
+        // each, into shared memory; the loop top's __syncwarp ordered the
+        // previous node's reads of them before these writes
+        if (lane < nch) {
+            crec[lane] = a.node_a[first + lane];
+            crec[8 + lane] = a.node_b[first + lane];
+        }
+        __syncwarp();
         for (int j = 0; j < nch; ++j) {
-            float4 na2, nb2;
-            if (j + 1 < nch) {  // load the next sibling while this one is evaluated
-                na2 = a.node_a[first + j + 1];
-                nb2 = a.node_b[first + j + 1];
-            }
+            const float4 na = crec[j], nb = crec[8 + j];
             child(first + j, na, nb, act, sp);
-            na = na2;
-            nb = nb2;
         }
     }
     if (MODE == 1) {
@@ -608,6 +612,8 @@ __global__ void __launch_bounds__(kGwnWarps * 32, (GRID && kNqGrid >= 4) ? 2 : 3
     constexpr int NQ = nq_of<GRID>();
     __shared__ int stk_node[kGwnWarps][kGwnStack];
     __shared__ unsigned stk_mask[kGwnWarps][kGwnStack * NQ];
+    __shared__ unsigned stk_meta[kGwnWarps][kGwnStack];
+    __shared__ float4 crec[kGwnWarps][16];
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
@@ -620,7 +626,7 @@ __global__ void __launch_bounds__(kGwnWarps * 32, (GRID && kNqGrid >= 4) ? 2 : 3
         g = __shfl_sync(FULL, g, 0);
         if ((long long)g >= a.ngroups) break;
         my_terms += (unsigned long long)gwn_group<GRID, SCREENED, PREC, SHAPE, NQ, ORDER, MODE>(
-            a, g, lane, stk_node[w], stk_mask[w], sigma, sigma_l2e);
+            a, g, lane, stk_node[w], stk_mask[w], stk_meta[w], crec[w], sigma, sigma_l2e);
     }
     if (a.terms_total) {
         for (int o = 16; o > 0; o >>= 1) my_terms += __shfl_down_sync(FULL, my_terms, o);
@@ -1093,6 +1099,8 @@ __global__ void __launch_bounds__(kGwnWarps * 32, kNqGrid >= 4 ? 2 : 3)
                 unsigned long long* __restrict__ work) {
     __shared__ int stk_node[kGwnWarps][kGwnStack];
     __shared__ unsigned stk_mask[kGwnWarps][kGwnStack * kNqGrid];
+    __shared__ unsigned stk_meta[kGwnWarps][kGwnStack];
+    __shared__ float4 crec[kGwnWarps][16];
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
@@ -1111,7 +1119,8 @@ __global__ void __launch_bounds__(kGwnWarps * 32, kNqGrid >= 4 ? 2 : 3)
         const GwnArgs& a = table[lo];
         const float sigma = a.sigma_dev ? *a.sigma_dev : a.sigma;
         int nt = gwn_group<true, SCREENED, PREC, SHAPE, kNqGrid, 0>(a, g - prefix[lo], lane, stk_node[w], stk_mask[w],
-                                                                sigma, sigma * 1.4426950408889634f);
+                                                                stk_meta[w], crec[w], sigma,
+                                                                sigma * 1.4426950408889634f);
         if (a.terms_total) {
             for (int o = 16; o > 0; o >>= 1) nt += __shfl_down_sync(FULL, nt, o);
             if (lane == 0 && nt) atomicAdd(a.terms_total, (unsigned long long)nt);
