@@ -713,7 +713,8 @@ __global__ void k_kb_local(KnnGrid g, const int* __restrict__ cell_start, const 
 // search, which needs no bound)
 constexpr int kKbActiveRadius = 3;
 __global__ void k_kb_active(KnnGrid g, const int* __restrict__ cell_start, const float4* __restrict__ pts,
-                            const int* __restrict__ active, const int* __restrict__ misc, float* __restrict__ kb) {
+                            const unsigned char* __restrict__ occ1, int D0, int D1, const int* __restrict__ active,
+                            const int* __restrict__ misc, float* __restrict__ kb) {
     const int na = misc[0];
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < na; t += gridDim.x * blockDim.x) {
         const int c = active[t];
@@ -736,6 +737,12 @@ __global__ void k_kb_active(KnnGrid g, const int* __restrict__ cell_start, const
                         if (max(abs(dx), max(abs(dy), abs(dz))) != r) continue;
                         const int xx = i + dx;
                         if (xx < 0 || xx >= g.G0) continue;
+                        // an empty cell by its bit in the level-1 child mask
+                        // (8 cells share a byte): no range loads
+                        if (occ1 && !((occ1[(xx >> 1) + (long long)D0 * ((yy >> 1) + (long long)D1 * (zz >> 1))] >>
+                                       ((xx & 1) | ((yy & 1) << 1) | ((zz & 1) << 2))) &
+                                      1))
+                            continue;
                         const int cc = xx + g.G0 * (yy + g.G1 * zz);
                         const int e = cell_start[cc + 1];
                         for (int s = cell_start[cc]; s < e; ++s) {
@@ -1438,8 +1445,9 @@ static int knn_query_cells(const KnnIndex& ix, const KnnArgs& a0, long long nq, 
     if (ix.kb_per_query) {
         DWG_TRY(ix.kb.reserve(ncell));
         KnnGrid g{ix.G[0], ix.G[1], ix.G[2], ix.lo[0], ix.lo[1], ix.lo[2], ix.h, ix.inv_h};
-        k_kb_active<<<num_sms() * 4, 128, 0, s>>>(g, ix.cell_start.ptr, ix.pts.ptr, ix.c_active.ptr, ix.c_misc.ptr,
-                                                  ix.kb.ptr);
+        const unsigned char* occ1 = ix.levels >= 1 ? ix.occ.ptr + ix.loff[1] : nullptr;
+        k_kb_active<<<num_sms() * 4, 128, 0, s>>>(g, ix.cell_start.ptr, ix.pts.ptr, occ1, ix.ldim[1][0],
+                                                  ix.ldim[1][1], ix.c_active.ptr, ix.c_misc.ptr, ix.kb.ptr);
     }
     k_cq_scatter<<<(unsigned)blocks, 256, 0, s>>>(a, ix.q_key.ptr, ix.c_fill.ptr, ix.q_order.ptr);
     DWG_CHECK_LAUNCH();
