@@ -340,18 +340,13 @@ def run_ours(a, rank, world, local_rank):
 
 
 def _dominant_roofline(census, roofs):
-    """The roofline whose kernel family takes the larger device time in one
-    step (kNN: k_knn_*, k_cq_*; GWN sums: k_gwn_*)."""
+    """The roofline of the kernel with the largest device time in one step
+    (the GWN weight read or the cell-grouped kNN, whichever leads)."""
     if not census:
         return "gwn"
-    ms = {"gwn": 0.0, "knn": 0.0}
-    for r in census.get("all", census.get("top", [])):
-        k = r["kernel"]
-        if "k_gwn" in k:
-            ms["gwn"] += r["ms"]
-        elif "k_knn" in k or "k_cq_" in k or "k_kb_" in k:
-            ms["knn"] += r["ms"]
-    best = max(ms, key=ms.get)
+    rows = census.get("all", census.get("top", []))
+    top = max(rows, key=lambda r: r["ms"]) if rows else None
+    best = "knn" if top and ("k_knn" in top["kernel"] or "k_cq_" in top["kernel"]) else "gwn"
     return best if "error" not in roofs.get(best, {"error": 1}) else "gwn"
 
 
