@@ -403,8 +403,12 @@ int dwg_slab_range(int samples, int rank, int world, int* z0, int* nz);
  * Batched reconstruction of many clouds (no counterpart in the reference,
  * which reconstructs one cloud per DWG_CUDA run).  Each cloud is a pipeline
  * with its own flags (params[i]; in_normal 3, one tile and one precision for
- * all); one iteration of all clouds is one CUDA graph whose grid sums run as
- * a single persistent launch over the bricks of every cloud.
+ * all); one iteration of all clouds is one CUDA graph.  The first iteration
+ * records every cloud's grid interaction lists while they fit (a quarter of
+ * the free memory stays reserved), then screening weights go to the largest
+ * lists first while they fit; clouds whose lists did not fit have their
+ * grids summed by a single persistent launch over their bricks.  The lists
+ * and weights are released by dwg_batch_finalize.
  * ------------------------------------------------------------------------ */
 typedef struct dwg_batch dwg_batch;
 int dwg_batch_create(const float* const* points_dev, const int* counts, int num_clouds, const dwg_params* params,
