@@ -13,6 +13,12 @@
  *   - Objects (octree, kNN index, pipeline) are owned by the library and freed
  *     with their *_destroy function.  A handle must not be used from two host
  *     threads at once.
+ *   - The library keeps per-device state for the life of the process, keyed by
+ *     the device ordinal: recycled streams, events and graph executables, one
+ *     allocation stream per device, the marching-cubes tables in constant
+ *     memory, kernel occupancy figures and the allocation-free scratch
+ *     address.  None of it survives a cudaDeviceReset: reset a device only
+ *     after the last call into the library.
  */
 #ifndef DWG_B200_H
 #define DWG_B200_H
