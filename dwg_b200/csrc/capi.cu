@@ -243,6 +243,11 @@ struct dwg_octree {
 };
 struct dwg_knn_index {
     KnnIndex ix;
+    // the zero repair's workspace: repairs on the same index start each
+    // flagged point's search from its neighbours of the previous repair
+    ZeroRepairWs zws;
+    DevBuf<float> zpos;  // the points in input order
+    bool zpos_ready = false;
 };
 struct dwg_batch {
     Batch b;
@@ -623,25 +628,30 @@ int dwg_zero_repair(dwg_knn_index* index, float* normals_dev, const unsigned cha
     API_GUARD({
         DWG_REQUIRE(index, "zero_repair: null index");
         (void)zero_count_dev;
-        ZeroRepairWs ws;
-        // positions in input order are needed for the query side
-        DevBuf<float> pos;
-        DWG_TRY(pos.reserve((size_t)index->ix.n * 3));
-        std::vector<float4> h(index->ix.n);
-        std::vector<float> hp((size_t)index->ix.n * 3);
-        DWG_CHECK_CUDA(cudaMemcpyAsync(h.data(), index->ix.pts.ptr, sizeof(float4) * index->ix.n,
-                                       cudaMemcpyDeviceToHost, S(stream)));
-        DWG_CHECK_CUDA(cudaStreamSynchronize(S(stream)));
-        for (int j = 0; j < index->ix.n; ++j) {
-            int id;
-            memcpy(&id, &h[j].w, 4);
-            hp[(size_t)id * 3] = h[j].x;
-            hp[(size_t)id * 3 + 1] = h[j].y;
-            hp[(size_t)id * 3 + 2] = h[j].z;
+        // positions in input order are needed for the query side (once per
+        // index: an index's points do not change)
+        DevBuf<float>& pos = index->zpos;
+        if (!index->zpos_ready) {
+            DWG_TRY(pos.reserve((size_t)index->ix.n * 3));
+            std::vector<float4> h(index->ix.n);
+            std::vector<float> hp((size_t)index->ix.n * 3);
+            DWG_CHECK_CUDA(cudaMemcpyAsync(h.data(), index->ix.pts.ptr, sizeof(float4) * index->ix.n,
+                                           cudaMemcpyDeviceToHost, S(stream)));
+            DWG_CHECK_CUDA(cudaStreamSynchronize(S(stream)));
+            for (int j = 0; j < index->ix.n; ++j) {
+                int id;
+                memcpy(&id, &h[j].w, 4);
+                hp[(size_t)id * 3] = h[j].x;
+                hp[(size_t)id * 3 + 1] = h[j].y;
+                hp[(size_t)id * 3 + 2] = h[j].z;
+            }
+            DWG_CHECK_CUDA(cudaMemcpyAsync(pos.ptr, hp.data(), sizeof(float) * hp.size(), cudaMemcpyHostToDevice,
+                                           S(stream)));
+            DWG_CHECK_CUDA(cudaStreamSynchronize(S(stream)));
+            index->zpos_ready = true;
         }
-        DWG_CHECK_CUDA(cudaMemcpyAsync(pos.ptr, hp.data(), sizeof(float) * hp.size(), cudaMemcpyHostToDevice,
-                                       S(stream)));
-        DWG_TRY(zero_repair(index->ix, pos.ptr, index->ix.n, normals_dev, is_zero_dev, k, min_zero, ws, S(stream)));
+        DWG_TRY(zero_repair(index->ix, pos.ptr, index->ix.n, normals_dev, is_zero_dev, k, min_zero, index->zws,
+                            S(stream)));
         DWG_CHECK_CUDA(cudaStreamSynchronize(S(stream)));
         return DWG_OK;
     })

@@ -243,12 +243,20 @@ struct KnnArgs {
     int* __restrict__ deep;
     float* __restrict__ deep_bound;  // per entry: a bound on the k-th squared distance (its walk's k-th key)
     int* __restrict__ deep_count;
+    // per query (null: none): a key above its k-th nearest key, ~0 for none
+    const unsigned long long* __restrict__ seed;
     // occupancy pyramid
     const unsigned char* __restrict__ occ;
     int levels;
     int ldim[KnnIndex::kMaxLevels][3];
     long long loff[KnnIndex::kMaxLevels];
 };
+
+// a seed key as a distance from the query that holds its k nearest: +inf
+// for none
+__device__ __forceinline__ float seed_radius(unsigned long long sd) {
+    return sd == ~0ull ? INFINITY : sqrtf(__uint_as_float((unsigned)(sd >> 32))) * 1.00002f + 1e-7f;
+}
 
 __device__ __forceinline__ long long knn_count(const KnnArgs& a) {
     long long nq = a.nq;
@@ -536,6 +544,10 @@ __global__ void __launch_bounds__(128, KMAX <= 10 ? 4 : 1) k_knn_thread(KnnArgs 
         } else {
             top.init(k);
         }
+        if (a.seed) {
+            const unsigned long long sd = a.seed[qi];
+            if (sd < top.mx) top.init_bound(k, sd);
+        }
         for (int r = 0;; ++r) {
             const float kd2 = top.mx == NONE ? INFINITY : __uint_as_float((unsigned)(top.mx >> 32)) * 1.00001f;
             for (int dz = -r; dz <= r; ++dz) {
@@ -710,14 +722,20 @@ __global__ void k_kb_local(KnnGrid g, const int* __restrict__ cell_start, const 
 // cell centre over the cells within Chebyshev radius r, r = 1, 2, 3 until 16
 // points are found (any 16 points bound the 16th nearest from above), +inf
 // when the radius-3 block holds fewer (those queries take the per-thread
-// search, which needs no bound)
+// search, which needs no bound) or when every query of the cell has a seed
 constexpr int kKbActiveRadius = 3;
 __global__ void k_kb_active(KnnGrid g, const int* __restrict__ cell_start, const float4* __restrict__ pts,
                             const unsigned char* __restrict__ occ1, int D0, int D1, const int* __restrict__ active,
-                            const int* __restrict__ misc, float* __restrict__ kb) {
+                            const int* __restrict__ misc, const unsigned int* __restrict__ sbits,
+                            float* __restrict__ kb) {
     const int na = misc[0];
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < na; t += gridDim.x * blockDim.x) {
         const int c = active[t];
+        // a cell whose queries all have seeds takes its radius from them
+        if (sbits && isfinite(__uint_as_float(sbits[c]))) {
+            kb[c] = INFINITY;
+            continue;
+        }
         const int i = c % g.G0, j = (c / g.G0) % g.G1, k = c / (g.G0 * g.G1);
         const float x = cell_mid(g.lo0, i, g.h), y = cell_mid(g.lo1, j, g.h), z = cell_mid(g.lo2, k, g.h);
         float d[kKnnBoundK];
@@ -849,7 +867,11 @@ static int build_kbound(const KnnIndex& ix, cudaStream_t s) {
 }
 
 // cell of every query, queries per cell, largest |q - x_c| per cell
-__global__ void k_cq_key(KnnArgs a, int* __restrict__ key, int* __restrict__ count, unsigned int* __restrict__ mbits) {
+// with seeds, sbits[c] gets the largest |q - x_c| + seed radius over the
+// cell's queries (+inf when one has no seed): the k nearest of every query of
+// the cell lie within it of the centre
+__global__ void k_cq_key(KnnArgs a, int* __restrict__ key, int* __restrict__ count, unsigned int* __restrict__ mbits,
+                         unsigned int* __restrict__ sbits) {
     if (a.gate_count && *a.gate_count <= a.gate_min) return;
     const long long nq = knn_count(a);
     for (long long qi = blockIdx.x * (long long)blockDim.x + threadIdx.x; qi < nq;
@@ -866,6 +888,7 @@ __global__ void k_cq_key(KnnArgs a, int* __restrict__ key, int* __restrict__ cou
         key[qi] = c;
         atomicAdd(&count[c], 1);
         atomicMax(&mbits[c], __float_as_uint(m));  // non-negative floats order as their bits
+        if (sbits) atomicMax(&sbits[c], __float_as_uint((m + seed_radius(a.seed[qi])) * 1.00002f));
     }
 }
 
@@ -910,6 +933,7 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
                                                              const int* __restrict__ cstart,
                                                              const int* __restrict__ ccount,
                                                              const unsigned int* __restrict__ mbits,
+                                                             const unsigned int* __restrict__ sbits,
                                                              const float* __restrict__ kb,
                                                              const int* __restrict__ order,
                                                              int* __restrict__ work, int* __restrict__ fb) {
@@ -934,6 +958,7 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
         const float x = cell_mid(a.g.lo0, ci, h), y = cell_mid(a.g.lo1, cj, h), z = cell_mid(a.g.lo2, ck, h);
         const int qs = cstart[c], qn = ccount[c];
         float R = (kb[c] + 2.0f * __uint_as_float(mbits[c])) * 1.00002f + 1e-6f * h;
+        if (sbits) R = fminf(R, __uint_as_float(sbits[c]) * 1.00002f + 1e-6f * h);
         bool ok = isfinite(R);
         int* cur = nodes[w][0];
         int nf = 0;
@@ -1036,7 +1061,11 @@ __global__ void __launch_bounds__(kCqWarps * 32) k_knn_cells(KnnArgs a, const in
             }
             const float ex = qx - x, ey = qy - y, ez = qz - z;
             const float rq = (kbc + sqrtf(ex * ex + ey * ey + ez * ez) * 1.00002f) * 1.00002f + 1e-7f;
-            const unsigned long long T = ((unsigned long long)__float_as_uint(rq * rq * 1.00002f) << 32) | 0xffffffffull;
+            unsigned long long T = ((unsigned long long)__float_as_uint(rq * rq * 1.00002f) << 32) | 0xffffffffull;
+            if (a.seed && has) {
+                const unsigned long long sd = a.seed[qi];
+                T = sd < T ? sd : T;
+            }
             TopK<KMAX> top;
             top.init_bound(k, T);
             int staged = 0;
@@ -1374,7 +1403,8 @@ static int knn_launch(const KnnArgs& a, long long nq, cudaStream_t s) {
 }
 
 template <int KMAX>
-static int cells_launch(const KnnIndex& ix, const KnnArgs& a, long long nq, cudaStream_t s) {
+static int cells_launch(const KnnIndex& ix, const KnnArgs& a, long long nq, const unsigned int* sbits,
+                        cudaStream_t s) {
     static int bps = 0;
     if (!bps) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_knn_cells<KMAX>, kCqWarps * 32, 0);
@@ -1382,7 +1412,7 @@ static int cells_launch(const KnnIndex& ix, const KnnArgs& a, long long nq, cuda
     }
     const long long grid = (long long)num_sms() * bps;
     k_knn_cells<KMAX><<<(unsigned)grid, kCqWarps * 32, 0, s>>>(
-        a, ix.c_active.ptr, ix.c_misc.ptr, ix.c_start.ptr, ix.c_count.ptr, ix.c_m.ptr, ix.kb.ptr, ix.q_order.ptr,
+        a, ix.c_active.ptr, ix.c_misc.ptr, ix.c_start.ptr, ix.c_count.ptr, ix.c_m.ptr, sbits, ix.kb.ptr, ix.q_order.ptr,
         ix.c_misc.ptr + 1, ix.c_fb.ptr);
     DWG_CHECK_LAUNCH();
     // the queries of cells whose candidate sets did not fit, per thread;
@@ -1425,13 +1455,19 @@ static int knn_query_cells(const KnnIndex& ix, const KnnArgs& a0, long long nq, 
     DWG_TRY(ix.c_deep_bound.reserve(nq));
     DWG_CHECK_CUDA(cudaMemsetAsync(ix.c_count.ptr, 0, sizeof(int) * (ncell + 1), s));
     DWG_CHECK_CUDA(cudaMemsetAsync(ix.c_m.ptr, 0, sizeof(unsigned int) * ncell, s));
+    unsigned int* sbits = nullptr;
+    if (a0.seed) {
+        DWG_TRY(ix.c_s.reserve(ncell));
+        DWG_CHECK_CUDA(cudaMemsetAsync(ix.c_s.ptr, 0, sizeof(unsigned int) * ncell, s));
+        sbits = ix.c_s.ptr;
+    }
     DWG_CHECK_CUDA(cudaMemsetAsync(ix.c_misc.ptr, 0, sizeof(int) * 8, s));
     KnnArgs a = a0;
     long long blocks = (nq + 255) / 256;
     const long long cap = (long long)num_sms() * 8;
     if (blocks > cap) blocks = cap;
     if (blocks < 1) blocks = 1;
-    k_cq_key<<<(unsigned)blocks, 256, 0, s>>>(a, ix.q_key.ptr, ix.c_count.ptr, ix.c_m.ptr);
+    k_cq_key<<<(unsigned)blocks, 256, 0, s>>>(a, ix.q_key.ptr, ix.c_count.ptr, ix.c_m.ptr, sbits);
     DWG_CHECK_LAUNCH();
     size_t bytes = 0;
     int* cin = ix.c_count.ptr;
@@ -1447,16 +1483,16 @@ static int knn_query_cells(const KnnIndex& ix, const KnnArgs& a0, long long nq, 
         KnnGrid g{ix.G[0], ix.G[1], ix.G[2], ix.lo[0], ix.lo[1], ix.lo[2], ix.h, ix.inv_h};
         const unsigned char* occ1 = ix.levels >= 1 ? ix.occ.ptr + ix.loff[1] : nullptr;
         k_kb_active<<<num_sms() * 4, 128, 0, s>>>(g, ix.cell_start.ptr, ix.pts.ptr, occ1, ix.ldim[1][0],
-                                                  ix.ldim[1][1], ix.c_active.ptr, ix.c_misc.ptr, ix.kb.ptr);
+                                                  ix.ldim[1][1], ix.c_active.ptr, ix.c_misc.ptr, sbits, ix.kb.ptr);
     }
     k_cq_scatter<<<(unsigned)blocks, 256, 0, s>>>(a, ix.q_key.ptr, ix.c_fill.ptr, ix.q_order.ptr);
     DWG_CHECK_LAUNCH();
     // k = 15 (the triangle queries) keeps 15 slots per lane instead of 16 and
     // k <= 10 (the zero repair) 10: every maximum search and the final sort
     // are shorter, and the lanes hold fewer registers
-    if (a.k == 15) return cells_launch<15>(ix, a, nq, s);
-    if (a.k <= 10) return cells_launch<10>(ix, a, nq, s);
-    return cells_launch<16>(ix, a, nq, s);
+    if (a.k == 15) return cells_launch<15>(ix, a, nq, sbits, s);
+    if (a.k <= 10) return cells_launch<10>(ix, a, nq, sbits, s);
+    return cells_launch<16>(ix, a, nq, sbits, s);
 }
 
 // ------------------------------------------------------------- subsets --
@@ -1563,6 +1599,7 @@ int knn_query(const KnnIndex& ix, const KnnQuery& q, int k, int* out, cudaStream
     a.deep = nullptr;
     a.deep_bound = nullptr;
     a.deep_count = nullptr;
+    a.seed = q.seed;
     if (k <= kKnnBoundK && !q.exclude && ix.n >= kKnnBoundK && q.use_cells) return knn_query_cells(ix, a, q.nq, s);
     // bucket the queries spatially (counting sort on device counts, no host sync)
     DWG_TRY(ix.q_key.reserve(q.nq));

@@ -32,6 +32,7 @@ struct KnnIndex {
     // workspace of the cell-grouped queries
     mutable DevBuf<int> c_count, c_start, c_fill, c_active, c_misc, c_fb, c_deep;
     mutable DevBuf<unsigned int> c_m;
+    mutable DevBuf<unsigned int> c_s;  // per cell: largest |q - x_c| + seed radius (seeded queries)
     mutable DevBuf<float> c_deep_bound;
     mutable DevBuf<unsigned char> c_scratch;
     // query bucketing workspace (grown on demand; not thread safe)
@@ -55,6 +56,10 @@ struct KnnQuery {
     const int* gate_count = nullptr;       // run only when *gate_count > gate_min
     int gate_min = 0;
     bool use_cells = true;                 // allow the cell-grouped search (k <= 16)
+    // per query (null: none): a key above the key of its k-th nearest point
+    // (squared distance bits << 32 | index), ~0 where there is none; the
+    // searches start from it instead of their own bounds where it is lower
+    const unsigned long long* seed = nullptr;
 };
 
 // out[j*k + i] = index of the i-th nearest; -1 when fewer than k candidates

@@ -110,12 +110,47 @@ int diffuse_normals(const int* knn, const float* tn, long long T, const unsigned
     return diffuse_finish(L, N, acc, is_zero, zero_count, s);
 }
 
-// SimpleUpdateNonzeroNormals (src/TurboDWG.cu:322-359)
-__global__ void k_zero_apply(const int* __restrict__ list, const int* __restrict__ count, int gate_min,
-                             const int* __restrict__ nb, int k, float* __restrict__ N) {
+// The seed of each flagged point: points do not move between calls, so any k
+// distinct unflagged points bound its k-th nearest unflagged distance from
+// above, and its k neighbours of the last call that queried it usually still
+// qualify (and are usually its k nearest again).  The key is the largest of
+// their squared distances, computed as the searches compute them and rounded
+// up, over every index: the k nearest keys all lie below it.  Points whose
+// recorded neighbours are incomplete, repeated or flagged get none (~0).
+__global__ void k_seed_keys(const int* __restrict__ list, const int* __restrict__ count, int gate_min,
+                            const int* __restrict__ prev, int k, int L, const unsigned char* __restrict__ is_zero,
+                            const float* __restrict__ P, unsigned long long* __restrict__ seed) {
     const int z = *count;
     if (z <= gate_min) return;
     for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < z; j += gridDim.x * blockDim.x) {
+        const int i = list[j];
+        const float qx = P[(size_t)i * 3], qy = P[(size_t)i * 3 + 1], qz = P[(size_t)i * 3 + 2];
+        int ids[kKnnBoundK];
+        bool ok = true;
+        float mx = 0.f;
+        for (int t = 0; t < k && ok; ++t) {
+            const int c = prev[(size_t)i * k + t];
+            ok = c >= 0 && c < L && !is_zero[c];
+            for (int u = 0; u < t && ok; ++u) ok = ids[u] != c;
+            if (!ok) break;
+            ids[t] = c;
+            const float d2 = sq3_rn(__fsub_rn(P[(size_t)c * 3], qx), __fsub_rn(P[(size_t)c * 3 + 1], qy),
+                                    __fsub_rn(P[(size_t)c * 3 + 2], qz));
+            mx = fmaxf(mx, d2);
+        }
+        seed[j] = ok ? ((unsigned long long)__float_as_uint(mx * 1.00002f) << 32) | 0xffffffffull : ~0ull;
+    }
+}
+
+// SimpleUpdateNonzeroNormals (src/TurboDWG.cu:322-359); the neighbours are
+// also recorded per point for the next call's seeds
+__global__ void k_zero_apply(const int* __restrict__ list, const int* __restrict__ count, int gate_min,
+                             const int* __restrict__ nb, int k, float* __restrict__ N, int* __restrict__ prev) {
+    const int z = *count;
+    if (z <= gate_min) return;
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < z; j += gridDim.x * blockDim.x) {
+        if (prev)
+            for (int t = 0; t < k; ++t) prev[(size_t)list[j] * k + t] = nb[(size_t)j * k + t];
         float sx = 0.f, sy = 0.f, sz = 0.f;
         for (int t = 0; t < k; ++t) {
             int c = nb[(size_t)j * k + t];
@@ -156,9 +191,25 @@ int zero_repair(const KnnIndex& ix, const float* pos, int L, float* N, const uns
     q.nq_dev_i32 = ws.count.ptr;
     q.gate_count = ws.count.ptr;
     q.gate_min = min_zero;
-    DWG_TRY(knn_query(ws.sub, q, k, ws.nb.ptr, s));
     long long blocks = (long long)num_sms() * 4;
-    k_zero_apply<<<(unsigned)blocks, 256, 0, s>>>(ws.list.ptr, ws.count.ptr, min_zero, ws.nb.ptr, k, N);
+    // seeds from the neighbours recorded by earlier calls (k <= 16: the
+    // cell-grouped search); the record starts empty
+    int* prev = nullptr;
+    if (k <= kKnnBoundK) {
+        if (!ws.prev.ptr || ws.prev.n < (size_t)L * k || ws.prev_k != k) {
+            DWG_TRY(ws.prev.reserve((size_t)L * k));
+            DWG_CHECK_CUDA(cudaMemsetAsync(ws.prev.ptr, 0xff, sizeof(int) * (size_t)L * k, s));
+            ws.prev_k = k;
+        }
+        DWG_TRY(ws.seed.reserve(L));
+        k_seed_keys<<<(unsigned)blocks, 256, 0, s>>>(ws.list.ptr, ws.count.ptr, min_zero, ws.prev.ptr, k, L, is_zero,
+                                                     pos, ws.seed.ptr);
+        DWG_CHECK_LAUNCH();
+        q.seed = ws.seed.ptr;
+        prev = ws.prev.ptr;
+    }
+    DWG_TRY(knn_query(ws.sub, q, k, ws.nb.ptr, s));
+    k_zero_apply<<<(unsigned)blocks, 256, 0, s>>>(ws.list.ptr, ws.count.ptr, min_zero, ws.nb.ptr, k, N, prev);
     DWG_CHECK_LAUNCH();
     return DWG_OK;
 }

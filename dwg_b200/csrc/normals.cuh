@@ -28,6 +28,11 @@ struct ZeroRepairWs {
     DevBuf<int> count;
     DevBuf<int> nb;
     DevBuf<unsigned char> scratch;
+    // per point, its k neighbours of the last call that queried it (-1:
+    // none), and per query of this call the key they bound its k-th nearest by
+    DevBuf<int> prev;
+    DevBuf<unsigned long long> seed;
+    int prev_k = 0;
 };
 int zero_repair(const KnnIndex& ix, const float* positions, int L, float* normals, const unsigned char* is_zero,
                 int k, int min_zero, ZeroRepairWs& ws, cudaStream_t s);

@@ -273,7 +273,10 @@ int dwg_diffuse_normals(const int* knn_dev, const float* tri_normals_dev, long l
  * GenerateKDTreeForDWG + kNN + SimpleUpdateNonzeroNormals
  * (src/TurboDWG.cu:145-177,322-359,585-644).  `index` must be built on the
  * same points.  Runs only when the flagged count exceeds `min_zero` (10 in
- * the reference), decided on the device. */
+ * the reference), decided on the device.  The index keeps each flagged
+ * point's neighbours: a later repair on the same index starts that point's
+ * search from them where they are still unflagged (same results, less
+ * search), so repairs on one index are not thread safe. */
 int dwg_zero_repair(dwg_knn_index* index, float* normals_dev, const unsigned char* is_zero_dev,
                     const int* zero_count_dev, int k, int min_zero, void* stream);
 /* Point normals = normalised mean of the normals of the k nearest leaves.

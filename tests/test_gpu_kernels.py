@@ -418,6 +418,33 @@ def test_zero_repair_far_queries_bit_exact(oracle_lib, dwg_lib, k):
     assert np.array_equal(n_dev.cpu().numpy(), ref)
 
 
+@pytest.mark.parametrize("L,k", [(420000, 10), (60000, 16)])
+def test_zero_repair_seeded_repeats_bit_exact(oracle_lib, dwg_lib, L, k):
+    # repairs on one index start each flagged point's search from its
+    # neighbours of the previous repair where those are still unflagged.  A
+    # flagged polar cap that grows (recorded neighbours become flagged: no
+    # seed), shrinks (seeds valid but no longer the nearest) and stays (seeds
+    # exact), with scattered flags that change each time; every repair must
+    # equal the oracle's repair from scratch.  420k points: a grid above 2^22
+    # cells (bounds of the queried cells only; far queries through the
+    # per-thread walk and the warp search), 60k: the whole-grid bound
+    rng = np.random.default_rng(14)
+    v = rng.standard_normal((L, 3))
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    Lpos = (0.45 * v).astype(np.float32)
+    N0 = rng.standard_normal((L, 3)).astype(np.float32)
+    N0 /= np.linalg.norm(N0, axis=1, keepdims=True)
+    ix = turbo.KnnIndex(cu(Lpos))
+    for cap, seed in ((0.8, 1), (0.75, 2), (0.85, 3), (0.85, 3)):
+        isz = (v[:, 2] > cap) | (np.random.default_rng(seed).random(L) < 0.002)
+        ref = oracle_lib.zero_repair(Lpos, N0, isz, k)
+        n_dev, isz_d = cu(N0), cu(isz.astype(np.uint8))
+        zc = torch.tensor([int(isz.sum())], dtype=torch.int32, device=DEV)
+        capi.check(dwg_lib.dwg_zero_repair(ix._h, capi.ptr(n_dev), capi.ptr(isz_d), capi.ptr(zc), k, 10, None))
+        torch.cuda.synchronize()
+        assert np.array_equal(n_dev.cpu().numpy(), ref), cap
+
+
 @pytest.mark.parametrize("tile", [0, 2])
 def test_gwn_grid_lists_bit_identical(tile):
     # dwg_gwn_grid with lists records the grid's interaction lists on its first
