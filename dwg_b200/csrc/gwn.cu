@@ -749,11 +749,16 @@ __global__ void __launch_bounds__(kGwnWarps * 32, 3) k_gwn_replay(GwnArgs a) {
 // entries in shared memory, two chunks in flight while it sums the third:
 // one lane hands each chunk to the bulk-copy (TMA) engine as two 1-D copies
 // (the chunk's weights and its entries are contiguous in global memory) that
-// complete on the ring slot's mbarrier; two 256-thread blocks per SM (106 KB
-// of ring and node records each).  The node terms a slot stands for were
-// counted when it was written.
+// complete on the ring slot's mbarrier.  Grid cells (two samples per lane,
+// 8-byte weights): two 256-thread blocks per SM, 106 KB of ring and node
+// records each; points (one sample, 4-byte weights): three blocks of 58 KB,
+// so that more warps cover the node records' round trips.  The node terms a
+// slot stands for were counted when it was written.
 constexpr int kWreadChunk = 16;
-constexpr int kWreadBlocks = 2;
+template <bool GRID>
+__host__ __device__ constexpr int wread_blocks() {
+    return GRID ? 2 : 3;
+}
 
 // the points of a multi-point leaf for one sample, out of line (rare in the
 // read path; its registers stay off the loop).  The running sum goes in and
@@ -783,11 +788,17 @@ __device__ __noinline__ LeafSum<Acc> leaf_points_ool(const float4* __restrict__ 
     return r;
 }
 constexpr int kWreadRing = 3;
-// per warp: the ring's weights (3 slots x C entries x 32 lanes x 8 bytes;
-// point weights use half), its entries (16 bytes each), then the node
-// records of the chunk being summed (two float4 per entry)
-constexpr int kWreadWarpBytes = kWreadRing * kWreadChunk * (32 * 8 + 16) + 2 * kWreadChunk * 16;
-constexpr int kWreadSmem = kGwnWarps * kWreadWarpBytes;
+// per warp: the ring's weights (3 slots x C entries x 32 lanes x WSIZE
+// bytes), its entries (16 bytes each), then the node records of the chunk
+// being summed (two float4 per entry); every part a multiple of 16 bytes
+template <int WSIZE>
+__host__ __device__ constexpr int wread_warp_bytes() {
+    return kWreadRing * kWreadChunk * (32 * WSIZE + 16) + 2 * kWreadChunk * 16;
+}
+template <bool GRID>
+__host__ __device__ constexpr int wread_smem() {
+    return kGwnWarps * wread_warp_bytes<(int)sizeof(typename WeightOf<nq_of<GRID>()>::T)>();
+}
 
 // 1-D bulk copies global -> shared (the TMA engine), completed on an
 // mbarrier: the barrier's phase completes when its one arrival (with the
@@ -848,13 +859,14 @@ __device__ __forceinline__ bool wread_issue(const W* __restrict__ wp, const int4
 }
 
 template <bool GRID, bool SCREENED, int PREC, int SHAPE>
-__global__ void __launch_bounds__(kGwnWarps * 32, kWreadBlocks) k_gwn_wread(GwnArgs a) {
+__global__ void __launch_bounds__(kGwnWarps * 32, wread_blocks<GRID>()) k_gwn_wread(GwnArgs a) {
     constexpr int NQ = nq_of<GRID>();
     constexpr int C = kWreadChunk;
-    constexpr int WB = kWreadWarpBytes;
     using WT = WeightOf<NQ>;
     using W = typename WT::T;
-    static_assert(sizeof(W) <= 8, "ring sized for two samples per lane");
+    constexpr int WS = (int)sizeof(W);
+    constexpr int WB = wread_warp_bytes<WS>();
+    static_assert(WS % 4 == 0 && (32 * WS) % 16 == 0, "weight rows of whole 16-byte units");
     using Acc = typename AccType<PREC>::T;
     extern __shared__ __align__(16) unsigned char wread_smem[];
     __shared__ __align__(8) unsigned long long wbar[kGwnWarps][kWreadRing];
@@ -864,8 +876,8 @@ __global__ void __launch_bounds__(kGwnWarps * 32, kWreadBlocks) k_gwn_wread(GwnA
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     W* const wring = reinterpret_cast<W*>(wread_smem + warp * WB);
-    int4* const lring = reinterpret_cast<int4*>(wread_smem + warp * WB + kWreadRing * C * 32 * 8);
-    float4* const rec = reinterpret_cast<float4*>(wread_smem + warp * WB + kWreadRing * C * (32 * 8 + 16));
+    int4* const lring = reinterpret_cast<int4*>(wread_smem + warp * WB + kWreadRing * C * 32 * WS);
+    float4* const rec = reinterpret_cast<float4*>(wread_smem + warp * WB + kWreadRing * C * (32 * WS + 16));
     unsigned long long* const bar = wbar[warp];
     if (lane == 0) {
         for (int r = 0; r < kWreadRing; ++r) mbar_init(bar + r);
@@ -1361,14 +1373,14 @@ static int listed_shape(GwnArgs& a, GwnList& L, const Octree& t, cudaStream_t s,
         int& bpw = bpw_dev[dev];
         if (!bpw) {
             DWG_CHECK_CUDA(cudaFuncSetAttribute(k_gwn_wread<GRID, SCREENED, PREC, SHAPE>,
-                                                cudaFuncAttributeMaxDynamicSharedMemorySize, kWreadSmem));
+                                                cudaFuncAttributeMaxDynamicSharedMemorySize, wread_smem<GRID>()));
             DWG_CHECK_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bpw, k_gwn_wread<GRID, SCREENED, PREC, SHAPE>,
-                                                                         kGwnWarps * 32, kWreadSmem));
+                                                                         kGwnWarps * 32, wread_smem<GRID>()));
             if (bpw < 1) bpw = 1;
         }
         const long long all = (long long)num_sms() * bpw;
         const unsigned gw = (unsigned)(a.ngroups < all * kGwnWarps ? (a.ngroups + kGwnWarps - 1) / kGwnWarps : all);
-        k_gwn_wread<GRID, SCREENED, PREC, SHAPE><<<gw, kGwnWarps * 32, kWreadSmem, s>>>(a);
+        k_gwn_wread<GRID, SCREENED, PREC, SHAPE><<<gw, kGwnWarps * 32, wread_smem<GRID>(), s>>>(a);
         DWG_CHECK_LAUNCH();
     }
     return DWG_OK;
