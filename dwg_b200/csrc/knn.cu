@@ -319,6 +319,17 @@ __global__ void k_knn_qscatter(KnnArgs a, int* __restrict__ fill, int* __restric
 
 
 // top-k state of one lane: an unsorted set of KMAX keys and its maximum
+// Batcher's odd-even merge sort on 16 inputs, 63 comparators in 10 layers
+// (the iterative form: for p = 1, 2, 4, 8, for d = p, p/2, ..., 1, for j =
+// d mod p, step 2d, for i < d, join i + j and i + j + d when both lie in the
+// same block of 2p); comparator t orders slots kSortLo[t] < kSortHi[t].  On
+// fewer slots the missing ones count as +infinity: a comparator that touches
+// one never swaps and is left out (59 remain for 15 slots, 32 for 10; the
+// odd-even transposition network took 105 and 45).
+constexpr int kSortNet = 63;
+constexpr unsigned char kSortLo[kSortNet] = {0, 2, 4, 6, 8, 10, 12, 14, 0, 1, 4, 5, 8, 9, 12, 13, 1, 5, 9, 13, 0, 1, 2, 3, 8, 9, 10, 11, 2, 3, 10, 11, 1, 3, 5, 9, 11, 13, 0, 1, 2, 3, 4, 5, 6, 7, 4, 5, 6, 7, 2, 3, 6, 7, 10, 11, 1, 3, 5, 7, 9, 11, 13};
+constexpr unsigned char kSortHi[kSortNet] = {1, 3, 5, 7, 9, 11, 13, 15, 2, 3, 6, 7, 10, 11, 14, 15, 2, 6, 10, 14, 4, 5, 6, 7, 12, 13, 14, 15, 4, 5, 12, 13, 2, 4, 6, 10, 12, 14, 8, 9, 10, 11, 12, 13, 14, 15, 8, 9, 10, 11, 4, 5, 8, 9, 12, 13, 2, 4, 6, 8, 10, 12, 14};
+
 template <int KMAX>
 struct TopK {
     unsigned long long e[KMAX];
@@ -363,6 +374,18 @@ struct TopK {
             replace_max(v);
         }
     }
+    template <int T>
+    __device__ __forceinline__ void sort_net() {
+        if constexpr (T < kSortNet) {
+            constexpr int lo = kSortLo[T], hi = kSortHi[T];
+            if constexpr (hi < KMAX) {
+                const unsigned long long a = e[lo], b = e[hi];
+                e[lo] = a < b ? a : b;
+                e[hi] = a < b ? b : a;
+            }
+            sort_net<T + 1>();
+        }
+    }
     // drop e[0] of a sorted set: the keys move down one slot, NONE enters on top
     __device__ __forceinline__ void shift_down() {
 #pragma unroll
@@ -384,19 +407,11 @@ struct TopK {
                 mpos = q;
             }
     }
-    // ascending order: a register network for small sets, an insertion sort
-    // in local memory otherwise (once per query)
+    // ascending order (once per query): up to 16 slots the sorting network
+    // of sort_net, more slots an insertion sort in local memory
     __device__ __forceinline__ void sort() {
-        if (KMAX <= 16) {
-#pragma unroll
-            for (int pass = 0; pass < KMAX; ++pass) {
-#pragma unroll
-                for (int q = pass & 1; q + 1 < KMAX; q += 2) {
-                    const unsigned long long a = e[q], b = e[q + 1];
-                    e[q] = a < b ? a : b;
-                    e[q + 1] = a < b ? b : a;
-                }
-            }
+        if constexpr (KMAX <= 16) {
+            sort_net<0>();
         } else {
             unsigned long long t[KMAX];
 #pragma unroll
