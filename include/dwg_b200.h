@@ -230,7 +230,7 @@ int dwg_mc_tables(int* edge_table_host, signed char* tri_table_host);
  * grid to 134,217,728 cells (e.g. 512^3); larger grids are rejected with
  * DWG_ERR_INVALID before any GPU work.  The first call on a device looks up
  * the array's device address (cudaGetSymbolAddress) and uploads the case
- * tables; make that first call before any stream capture.  Every call reuses
+ * tables.  Every call reuses
  * the array (the scan rewrites each slot it reads), so calls that overlap on
  * the GPU (different streams or threads at once) race.  The looked-up
  * address and the tables are cached per device ordinal and do not survive a
