@@ -931,18 +931,18 @@ __global__ void __launch_bounds__(kGwnWarps * 32, wread_blocks<GRID>()) k_gwn_wr
             const int4* lc = lring + r * C;
             const unsigned long long first = e0 + c * C;
             const int cnt = e1 - first < (unsigned long long)C ? (int)(e1 - first) : C;
-            // a full chunk of node entries (the common case): the C node
-            // records are loaded at once, a lane each, into shared memory
-            // (one round trip per chunk rather than one per entry), then
-            // summed unrolled
+            // the chunk's node records (for a multi-point leaf, its node's)
+            // are loaded at once, a lane each, into shared memory: one round
+            // trip per chunk rather than one per entry.  A full chunk of node
+            // entries (the common case) is then summed unrolled.
+            if (lane < cnt) {
+                const int x = lc[lane].x & 0x7fffffff;
+                rec[lane] = a.node_a[x];
+                rec[C + lane] = a.node_b[x];
+            }
             const bool full = cnt == C && __ballot_sync(FULL, lc[lane & (C - 1)].x < 0) == 0;
+            __syncwarp();  // the warp's previous readers passed the chunk-end __syncwarp
             if (full) {
-                if (lane < C) {
-                    const int x = lc[lane].x;
-                    rec[lane] = a.node_a[x];
-                    rec[C + lane] = a.node_b[x];
-                }
-                __syncwarp();  // the warp's previous readers passed the chunk-end __syncwarp
 #pragma unroll
                 for (int k = 0; k < C; ++k) {
                     const float4 na = rec[k], nb = rec[C + k];
@@ -958,10 +958,10 @@ __global__ void __launch_bounds__(kGwnWarps * 32, wread_blocks<GRID>()) k_gwn_wr
             }
             for (int k = full ? C : 0; k < cnt; ++k) {
                 const int4 e = lc[k];
+                const float4 na = rec[k], nb = rec[C + k];
                 if (e.x < 0) {  // a multi-point leaf: its points for the lanes that reached it
-                    const int cidx = e.x & 0x7fffffff;
-                    const unsigned meta = (unsigned)__float_as_int(a.node_b[cidx].w);
-                    const int st = (int)(meta & kMetaIndex), pc = __float_as_int(a.node_a[cidx].w);
+                    const unsigned meta = (unsigned)__float_as_int(nb.w);
+                    const int st = (int)(meta & kMetaIndex), pc = __float_as_int(na.w);
 #pragma unroll
                     for (int u = 0; u < NQ; ++u) {
                         if (((unsigned)(u == 0 ? e.y : (u == 1 ? e.z : e.w)) >> lane) & 1u) {
@@ -973,7 +973,6 @@ __global__ void __launch_bounds__(kGwnWarps * 32, wread_blocks<GRID>()) k_gwn_wr
                         }
                     }
                 } else {
-                    const float4 na = a.node_a[e.x], nb = a.node_b[e.x];
                     float wu[NQ];
                     WT::unpack(wc[k * 32 + lane], wu);
 #pragma unroll
