@@ -319,6 +319,25 @@ __global__ void k_knn_qscatter(KnnArgs a, int* __restrict__ fill, int* __restric
 
 
 // top-k state of one lane: an unsorted set of KMAX keys and its maximum
+// (value, slot) of the largest of v[LO, LO + N), the lowest slot among equal
+// values (what a scan from LO with a strict comparison finds), by a
+// tournament: depth log2 N instead of a chain of N - 1 dependent compares
+template <int LO, int N, typename T, int M>
+__device__ __forceinline__ void tour_max(const T (&v)[M], T& m, int& p) {
+    if constexpr (N == 1) {
+        m = v[LO];
+        p = LO;
+    } else {
+        T m1, m2;
+        int p1, p2;
+        tour_max<LO, N / 2>(v, m1, p1);
+        tour_max<LO + N / 2, N - N / 2>(v, m2, p2);
+        const bool r = m2 > m1;
+        m = r ? m2 : m1;
+        p = r ? p2 : p1;
+    }
+}
+
 // Batcher's odd-even merge sort on 16 inputs, 63 comparators in 10 layers
 // (the iterative form: for p = 1, 2, 4, 8, for d = p, p/2, ..., 1, for j =
 // d mod p, step 2d, for i < d, join i + j and i + j + d when both lie in the
@@ -361,14 +380,7 @@ struct TopK {
             for (int q = 0; q < KMAX; ++q)
                 if (q == fill) e[q] = v;
             if (++fill == k) {
-                mx = e[0];
-                mpos = 0;
-#pragma unroll
-                for (int q = 1; q < KMAX; ++q)
-                    if (e[q] > mx) {
-                        mx = e[q];
-                        mpos = q;
-                    }
+                max_slot();
             }
         } else {
             replace_max(v);
@@ -386,6 +398,21 @@ struct TopK {
             sort_net<T + 1>();
         }
     }
+    // mx and mpos: the largest key and its lowest slot
+    __device__ __forceinline__ void max_slot() {
+        if constexpr (KMAX <= 16) {
+            tour_max<0, KMAX>(e, mx, mpos);
+        } else {
+            mx = e[0];
+            mpos = 0;
+#pragma unroll
+            for (int q = 1; q < KMAX; ++q)
+                if (e[q] > mx) {
+                    mx = e[q];
+                    mpos = q;
+                }
+        }
+    }
     // drop e[0] of a sorted set: the keys move down one slot, NONE enters on top
     __device__ __forceinline__ void shift_down() {
 #pragma unroll
@@ -398,14 +425,7 @@ struct TopK {
 #pragma unroll
         for (int q = 0; q < KMAX; ++q)
             if (q == mpos) e[q] = v;
-        mx = e[0];
-        mpos = 0;
-#pragma unroll
-        for (int q = 1; q < KMAX; ++q)
-            if (e[q] > mx) {
-                mx = e[q];
-                mpos = q;
-            }
+        max_slot();
     }
     // ascending order (once per query): up to 16 slots the sorting network
     // of sort_net, more slots an insertion sort in local memory
@@ -703,27 +723,13 @@ __global__ void k_kb_local(KnnGrid g, const int* __restrict__ cell_start, const 
                         for (int q = 0; q < kKnnBoundK; ++q)
                             if (q == cnt) d[q] = d2;
                         if (cnt == kKnnBoundK - 1) {
-                            mx = d[0];
-                            mpos = 0;
-#pragma unroll
-                            for (int q = 1; q < kKnnBoundK; ++q)
-                                if (d[q] > mx) {
-                                    mx = d[q];
-                                    mpos = q;
-                                }
+                            tour_max<0, kKnnBoundK>(d, mx, mpos);
                         }
                     } else if (d2 < mx) {
 #pragma unroll
                         for (int q = 0; q < kKnnBoundK; ++q)
                             if (q == mpos) d[q] = d2;
-                        mx = d[0];
-                        mpos = 0;
-#pragma unroll
-                        for (int q = 1; q < kKnnBoundK; ++q)
-                            if (d[q] > mx) {
-                                mx = d[q];
-                                mpos = q;
-                            }
+                        tour_max<0, kKnnBoundK>(d, mx, mpos);
                     }
                     ++cnt;
                 }
@@ -787,27 +793,13 @@ __global__ void k_kb_active(KnnGrid g, const int* __restrict__ cell_start, const
                                 for (int q = 0; q < kKnnBoundK; ++q)
                                     if (q == cnt) d[q] = d2;
                                 if (cnt == kKnnBoundK - 1) {
-                                    mx = d[0];
-                                    mpos = 0;
-#pragma unroll
-                                    for (int q = 1; q < kKnnBoundK; ++q)
-                                        if (d[q] > mx) {
-                                            mx = d[q];
-                                            mpos = q;
-                                        }
+                                    tour_max<0, kKnnBoundK>(d, mx, mpos);
                                 }
                             } else if (d2 < mx) {
 #pragma unroll
                                 for (int q = 0; q < kKnnBoundK; ++q)
                                     if (q == mpos) d[q] = d2;
-                                mx = d[0];
-                                mpos = 0;
-#pragma unroll
-                                for (int q = 1; q < kKnnBoundK; ++q)
-                                    if (d[q] > mx) {
-                                        mx = d[q];
-                                        mpos = q;
-                                    }
+                                tour_max<0, kKnnBoundK>(d, mx, mpos);
                             }
                             ++cnt;
                         }
